@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""FP32 CSR SpGEMM benchmark on B200 (one process per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload poisson_reuse|plain]
+
+Default workload (the descriptor-reuse case): C = A * A for the 5-point
+Laplacian on a 1024 x 1024 grid (N = 1,048,576, nnz(A) = 5,238,784,
+nnz(C) = 13,611,012, 26,177,544 intermediate products). The structure is
+analysed once; every step rescales A's values entry-wise by U(0.5, 1.5)
+(seeded) and re-executes the numeric phase only, replayed from a CUDA graph.
+
+Printed as one JSON line by rank 0:
+  value   GFLOP/s = 2 * products / step time, device-timed with CUDA events on
+          the plan's stream, operands resident in HBM, L2 flushed (256 MiB
+          write) before every step
+  e2e     the same metric through the public C API (rvsp_spgemm_compute) with
+          pinned host buffers: the H2D copy of the new values and the D2H copy
+          of C inside the timed region (wall clock)
+  roofline  algorithmic bytes of one numeric pass / its kernel time vs the
+          measured HBM copy bandwidth (MEASURED_PEAKS.json)
+  cpu_baseline  the reference's scalar numeric pass (oracle/_ref, compiled
+          from the reference sources) on 1 host core, bounded sample
+With --impl reference the reference's CPU implementation is timed instead,
+on all host cores (row panels), with the same workload, metric and unit.
+
+N > 1 (torchrun): every rank runs its own full-size product on its own GPU
+(independent products, no data-path collective; weak scaling); a gloo
+barrier brackets the timed loop and the step time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+RANK = int(os.environ.get("RANK", "0"))
+WORLD = int(os.environ.get("WORLD_SIZE", "1"))
+LOCAL_RANK = int(os.environ.get("LOCAL_RANK", "0"))
+if WORLD > 1:
+    # one GPU per process: both this process's CUDA runtimes see it as device 0
+    os.environ["CUDA_VISIBLE_DEVICES"] = str(LOCAL_RANK)
+
+sys.path.insert(0, os.path.join(ROOT, "rv-sparse_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "SpGEMM GFLOP/s, HBM % of roofline: learned-binned vs exact-symbolic, 1 B200"
+UNIT = "GFLOP/s"
+
+
+def log(*a):
+    if RANK == 0:
+        print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            idx = os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+
+def poisson_workload():
+    from rvsp_b200 import gen
+    A = gen.poisson2d(1024)
+    P = gen.products(A, A)
+    return A, P
+
+
+def algorithmic_bytes(M, nnz_a, nnz_c, b_rows=None, nnz_b=None):
+    """Compulsory bytes: A's arrays once, B's once when B is a distinct matrix,
+    C's row pointer and its col_idx + values once (read+write on reuse)."""
+    b = 0 if b_rows is None else 4 * (b_rows + 1) + 8 * nnz_b
+    return 4 * (M + 1) + 8 * nnz_a + b + 4 * (M + 1) + 8 * nnz_c
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import torch
+
+    import rvsp_b200 as rv
+
+    dist = None
+    if WORLD > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(0)
+    torch.zeros(1, device="cuda")  # context current on this thread for both runtimes
+    L = rv.lib()
+
+    A, P = poisson_workload()
+    M, nnz_a = A.rows, A.nnz
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    drp, dci, dv = dev(A.row_ptr), dev(A.col_idx), dev(A.values.copy())
+
+    plan = C.c_void_p()
+    rv.check(L.rvsp_cuda_plan_create(C.byref(plan), rv.RVSP_CUDA_ALGO_EXACT), "plan")
+    nnz = C.c_int64()
+    wsz = C.c_size_t()
+    rv.check(L.rvsp_cuda_symbolic(plan, M, A.cols, nnz_a, drp.data_ptr(), dci.data_ptr(), M,
+                                  A.cols, nnz_a, drp.data_ptr(), dci.data_ptr(), C.byref(nnz),
+                                  C.byref(wsz)), "symbolic")
+    nnz_c = nnz.value
+    crp = torch.zeros(M + 1, dtype=torch.int32, device="cuda")
+    cci = torch.zeros(nnz_c, dtype=torch.int32, device="cuda")
+    cv = torch.zeros(nnz_c, dtype=torch.float32, device="cuda")
+    ptrs = lambda: (drp.data_ptr(), dci.data_ptr(), dv.data_ptr(), drp.data_ptr(),  # noqa: E731
+                    dci.data_ptr(), dv.data_ptr(), crp.data_ptr(), cci.data_ptr(), cv.data_ptr())
+    rv.check(L.rvsp_cuda_numeric(plan, *ptrs(), 1, None), "numeric fill")
+    torch.cuda.synchronize()
+    # parity of the first pass against the reference kernel's output digests
+    parity = None
+    gold = os.path.join(ROOT, "tests", "golden", "ref_outputs.json")
+    if os.path.exists(gold):
+        d = json.load(open(gold))["digests"]["poisson2d_1024"]
+        parity = (sha(crp.cpu().numpy()) == d["row_ptr_sha256"] and
+                  sha(cci.cpu().numpy()) == d["col_idx_sha256"] and
+                  sha(cv.cpu().numpy()) == d["values_sha256"])
+    rv.check(L.rvsp_cuda_plan_set_async(plan, 1), "async")
+    stream = torch.cuda.ExternalStream(L.rvsp_cuda_plan_stream(plan))
+
+    rng = np.random.default_rng(1000 + RANK)
+    R = 4
+    variants = [dev((A.values * rng.uniform(0.5, 1.5, nnz_a)).astype(np.float32)) for _ in range(R)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step(i, ev0=None, ev1=None):
+        with torch.cuda.stream(stream):
+            dv.copy_(variants[i % R])
+            flush.zero_()
+            if ev0 is not None:
+                ev0.record(stream)
+            st = L.rvsp_cuda_numeric(plan, *ptrs(), 0, None)
+            if ev1 is not None:
+                ev1.record(stream)
+        rv.check(st, "numeric reuse")
+
+    sampler = ClockSampler()
+    sampler.start()
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    l0 = rv.launch_count()
+    for i in range(args.steps):
+        step(args.warmup + i, *evs[i])
+    torch.cuda.synchronize()
+    launches = rv.launch_count() - l0
+    if dist:
+        dist.barrier()
+    times = [a.elapsed_time(b) for a, b in evs]  # ms
+    ms = sum(times) / len(times)
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t[0])
+    value = 2.0 * P * WORLD / (ms_max * 1e-3) / 1e9
+
+    # end to end through the public API with pinned host buffers
+    e2e = run_e2e(rv, A, P, args, torch)
+    clocks = sampler.stop()
+
+    rv.check(L.rvsp_cuda_plan_set_async(plan, 0))
+    L.rvsp_cuda_plan_destroy(plan)
+    if dist:
+        dist.barrier()
+    if RANK != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    hbm, peak_kind = peaks()
+    bytes_alg = algorithmic_bytes(M, nnz_a, nnz_c)
+    achieved = bytes_alg / (ms * 1e-3) / 1e9
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tr_path):
+        traffic = json.load(open(tr_path)).get("poisson2d_1024_reuse")
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": WORLD,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (5-point Laplacian, values rescaled U(0.5,1.5) per step, seeded)",
+        "config": {"workload": "poisson2d_1024_descriptor_reuse", "grid": 1024, "rows": M,
+                   "nnz_a": nnz_a, "nnz_c": nnz_c, "products": P, "path": "numeric-only, CUDA graph",
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": f"{WORLD} independent products, one per GPU"},
+        "parity_first_pass_vs_reference": parity,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "traffic": traffic,
+                     "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_tiny<REUSE>",
+                     "bytes_per_launch": bytes_alg},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if WORLD == 1:
+        out["cpu_baseline"] = cpu_baseline(A, P)
+    print(json.dumps(out), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_e2e(rv, A, P, args, torch):
+    import ctypes as C
+    L = rv.lib()
+
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        return t
+
+    hrp, hci, hv = pinned(A.row_ptr), pinned(A.col_idx), pinned(A.values.copy())
+    a = rv.csr_struct(A.rows, A.cols, A.nnz, hrp, hci, hv)
+    d = rv.Descriptor(rv.RVSP_SPGEMM_ALGO_CUDA)
+    st, ws, nnz = d.work_estimation(a, a)
+    rv.check(st, "e2e estimation")
+    crp = pinned(np.zeros(A.rows + 1, np.int32))
+    cci = pinned(np.zeros(nnz, np.int32))
+    cv = pinned(np.zeros(nnz, np.float32))
+    wsb = np.zeros(max(ws, 4), np.uint8)
+    c = rv.csr_struct(A.rows, A.cols, nnz, crp, cci, cv)
+    rv.check(d.compute(a, a, c, wsb), "e2e first compute")
+    rng = np.random.default_rng(2000 + RANK)
+    variants = [(A.values * rng.uniform(0.5, 1.5, A.nnz)).astype(np.float32) for _ in range(4)]
+    hvn = hv.numpy()
+    for i in range(args.warmup):
+        hvn[:] = variants[i % 4]
+        rv.check(d.compute(a, a, c, wsb))
+    times = []
+    for i in range(args.steps):
+        hvn[:] = variants[i % 4]
+        t0 = time.perf_counter()
+        st = d.compute(a, a, c, wsb)
+        times.append(time.perf_counter() - t0)
+        rv.check(st, "e2e compute")
+    d.close()
+    t = sum(times) / len(times)
+    return {"value": round(2.0 * P / t / 1e9, 3), "unit": UNIT,
+            "h2d_bytes_per_step": int(A.nnz * 4),
+            "d2h_bytes_per_step": int(nnz * 4 + (A.rows + 1) * 4),
+            "api": "rvsp_spgemm_compute (descriptor reuse), pinned host A/C",
+            "ms_per_step": round(t * 1e3, 4)}
+
+
+def cpu_baseline(A, P, budget_s=10.0):
+    """Reference scalar numeric pass (oracle/_ref) on 1 host core, bounded sample."""
+    import oracle
+    if not oracle.ref_available():
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    rp, ci, _, _, st = oracle.ref_spgemm(A, A)
+    cv = np.zeros(max(int(rp[-1]), 1), np.float32)
+    t1 = oracle.ref_time_numeric(A, A, rp, ci, cv, nthreads=1, repeats=1)
+    reps = max(1, int(budget_s / max(t1, 1e-3)))
+    t = oracle.ref_time_numeric(A, A, rp, ci, cv, nthreads=1, repeats=reps)
+    return {"value": round(2.0 * P * reps / t / 1e9, 4), "unit": UNIT, "cores": 1,
+            "kind": "reference",
+            "sample": f"full 1024^2 Poisson numeric pass (rvsp_spgemm_scalar_f32_numeric) x {reps}, "
+                      f"{t:.1f} s, 1 thread"}
+
+
+def run_reference(args):
+    """The reference's own CPU numeric pass on all host cores (row panels)."""
+    if RANK != 0:
+        return
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/librvsp_ref.so not built"}), flush=True)
+        return
+    A, P = poisson_workload()
+    cores = len(os.sched_getaffinity(0))
+    rp, ci, _, _, st = oracle.ref_spgemm(A, A)
+    cv = np.zeros(max(int(rp[-1]), 1), np.float32)
+    rng = np.random.default_rng(1000)
+    variants = [(A.values * rng.uniform(0.5, 1.5, A.nnz)).astype(np.float32) for _ in range(4)]
+    from rvsp_b200.gen import CSR
+
+    def step(i):
+        Ai = CSR(A.rows, A.cols, A.row_ptr, A.col_idx, variants[i % 4])
+        return oracle.ref_time_numeric(Ai, Ai, rp, ci, cv, nthreads=cores, repeats=1)
+
+    for i in range(args.warmup):
+        step(i)
+    times = [step(args.warmup + i) for i in range(args.steps)]
+    t = sum(times) / len(times)
+    value = 2.0 * P / t / 1e9
+    out = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": WORLD,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 4),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (5-point Laplacian, values rescaled U(0.5,1.5) per step, seeded)",
+           "config": {"workload": "poisson2d_1024_descriptor_reuse", "grid": 1024, "rows": A.rows,
+                      "products": P, "path": "numeric-only (reference rvsp_spgemm_scalar_f32_numeric)"},
+           "impl": "reference",
+           "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores,
+                            "kind": "reference",
+                            "sample": f"full numeric pass per step, {cores} threads on row panels"},
+           "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

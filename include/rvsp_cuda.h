@@ -1,0 +1,155 @@
+/*
+ * rvsp_cuda.h -- the C ABI of the B200 SpGEMM backend.
+ *
+ * This is the boundary the reference's host C calls to reach the GPU: plain
+ * pointers, sizes and status codes, no CUDA or C++ types. Each entry point
+ * names the reference function or struct it replaces when the reference adds
+ * RVSP_BACKEND_CUDA (see INTEGRATION.md for the reference-side patch).
+ *
+ * Conventions
+ *   - Return values are rvsp_status_t codes (0 = success).
+ *   - Array arguments may be host or device pointers (device memory of the
+ *     current CUDA device); residency is detected per pointer.
+ *   - Index arrays are int32, values FP32, op counts int64, as in the
+ *     reference (rv-sparse include/rv_sparse_types.h:53-67).
+ *   - Inputs are canonical CSR, unchecked (rv-sparse
+ *     src/kernels/spgemm/rvsp_spgemm.h:12-17), except in rvsp_cuda_csr_check.
+ *   - A plan is not thread-safe; different plans are independent.
+ */
+
+#ifndef RVSP_CUDA_H
+#define RVSP_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RVSP_CUDA_API __attribute__((visibility("default")))
+#else
+#define RVSP_CUDA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Opaque device-side state of one SpGEMM descriptor. */
+typedef struct rvsp_cuda_plan *rvsp_cuda_plan_t;
+
+/* Plan algorithms (values of rvsp_spgemm_algo_t). */
+#define RVSP_CUDA_ALGO_EXACT 4
+#define RVSP_CUDA_ALGO_LEARNED 5
+
+/* Number of usable CUDA devices (0 when no driver or device). */
+RVSP_CUDA_API int rvsp_cuda_device_count(void);
+
+/* Text of the last CUDA error seen by this library on this thread. */
+RVSP_CUDA_API const char *rvsp_cuda_last_error(void);
+
+/* 1 if p is device (or managed) memory, 0 if host memory. */
+RVSP_CUDA_API int rvsp_cuda_is_device_pointer(const void *p);
+
+/* Frees arrays the one-shot path allocated on the device
+ * (owns_data == RVSP_OWNS_DEVICE; rv-sparse src/core/matrix.c:99-104 frees
+ * host arrays with free()). NULL is accepted. */
+RVSP_CUDA_API void rvsp_cuda_free(void *device_ptr);
+
+/*
+ * Plan lifecycle. Replaces the state of struct rvsp_spgemm_descr
+ * (rv-sparse src/core/spgemm_descr.c:19-37) and its create/destroy
+ * (spgemm_descr.c:66-100). The plan owns a CUDA stream, the analysed
+ * structure on the device and the cached numeric CUDA graph.
+ */
+RVSP_CUDA_API int rvsp_cuda_plan_create(rvsp_cuda_plan_t *plan, int algo);
+RVSP_CUDA_API void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t plan);
+
+/* When async is nonzero, calls whose outputs are all device-resident return
+ * once the work is enqueued on the plan's stream instead of synchronising. */
+RVSP_CUDA_API int rvsp_cuda_plan_set_async(rvsp_cuda_plan_t plan, int async);
+
+/* The plan's cudaStream_t, as an opaque pointer (for event timing). */
+RVSP_CUDA_API void *rvsp_cuda_plan_stream(rvsp_cuda_plan_t plan);
+
+/*
+ * Structure analysis. Replaces rvsp_symbolic_count
+ * (rv-sparse src/kernels/spgemm/rvsp_symbolic.c:13-87) as called by
+ * rvsp_spgemm_work_estimation (spgemm_descr.c:162-255): per-row op counts,
+ * exact nnz per output row, exclusive prefix into C's row pointer, kept on
+ * the device in the plan. Fails with RVSP_ERROR_ALLOCATION_FAILED when
+ * nnz(C) exceeds INT32_MAX (rvsp_symbolic.c:69).
+ * *ws_bytes_out is the device workspace compute needs.
+ */
+RVSP_CUDA_API int rvsp_cuda_symbolic(rvsp_cuda_plan_t plan,
+                       int32_t a_rows, int32_t a_cols, int32_t a_nnz,
+                       const int32_t *a_row_ptr, const int32_t *a_col_idx,
+                       int32_t b_rows, int32_t b_cols, int32_t b_nnz,
+                       const int32_t *b_row_ptr, const int32_t *b_col_idx,
+                       int64_t *c_nnz_out, size_t *ws_bytes_out);
+
+/*
+ * Numeric phase on the analysed structure. Replaces, as driven by
+ * rvsp_spgemm_compute (spgemm_descr.c:257-355): the row-pointer copy
+ * (:325), rvsp_symbolic_fill (rvsp_symbolic.c:91-137) when fill_structure is
+ * nonzero, and the numeric function RVSP_NUMERIC_FN
+ * (rv-sparse src/kernels/spgemm/gustavson_core_f32.inc:18-64 with
+ * accum_scalar_f32.c:20-71). With fill_structure == 0 the column indices in
+ * c_col_idx are taken as the structure and only c_values are written.
+ * workspace may be NULL or host memory (the plan then uses its own device
+ * workspace) or device memory of at least the size symbolic reported.
+ */
+RVSP_CUDA_API int rvsp_cuda_numeric(rvsp_cuda_plan_t plan,
+                      const int32_t *a_row_ptr, const int32_t *a_col_idx, const float *a_values,
+                      const int32_t *b_row_ptr, const int32_t *b_col_idx, const float *b_values,
+                      int32_t *c_row_ptr, int32_t *c_col_idx, float *c_values,
+                      int fill_structure, void *workspace);
+
+/* Per-row intermediate product counts of the last analysis.
+ * Replaces rvsp_spgemm_get_op_counts (spgemm_descr.c:357-380). */
+RVSP_CUDA_API int rvsp_cuda_op_counts(rvsp_cuda_plan_t plan, int64_t *op_counts_out, int32_t n);
+
+/*
+ * One-call product. Replaces the raw kernel rvsp_spgemm_scalar_f32
+ * (RVSP_SPGEMM_PARAMS, rv-sparse src/kernels/spgemm/rvsp_spgemm.h:68-82;
+ * gustavson_core_f32.inc:66-193): analysis, C allocation, fill, numeric.
+ * C's arrays are allocated by the callee where the inputs live (device
+ * inputs: cudaMalloc, release with rvsp_cuda_free; host inputs: malloc,
+ * release with free). op_counts_out is optional (a_rows entries, host or
+ * device). algo is RVSP_CUDA_ALGO_EXACT or RVSP_CUDA_ALGO_LEARNED.
+ */
+RVSP_CUDA_API int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, int32_t b_cols,
+                         const int32_t *a_row_ptr, const int32_t *a_col_idx,
+                         const float *a_values,
+                         const int32_t *b_row_ptr, const int32_t *b_col_idx,
+                         const float *b_values,
+                         int32_t **c_row_ptr_out, int32_t **c_col_idx_out,
+                         float **c_values_out, int32_t *c_nnz_out, int64_t *op_counts_out);
+
+/*
+ * Canonical-CSR check on the device. Replaces rvsp_csr_check
+ * (rv-sparse src/kernels/spgemm/rvsp_support.c:37-127) with the same result
+ * codes (0 ok, 1 bad row_ptr, 2 column out of range, 3 unsorted,
+ * 4 duplicate) and the lowest offending row in *bad_row_out (or -1).
+ */
+RVSP_CUDA_API int rvsp_cuda_csr_check(int32_t rows, int32_t cols, int32_t nnz,
+                        const int32_t *row_ptr, const int32_t *col_idx,
+                        int32_t *bad_row_out);
+
+/*
+ * Basic CSR validation of host or device arrays. Replaces the loops of
+ * rvsp_csr_validate (rv-sparse src/core/matrix.c:51-90): row_ptr[rows] == nnz,
+ * non-decreasing row offsets within [0, nnz], columns in range; sortedness
+ * and duplicates are not checked. Returns RVSP_SUCCESS or
+ * RVSP_ERROR_INVALID_CSR (or a null-pointer / argument error).
+ */
+RVSP_CUDA_API int rvsp_cuda_csr_validate(int32_t rows, int32_t cols, int32_t nnz,
+                           const int32_t *row_ptr, const int32_t *col_idx);
+
+/* Number of kernels this library has launched in this process (graph
+ * replays count each kernel node), for launch accounting in benchmarks. */
+RVSP_CUDA_API int64_t rvsp_cuda_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RVSP_CUDA_H */

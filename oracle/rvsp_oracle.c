@@ -1,0 +1,268 @@
+/*
+ * CPU oracle for FP32 CSR SpGEMM (C = A * B).
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is the checker that the CUDA backend is
+ * compared against. It is loaded by tests/, by __graft_entry__.smoke() and by
+ * the cpu_baseline leg of bench.py, never by the library itself.
+ *
+ * It restates the reference's scalar Gustavson path in plain C:
+ *
+ *   per-row op count and distinct-column count
+ *       rv-sparse src/kernels/spgemm/rvsp_symbolic.c:13-87
+ *   distinct columns of a row, sorted ascending
+ *       rv-sparse src/kernels/spgemm/rvsp_symbolic.c:91-137, rvsp_sort.h:105-124
+ *   numeric pass: for each A entry (k, a) in row order, for each B entry
+ *   (j, b) of row k in order, acc[j] += a * b, starting from +0.0f, then the
+ *   row is drained in ascending column order
+ *       rv-sparse src/kernels/spgemm/gustavson_core_f32.inc:18-64,
+ *       src/kernels/spgemm/accum_scalar_f32.c:20-71 (line 69)
+ *   canonical CSR validation
+ *       rv-sparse src/kernels/spgemm/rvsp_support.c:37-127
+ *
+ * The reference is built with -std=c11, under which GCC does not contract
+ * a * b + c into an FMA. This file is built with -ffp-contract=off for the
+ * same reason, so every product is rounded to FP32 before it is added.
+ *
+ * An FP64 variant of the numeric pass gives the error yardstick for the
+ * FP32 results. It has no reference counterpart.
+ *
+ * Every entry point works on a half-open row range [row_begin, row_end) so a
+ * test can check sampled rows of a product too large to redo in full.
+ */
+
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORACLE_OK 0
+#define ORACLE_ERR_ALLOC -6
+#define ORACLE_ERR_INVALID -2
+
+/* Canonical CSR check; codes follow rvsp_csr_status_t
+ * (rv-sparse src/kernels/spgemm/rvsp_spgemm.h:38-45):
+ * 0 ok, 1 bad row_ptr, 2 column out of range, 3 unsorted, 4 duplicate. */
+int oracle_csr_check(int32_t rows, int32_t cols, const int32_t *row_ptr,
+                     const int32_t *col_idx, int32_t *bad_row_out)
+{
+    if (bad_row_out)
+        *bad_row_out = -1;
+    if (rows < 0 || cols < 0 || !row_ptr || row_ptr[0] != 0)
+        return 1;
+    for (int32_t r = 0; r < rows; r++)
+    {
+        int32_t s = row_ptr[r], e = row_ptr[r + 1];
+        if (e < s)
+        {
+            if (bad_row_out)
+                *bad_row_out = r;
+            return 1;
+        }
+        int32_t last = -1;
+        for (int32_t p = s; p < e; p++)
+        {
+            int32_t c = col_idx[p];
+            int code = 0;
+            if (c < 0 || c >= cols)
+                code = 2;
+            else if (c == last)
+                code = 4;
+            else if (c < last)
+                code = 3;
+            if (code)
+            {
+                if (bad_row_out)
+                    *bad_row_out = r;
+                return code;
+            }
+            last = c;
+        }
+    }
+    return 0;
+}
+
+/* Per-row intermediate products and distinct output columns for rows
+ * [row_begin, row_end). ops_out and cnt_out are indexed from row_begin.
+ * Returns the sum of cnt_out. */
+int64_t oracle_symbolic(int32_t row_begin, int32_t row_end, int32_t n_cols,
+                        const int32_t *a_rp, const int32_t *a_ci,
+                        const int32_t *b_rp, const int32_t *b_ci,
+                        int64_t *ops_out, int64_t *cnt_out)
+{
+    uint8_t *seen = (uint8_t *)calloc((size_t)(n_cols > 0 ? n_cols : 1), 1);
+    int32_t *list = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n_cols > 0 ? n_cols : 1));
+    if (!seen || !list)
+    {
+        free(seen);
+        free(list);
+        return -1;
+    }
+    int64_t total = 0;
+    for (int32_t r = row_begin; r < row_end; r++)
+    {
+        int64_t ops = 0;
+        int64_t cnt = 0;
+        for (int32_t p = a_rp[r]; p < a_rp[r + 1]; p++)
+        {
+            int32_t k = a_ci[p];
+            ops += b_rp[k + 1] - b_rp[k];
+            for (int32_t q = b_rp[k]; q < b_rp[k + 1]; q++)
+            {
+                int32_t j = b_ci[q];
+                if (!seen[j])
+                {
+                    seen[j] = 1;
+                    list[cnt++] = j;
+                }
+            }
+        }
+        for (int64_t t = 0; t < cnt; t++)
+            seen[list[t]] = 0;
+        if (ops_out)
+            ops_out[r - row_begin] = ops;
+        if (cnt_out)
+            cnt_out[r - row_begin] = cnt;
+        total += cnt;
+    }
+    free(seen);
+    free(list);
+    return total;
+}
+
+static int cmp_i32(const void *x, const void *y)
+{
+    int32_t a = *(const int32_t *)x, b = *(const int32_t *)y;
+    return (a > b) - (a < b);
+}
+
+/*
+ * Full product for rows [row_begin, row_end): writes the row offsets
+ * (relative, c_rp[0] = 0, row_end - row_begin + 1 entries), the sorted column
+ * indices and the FP32 values. c_ci / c_v must hold the total returned by
+ * oracle_symbolic for the same range. Values follow the reference's order of
+ * operations exactly.
+ */
+int oracle_spgemm_f32(int32_t row_begin, int32_t row_end, int32_t n_cols,
+                      const int32_t *a_rp, const int32_t *a_ci, const float *a_v,
+                      const int32_t *b_rp, const int32_t *b_ci, const float *b_v,
+                      int64_t *c_rp, int32_t *c_ci, float *c_v)
+{
+    size_t n = (size_t)(n_cols > 0 ? n_cols : 1);
+    uint8_t *seen = (uint8_t *)calloc(n, 1);
+    float *acc = (float *)calloc(n, sizeof(float));
+    if (!seen || !acc)
+    {
+        free(seen);
+        free(acc);
+        return ORACLE_ERR_ALLOC;
+    }
+    int64_t pos = 0;
+    c_rp[0] = 0;
+    for (int32_t r = row_begin; r < row_end; r++)
+    {
+        int64_t start = pos;
+        /* structure: distinct columns, then ascending order */
+        for (int32_t p = a_rp[r]; p < a_rp[r + 1]; p++)
+        {
+            int32_t k = a_ci[p];
+            for (int32_t q = b_rp[k]; q < b_rp[k + 1]; q++)
+            {
+                int32_t j = b_ci[q];
+                if (!seen[j])
+                {
+                    seen[j] = 1;
+                    c_ci[pos++] = j;
+                }
+            }
+        }
+        qsort(c_ci + start, (size_t)(pos - start), sizeof(int32_t), cmp_i32);
+        /* values: k-order, product rounded to FP32, then added */
+        for (int32_t p = a_rp[r]; p < a_rp[r + 1]; p++)
+        {
+            int32_t k = a_ci[p];
+            float a = a_v[p];
+            for (int32_t q = b_rp[k]; q < b_rp[k + 1]; q++)
+            {
+                float prod = a * b_v[q];
+                acc[b_ci[q]] = acc[b_ci[q]] + prod;
+            }
+        }
+        for (int64_t t = start; t < pos; t++)
+        {
+            c_v[t] = acc[c_ci[t]];
+            acc[c_ci[t]] = 0.0f;
+            seen[c_ci[t]] = 0;
+        }
+        c_rp[r - row_begin + 1] = pos;
+    }
+    free(seen);
+    free(acc);
+    return ORACLE_OK;
+}
+
+/*
+ * FP64 numeric pass over a given output pattern (rows [row_begin, row_end),
+ * c_rp relative as produced above). Inputs are the FP32 values widened to
+ * double; the products and sums are exact-ish double arithmetic. This is the
+ * yardstick for the relative error of FP32 results.
+ */
+int oracle_numeric_f64(int32_t row_begin, int32_t row_end, int32_t n_cols,
+                       const int32_t *a_rp, const int32_t *a_ci, const float *a_v,
+                       const int32_t *b_rp, const int32_t *b_ci, const float *b_v,
+                       const int64_t *c_rp, const int32_t *c_ci, double *c_v)
+{
+    double *acc = (double *)calloc((size_t)(n_cols > 0 ? n_cols : 1), sizeof(double));
+    if (!acc)
+        return ORACLE_ERR_ALLOC;
+    for (int32_t r = row_begin; r < row_end; r++)
+    {
+        for (int32_t p = a_rp[r]; p < a_rp[r + 1]; p++)
+        {
+            int32_t k = a_ci[p];
+            double a = (double)a_v[p];
+            for (int32_t q = b_rp[k]; q < b_rp[k + 1]; q++)
+                acc[b_ci[q]] += a * (double)b_v[q];
+        }
+        for (int64_t t = c_rp[r - row_begin]; t < c_rp[r - row_begin + 1]; t++)
+        {
+            c_v[t] = acc[c_ci[t]];
+            acc[c_ci[t]] = 0.0;
+        }
+    }
+    free(acc);
+    return ORACLE_OK;
+}
+
+/*
+ * Numeric-only FP32 pass over a given pattern, the descriptor-reuse path
+ * (rv-sparse src/core/spgemm_descr.c:257-355 with filled_into == C->col_idx:
+ * the structure is kept and only the values are recomputed).
+ */
+int oracle_numeric_f32(int32_t row_begin, int32_t row_end, int32_t n_cols,
+                       const int32_t *a_rp, const int32_t *a_ci, const float *a_v,
+                       const int32_t *b_rp, const int32_t *b_ci, const float *b_v,
+                       const int64_t *c_rp, const int32_t *c_ci, float *c_v)
+{
+    float *acc = (float *)calloc((size_t)(n_cols > 0 ? n_cols : 1), sizeof(float));
+    if (!acc)
+        return ORACLE_ERR_ALLOC;
+    for (int32_t r = row_begin; r < row_end; r++)
+    {
+        for (int32_t p = a_rp[r]; p < a_rp[r + 1]; p++)
+        {
+            int32_t k = a_ci[p];
+            float a = a_v[p];
+            for (int32_t q = b_rp[k]; q < b_rp[k + 1]; q++)
+            {
+                float prod = a * b_v[q];
+                acc[b_ci[q]] = acc[b_ci[q]] + prod;
+            }
+        }
+        for (int64_t t = c_rp[r - row_begin]; t < c_rp[r - row_begin + 1]; t++)
+        {
+            c_v[t] = acc[c_ci[t]];
+            acc[c_ci[t]] = 0.0f;
+        }
+    }
+    free(acc);
+    return ORACLE_OK;
+}

@@ -1,0 +1,634 @@
+// C-ABI implementation of the B200 SpGEMM backend (include/rvsp_cuda.h).
+//
+// A plan is the device-side half of an rv-sparse descriptor
+// (rv-sparse src/core/spgemm_descr.c:19-37): it keeps the analysed structure
+// of C on the device (row pointer, per-row op counts, row bins, heavy work
+// items), staging copies of host-resident operands, and the CUDA graph of the
+// numeric-only pass used when the descriptor is reused.
+//
+// Pipeline of one product (all on the plan's stream):
+//   analysis   k_analyze -> (bin histogram to host) -> k_bin_scatter
+//   count      k_tiny / k_warp / k_heavy in COUNT mode -> k_scan_* -> nnz
+//   fill       the same kernels in FILL mode write sorted columns + values
+//   reuse      REUSE mode writes values on the known pattern (graph replay)
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "rv_sparse_types.h"
+#include "rvsp_cuda.h"
+#include "rvsp_internal.h"
+#include "spgemm_kernels.cuh"
+
+using namespace rvsp;
+
+namespace rvsp {
+
+thread_local std::string g_err;
+std::atomic<long long> g_launches{0};
+
+int fail(cudaError_t e, const char* what) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? RVSP_ERROR_ALLOCATION_FAILED
+                                          : RVSP_ERROR_DEVICE_FAILURE;
+}
+
+bool is_dev(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+cudaError_t DevBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = bytes < 256 ? 256 : bytes;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+
+// ---------------------------------------------------------------------------
+// kernel configuration
+// ---------------------------------------------------------------------------
+template <int CAP, int MODE>
+constexpr int warps_for() {
+    constexpr int per = warp_smem_bytes<CAP, MODE>();
+    constexpr int w = 65536 / per;
+    return w > 8 ? 8 : (w < 1 ? 1 : w);
+}
+
+template <int MODE>
+constexpr int heavy_warps() {
+    return MODE == COUNT ? 8 : 2;
+}
+
+template <int CAP, int MODE>
+static void set_warp_attr() {
+    constexpr int W = warps_for<CAP, MODE>();
+    cudaFuncSetAttribute(k_warp<CAP, W, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         W * warp_smem_bytes<CAP, MODE>());
+}
+
+template <int MODE>
+static void set_mode_attrs() {
+    set_warp_attr<64, MODE>();
+    set_warp_attr<128, MODE>();
+    set_warp_attr<256, MODE>();
+    set_warp_attr<512, MODE>();
+    set_warp_attr<1024, MODE>();
+    set_warp_attr<2048, MODE>();
+    set_warp_attr<4096, MODE>();
+    constexpr int W = heavy_warps<MODE>();
+    cudaFuncSetAttribute(k_heavy<W, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         W * heavy_smem_bytes<MODE>());
+}
+
+static std::once_flag g_attr_once;
+void init_kernel_attributes() {
+    std::call_once(g_attr_once, [] {
+        set_mode_attrs<COUNT>();
+        set_mode_attrs<FILL>();
+        set_mode_attrs<REUSE>();
+        cudaGetLastError();
+    });
+}
+
+void note_launch(rvsp_cuda_plan* plan, int n) {
+    if (plan && plan->capturing)
+        plan->graph_kernels += n;
+    else
+        g_launches += n;
+}
+
+template <int CAP, int MODE>
+static void launch_warp(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B,
+                        const int32_t* rows, int n, const RowOut& o) {
+    constexpr int W = warps_for<CAP, MODE>();
+    const int grid = (n + W - 1) / W;
+    k_warp<CAP, W, MODE><<<grid, W * 32, W * warp_smem_bytes<CAP, MODE>(), plan->stream>>>(
+        A, B, rows, n, o.cnt, o.c_rp, o.c_ci, o.c_v, o.err);
+    note_launch(plan, 1);
+}
+
+template <int MODE>
+static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B,
+                        const RowOut& o) {
+    const int32_t* rows = plan->bin_rows.as<int32_t>();
+    for (int b = BIN_TINY; b < NUM_BINS; ++b) {
+        const int n = plan->bin_count[b];
+        if (n == 0) continue;
+        const int32_t* r = rows + plan->offs.off[b];
+        if (b == BIN_TINY) {
+            k_tiny<MODE><<<(n + TINY_TPB - 1) / TINY_TPB, TINY_TPB, 0, plan->stream>>>(
+                A, B, r, n, o.cnt, o.c_rp, o.c_ci, o.c_v, o.err);
+            note_launch(plan, 1);
+        } else if (b < BIN_HEAVY) {
+            switch (WARP_CAP_MIN << (b - BIN_WARP0)) {
+                case 64: launch_warp<64, MODE>(plan, A, B, r, n, o); break;
+                case 128: launch_warp<128, MODE>(plan, A, B, r, n, o); break;
+                case 256: launch_warp<256, MODE>(plan, A, B, r, n, o); break;
+                case 512: launch_warp<512, MODE>(plan, A, B, r, n, o); break;
+                case 1024: launch_warp<1024, MODE>(plan, A, B, r, n, o); break;
+                case 2048: launch_warp<2048, MODE>(plan, A, B, r, n, o); break;
+                default: launch_warp<4096, MODE>(plan, A, B, r, n, o); break;
+            }
+        } else if (plan->n_items > 0) {
+            constexpr int W = heavy_warps<MODE>();
+            const int grid = (plan->n_items + W - 1) / W;
+            k_heavy<W, MODE><<<grid, W * 32, W * heavy_smem_bytes<MODE>(), plan->stream>>>(
+                A, B, plan->items.as<HeavyItem>(), plan->n_items, plan->item_cnt.as<int32_t>(),
+                o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err);
+            note_launch(plan, 1);
+        }
+    }
+}
+
+void run_rows(rvsp_cuda_plan* plan, int mode, const CsrView& A, const CsrView& B,
+              const RowOut& o) {
+    if (mode == COUNT) launch_bins<COUNT>(plan, A, B, o);
+    else if (mode == FILL) launch_bins<FILL>(plan, A, B, o);
+    else launch_bins<REUSE>(plan, A, B, o);
+}
+
+// Exclusive scan of n int32 counts. total_dev receives the sum.
+int scan_counts(rvsp_cuda_plan* plan, const int32_t* in, int64_t n, int64_t* out64,
+                int32_t* out32, int64_t* total_dev) {
+    const int64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (ntiles == 0) return RVSP_SUCCESS;
+    cudaError_t e = plan->scan_tmp.ensure((size_t)ntiles * sizeof(int64_t));
+    if (e != cudaSuccess) return fail(e, "scan workspace");
+    int64_t* tmp = plan->scan_tmp.as<int64_t>();
+    k_scan_reduce<<<(unsigned)ntiles, SCAN_TPB, 0, plan->stream>>>(in, n, tmp);
+    k_scan_tiles<<<1, SCAN_TPB, 0, plan->stream>>>(tmp, ntiles, total_dev);
+    k_scan_apply<<<(unsigned)ntiles, SCAN_TPB, 0, plan->stream>>>(
+        in, n, tmp, total_dev, out64, out32, &plan->misc.as<Misc>()->overflow);
+    note_launch(plan, 3);
+    return RVSP_SUCCESS;
+}
+
+// Resolves an array to device memory, staging host memory into buf.
+// Index arrays (cache_ok) are re-used when the same host pointer was staged
+// before; values are always re-uploaded.
+template <class T>
+static int resolve(rvsp_cuda_plan* plan, DevBuf& buf, const void*& key, const T* ptr, size_t n,
+                   bool cache_ok, const T** out) {
+    if (n == 0) {
+        cudaError_t e = buf.ensure(sizeof(T));
+        if (e != cudaSuccess) return fail(e, "staging");
+        *out = buf.as<T>();
+        return RVSP_SUCCESS;
+    }
+    if (is_dev(ptr)) {
+        *out = ptr;
+        return RVSP_SUCCESS;
+    }
+    if (!(cache_ok && key == ptr && buf.p)) {
+        cudaError_t e = buf.ensure(n * sizeof(T));
+        if (e != cudaSuccess) return fail(e, "staging alloc");
+        e = cudaMemcpyAsync(buf.p, ptr, n * sizeof(T), cudaMemcpyHostToDevice, plan->stream);
+        if (e != cudaSuccess) return fail(e, "staging copy");
+        key = ptr;
+    }
+    *out = buf.as<T>();
+    return RVSP_SUCCESS;
+}
+
+int stage_operands(rvsp_cuda_plan* plan, const int32_t* a_rp, const int32_t* a_ci,
+                   const float* a_v, const int32_t* b_rp, const int32_t* b_ci,
+                   const float* b_v, bool cache_index, CsrView* A, CsrView* B) {
+    int st;
+    const int32_t *d_arp, *d_aci, *d_brp, *d_bci;
+    const float *d_av = nullptr, *d_bv = nullptr;
+    const size_t an = (size_t)plan->a_nnz, bn = (size_t)plan->b_nnz;
+    if ((st = resolve(plan, plan->s_arp, plan->key[0], a_rp, (size_t)plan->a_rows + 1,
+                      cache_index, &d_arp)))
+        return st;
+    if ((st = resolve(plan, plan->s_aci, plan->key[1], a_ci, an, cache_index, &d_aci))) return st;
+    const void* dummy = nullptr;
+    if (a_v && (st = resolve(plan, plan->s_av, dummy, a_v, an, false, &d_av))) return st;
+    if (b_rp == a_rp && b_ci == a_ci && plan->b_rows == plan->a_rows && bn == an) {
+        d_brp = d_arp;  // C = A * A: one staged copy serves both operands
+        d_bci = d_aci;
+    } else {
+        if ((st = resolve(plan, plan->s_brp, plan->key[2], b_rp, (size_t)plan->b_rows + 1,
+                          cache_index, &d_brp)))
+            return st;
+        if ((st = resolve(plan, plan->s_bci, plan->key[3], b_ci, bn, cache_index, &d_bci)))
+            return st;
+    }
+    if (b_v) {
+        if (b_v == a_v && bn == an) d_bv = d_av;
+        else if ((st = resolve(plan, plan->s_bv, dummy, b_v, bn, false, &d_bv))) return st;
+    }
+    *A = CsrView{d_arp, d_aci, d_av, plan->a_rows, plan->a_cols, plan->a_nnz};
+    *B = CsrView{d_brp, d_bci, d_bv, plan->b_rows, plan->b_cols, plan->b_nnz};
+    return RVSP_SUCCESS;
+}
+
+// Analysis + binning. Leaves per-row op counts, bins and heavy items in the
+// plan; one device->host read of the bin histogram.
+int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool features) {
+    const int64_t M = plan->a_rows;
+    cudaError_t e;
+#define ENS(buf, bytes)                                        \
+    if ((e = (buf).ensure(bytes)) != cudaSuccess) return fail(e, "plan alloc " #buf)
+    ENS(plan->ops, M * 8);
+    ENS(plan->ub, M * 4);
+    ENS(plan->bin, M);
+    ENS(plan->chunk_lo, M * 4);
+    ENS(plan->nchunks, M * 4);
+    ENS(plan->cnt, M * 4);
+    ENS(plan->c_rp, (M + 1) * 4);
+    ENS(plan->bin_rows, M * 4);
+    ENS(plan->misc, sizeof(Misc));
+    if (features) ENS(plan->feat, M * 16);
+    Misc* misc = plan->misc.as<Misc>();
+    if ((e = cudaMemsetAsync(misc, 0, sizeof(Misc), plan->stream)) != cudaSuccess)
+        return fail(e, "memset");
+    AnalyzeOut out{plan->ops.as<int64_t>(), plan->ub.as<int32_t>(), plan->bin.as<uint8_t>(),
+                   plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
+                   features ? plan->feat.as<float4>() : nullptr, misc->hist, misc->totals,
+                   &misc->err};
+    k_analyze<<<(unsigned)((M + AN_TILE - 1) / AN_TILE), AN_TILE, 0, plan->stream>>>(A, B, out);
+    note_launch(plan, 1);
+    if ((e = cudaMemcpyAsync(&plan->host_misc, misc, sizeof(Misc), cudaMemcpyDeviceToHost,
+                             plan->stream)) != cudaSuccess)
+        return fail(e, "histogram read");
+    if ((e = cudaStreamSynchronize(plan->stream)) != cudaSuccess) return fail(e, "analysis");
+    if (plan->host_misc.err) {
+        g_err = "operand structure out of range (row_ptr or col_idx)";
+        return RVSP_ERROR_INVALID_CSR;
+    }
+    int32_t acc = 0;
+    for (int b = 0; b < NUM_BINS; ++b) {
+        plan->bin_count[b] = plan->host_misc.hist[b];
+        plan->offs.off[b] = acc;
+        if (b != BIN_EMPTY) acc += plan->bin_count[b];
+    }
+    plan->n_items = (int32_t)plan->host_misc.totals[0];
+    plan->products = plan->host_misc.totals[1];
+    ENS(plan->items, (size_t)plan->n_items * sizeof(HeavyItem));
+    ENS(plan->item_cnt, (size_t)plan->n_items * 4);
+    ENS(plan->item_scan, ((size_t)plan->n_items + 1) * 8);
+#undef ENS
+    k_bin_scatter<<<(unsigned)((M + 255) / 256), 256, 0, plan->stream>>>(
+        (int32_t)M, plan->bin.as<uint8_t>(), plan->chunk_lo.as<int32_t>(),
+        plan->nchunks.as<int32_t>(), plan->offs, misc->cursor, plan->bin_rows.as<int32_t>(),
+        &misc->item_cursor, plan->items.as<HeavyItem>());
+    note_launch(plan, 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "analysis launch");
+    return RVSP_SUCCESS;
+}
+
+// Exact count + scan: C's row pointer in plan->c_rp, nnz in plan->c_nnz.
+int count_exact(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
+    cudaError_t e;
+    const int64_t M = plan->a_rows;
+    if ((e = cudaMemsetAsync(plan->cnt.p, 0, M * 4, plan->stream)) != cudaSuccess)
+        return fail(e, "memset");
+    Misc* misc = plan->misc.as<Misc>();
+    RowOut o{plan->cnt.as<int32_t>(), nullptr, nullptr, nullptr, &misc->err};
+    run_rows(plan, COUNT, A, B, o);
+    int st = scan_counts(plan, plan->cnt.as<int32_t>(), M, nullptr, plan->c_rp.as<int32_t>(),
+                         &misc->scan_total);
+    if (st) return st;
+    if (plan->n_items > 0) {
+        st = scan_counts(plan, plan->item_cnt.as<int32_t>(), plan->n_items,
+                         plan->item_scan.as<int64_t>(), nullptr, &misc->scan_total2);
+        if (st) return st;
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "count launch");
+    if ((e = cudaMemcpyAsync(&plan->host_misc, misc, sizeof(Misc), cudaMemcpyDeviceToHost,
+                             plan->stream)) != cudaSuccess)
+        return fail(e, "count read");
+    if ((e = cudaStreamSynchronize(plan->stream)) != cudaSuccess) return fail(e, "count");
+    if (plan->host_misc.err) {
+        g_err = "operand structure out of range (row_ptr or col_idx)";
+        return RVSP_ERROR_INVALID_CSR;
+    }
+    if (plan->host_misc.overflow || plan->host_misc.scan_total > INT32_MAX) {
+        g_err = "nnz(C) exceeds INT32_MAX";
+        return RVSP_ERROR_ALLOCATION_FAILED;
+    }
+    plan->c_nnz = plan->host_misc.scan_total;
+    return RVSP_SUCCESS;
+}
+
+void reset_graph(rvsp_cuda_plan* plan) {
+    if (plan->gexec) cudaGraphExecDestroy(plan->gexec);
+    plan->gexec = nullptr;
+    plan->graph_kernels = 0;
+    memset(plan->gkey, 0, sizeof(plan->gkey));
+}
+
+// Numeric-only pass on a known pattern, replayed from a CUDA graph keyed on
+// the device pointers it reads and writes.
+int reuse_numeric(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, const int32_t* c_ci,
+                  float* c_v) {
+    const void* key[8] = {A.rp, A.ci, A.v, B.rp, B.ci, B.v, c_ci, c_v};
+    cudaError_t e;
+    if (!(plan->gexec && memcmp(key, plan->gkey, sizeof(key)) == 0)) {
+        reset_graph(plan);
+        cudaGraph_t g = nullptr;
+        if ((e = cudaStreamBeginCapture(plan->stream, cudaStreamCaptureModeThreadLocal)) !=
+            cudaSuccess)
+            return fail(e, "begin capture");
+        plan->capturing = true;
+        RowOut o{nullptr, plan->c_rp.as<int32_t>(), const_cast<int32_t*>(c_ci), c_v,
+                 &plan->misc.as<Misc>()->err};
+        run_rows(plan, REUSE, A, B, o);
+        plan->capturing = false;
+        e = cudaStreamEndCapture(plan->stream, &g);
+        if (e != cudaSuccess) return fail(e, "end capture");
+        e = cudaGraphInstantiate(&plan->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            plan->gexec = nullptr;
+            return fail(e, "graph instantiate");
+        }
+        memcpy(plan->gkey, key, sizeof(key));
+    }
+    if ((e = cudaGraphLaunch(plan->gexec, plan->stream)) != cudaSuccess)
+        return fail(e, "graph launch");
+    g_launches += plan->graph_kernels;
+    return RVSP_SUCCESS;
+}
+
+}  // namespace rvsp
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int rvsp_cuda_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+const char* rvsp_cuda_last_error(void) { return g_err.c_str(); }
+
+int rvsp_cuda_is_device_pointer(const void* p) { return is_dev(p) ? 1 : 0; }
+
+void rvsp_cuda_free(void* p) {
+    if (p) cudaFree(p);
+}
+
+int64_t rvsp_cuda_launch_count(void) { return (int64_t)g_launches.load(); }
+
+int rvsp_cuda_plan_create(rvsp_cuda_plan_t* out, int algo) {
+    if (!out) return RVSP_ERROR_NULL_POINTER;
+    *out = nullptr;
+    if (algo != RVSP_CUDA_ALGO_EXACT && algo != RVSP_CUDA_ALGO_LEARNED)
+        return RVSP_ERROR_UNSUPPORTED_BACKEND;
+    if (rvsp_cuda_device_count() == 0) {
+        g_err = "no CUDA device";
+        return RVSP_ERROR_UNSUPPORTED_BACKEND;
+    }
+    init_kernel_attributes();
+    rvsp_cuda_plan* p = new (std::nothrow) rvsp_cuda_plan();
+    if (!p) return RVSP_ERROR_ALLOCATION_FAILED;
+    p->algo = algo;
+    // A blocking stream: work the caller queued on the legacy default stream
+    // (e.g. filling device-resident operands) is ordered before the plan's
+    // kernels, and the caller's later default-stream work after them.
+    cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamDefault);
+    if (e != cudaSuccess) {
+        delete p;
+        return fail(e, "stream create");
+    }
+    *out = p;
+    return RVSP_SUCCESS;
+}
+
+void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
+    if (!p) return;
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    reset_graph(p);
+    DevBuf* bufs[] = {&p->s_arp, &p->s_aci, &p->s_av, &p->s_brp, &p->s_bci, &p->s_bv,
+                      &p->ops, &p->ub, &p->bin, &p->chunk_lo, &p->nchunks, &p->feat,
+                      &p->cnt, &p->c_rp, &p->bin_rows, &p->items, &p->item_cnt,
+                      &p->item_scan, &p->scan_tmp, &p->misc, &p->s_cci, &p->s_cv,
+                      &p->pred_cap, &p->slot_off, &p->tmp_ci, &p->tmp_v, &p->row_flag};
+    for (DevBuf* b : bufs) b->release();
+    if (p->stream) cudaStreamDestroy(p->stream);
+    delete p;
+}
+
+int rvsp_cuda_plan_set_async(rvsp_cuda_plan_t p, int async) {
+    if (!p) return RVSP_ERROR_NULL_POINTER;
+    p->async = async ? 1 : 0;
+    return RVSP_SUCCESS;
+}
+
+void* rvsp_cuda_plan_stream(rvsp_cuda_plan_t p) { return p ? (void*)p->stream : nullptr; }
+
+int rvsp_cuda_symbolic(rvsp_cuda_plan_t plan, int32_t a_rows, int32_t a_cols, int32_t a_nnz,
+                       const int32_t* a_rp, const int32_t* a_ci, int32_t b_rows, int32_t b_cols,
+                       int32_t b_nnz, const int32_t* b_rp, const int32_t* b_ci,
+                       int64_t* c_nnz_out, size_t* ws_bytes_out) {
+    if (!plan || !a_rp || !b_rp || !c_nnz_out || !ws_bytes_out) return RVSP_ERROR_NULL_POINTER;
+    if ((a_nnz > 0 && !a_ci) || (b_nnz > 0 && !b_ci)) return RVSP_ERROR_NULL_POINTER;
+    if (a_rows <= 0 || a_cols <= 0 || b_rows <= 0 || b_cols <= 0 || a_nnz < 0 || b_nnz < 0)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    if (a_cols != b_rows) return RVSP_ERROR_INVALID_ARGUMENT;
+    plan->analysed = false;
+    plan->filled = nullptr;
+    plan->filled_host = nullptr;
+    reset_graph(plan);
+    plan->a_rows = a_rows;
+    plan->a_cols = a_cols;
+    plan->a_nnz = a_nnz;
+    plan->b_rows = b_rows;
+    plan->b_cols = b_cols;
+    plan->b_nnz = b_nnz;
+    memset(plan->key, 0, sizeof(plan->key));
+    CsrView A, B;
+    int st = stage_operands(plan, a_rp, a_ci, nullptr, b_rp, b_ci, nullptr, false, &A, &B);
+    if (st) return st;
+    if ((st = analyze(plan, A, B, plan->algo == RVSP_CUDA_ALGO_LEARNED))) return st;
+    if ((st = count_exact(plan, A, B))) return st;
+    plan->analysed = true;
+    *c_nnz_out = plan->c_nnz;
+    *ws_bytes_out = 256;
+    return RVSP_SUCCESS;
+}
+
+int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t* a_ci,
+                      const float* a_v, const int32_t* b_rp, const int32_t* b_ci,
+                      const float* b_v, int32_t* c_rp, int32_t* c_ci, float* c_v,
+                      int fill_structure, void* workspace) {
+    (void)workspace;
+    if (!plan || !a_rp || !b_rp || !c_rp || !c_ci || !c_v) return RVSP_ERROR_NULL_POINTER;
+    if (!a_ci || !a_v || !b_ci || !b_v) return RVSP_ERROR_NULL_POINTER;
+    if (!plan->analysed) return RVSP_ERROR_INVALID_ARGUMENT;
+    CsrView A, B;
+    int st = stage_operands(plan, a_rp, a_ci, a_v, b_rp, b_ci, b_v, true, &A, &B);
+    if (st) return st;
+    cudaError_t e;
+    const int64_t M = plan->a_rows, nnz = plan->c_nnz;
+    const bool dev_rp = is_dev(c_rp), dev_ci = is_dev(c_ci), dev_v = is_dev(c_v);
+    // row pointer: the analysed structure
+    if ((e = cudaMemcpyAsync(c_rp, plan->c_rp.p, (M + 1) * 4,
+                             dev_rp ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                             plan->stream)) != cudaSuccess)
+        return fail(e, "row_ptr copy");
+    int32_t* d_ci = c_ci;
+    float* d_v = c_v;
+    if (!dev_ci) {
+        if ((e = plan->s_cci.ensure((size_t)nnz * 4)) != cudaSuccess) return fail(e, "C staging");
+        d_ci = plan->s_cci.as<int32_t>();
+    }
+    if (!dev_v) {
+        if ((e = plan->s_cv.ensure((size_t)nnz * 4)) != cudaSuccess) return fail(e, "C staging");
+        d_v = plan->s_cv.as<float>();
+    }
+    if (nnz > 0) {
+        if (fill_structure) {
+            RowOut o{nullptr, plan->c_rp.as<int32_t>(), d_ci, d_v, &plan->misc.as<Misc>()->err};
+            run_rows(plan, FILL, A, B, o);
+            if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "fill launch");
+            if (!dev_ci) {
+                if ((e = cudaMemcpyAsync(c_ci, d_ci, (size_t)nnz * 4, cudaMemcpyDeviceToHost,
+                                         plan->stream)) != cudaSuccess)
+                    return fail(e, "col_idx copy");
+                plan->filled_host = c_ci;
+            }
+        } else {
+            if (!dev_ci && plan->filled_host != c_ci) {
+                if ((e = cudaMemcpyAsync(d_ci, c_ci, (size_t)nnz * 4, cudaMemcpyHostToDevice,
+                                         plan->stream)) != cudaSuccess)
+                    return fail(e, "col_idx upload");
+                plan->filled_host = c_ci;
+            }
+            if ((st = reuse_numeric(plan, A, B, d_ci, d_v))) return st;
+        }
+        if (!dev_v &&
+            (e = cudaMemcpyAsync(c_v, d_v, (size_t)nnz * 4, cudaMemcpyDeviceToHost,
+                                 plan->stream)) != cudaSuccess)
+            return fail(e, "values copy");
+    }
+    const bool all_dev = dev_rp && dev_ci && dev_v;
+    if (!(plan->async && all_dev)) {
+        int32_t err = 0;
+        if ((e = cudaMemcpyAsync(&plan->host_misc.err, &plan->misc.as<Misc>()->err, 4,
+                                 cudaMemcpyDeviceToHost, plan->stream)) != cudaSuccess)
+            return fail(e, "error word read");
+        if ((e = cudaStreamSynchronize(plan->stream)) != cudaSuccess) return fail(e, "numeric");
+        err = plan->host_misc.err;
+        if (err) {
+            g_err = "operand structure out of range (row_ptr or col_idx)";
+            return RVSP_ERROR_INVALID_CSR;
+        }
+    }
+    return RVSP_SUCCESS;
+}
+
+int rvsp_cuda_op_counts(rvsp_cuda_plan_t plan, int64_t* out, int32_t n) {
+    if (!plan || !out) return RVSP_ERROR_NULL_POINTER;
+    if (!plan->analysed) return RVSP_ERROR_INVALID_ARGUMENT;
+    if (n < plan->a_rows) return RVSP_ERROR_INVALID_ARGUMENT;
+    cudaError_t e = cudaMemcpyAsync(out, plan->ops.p, (size_t)plan->a_rows * 8,
+                                    is_dev(out) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                    plan->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(plan->stream);
+    return e == cudaSuccess ? RVSP_SUCCESS : fail(e, "op counts");
+}
+
+static int csr_check_impl(bool canonical, int32_t rows, int32_t cols, int32_t nnz,
+                          const int32_t* rp, const int32_t* ci, int32_t* bad_row_out) {
+    if (bad_row_out) *bad_row_out = -1;
+    if (rows < 0 || cols < 0 || nnz < 0 || !rp) return 1;
+    if (nnz > 0 && !ci) return 1;
+    const bool dev = is_dev(rp);
+    int32_t first = 0;
+    cudaError_t e = cudaSuccess;
+    if (dev) {
+        if ((e = cudaMemcpy(&first, rp, 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
+            return fail(e, "csr check");
+    } else {
+        first = rp[0];
+    }
+    if (first != 0) return 1;
+    if (rows == 0) return 0;
+    const int32_t *d_rp = rp, *d_ci = ci;
+    void *tmp_rp = nullptr, *tmp_ci = nullptr, *worst = nullptr;
+    if (!dev) {
+        if ((e = cudaMalloc(&tmp_rp, ((size_t)rows + 1) * 4)) != cudaSuccess) return fail(e, "csr check");
+        cudaMemcpy(tmp_rp, rp, ((size_t)rows + 1) * 4, cudaMemcpyHostToDevice);
+        d_rp = (const int32_t*)tmp_rp;
+    }
+    if (!is_dev(ci) && nnz > 0) {
+        if ((e = cudaMalloc(&tmp_ci, (size_t)nnz * 4)) != cudaSuccess) {
+            cudaFree(tmp_rp);
+            return fail(e, "csr check");
+        }
+        cudaMemcpy(tmp_ci, ci, (size_t)nnz * 4, cudaMemcpyHostToDevice);
+        d_ci = (const int32_t*)tmp_ci;
+    }
+    unsigned long long init = ~0ull, res = ~0ull;
+    e = cudaMalloc(&worst, 8);
+    if (e == cudaSuccess) e = cudaMemcpy(worst, &init, 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        if (canonical)
+            k_csr_check<true><<<(rows + 255) / 256, 256>>>(rows, cols, nnz, d_rp, d_ci,
+                                                           (unsigned long long*)worst);
+        else
+            k_csr_check<false><<<(rows + 255) / 256, 256>>>(rows, cols, nnz, d_rp, d_ci,
+                                                            (unsigned long long*)worst);
+        note_launch(nullptr, 1);
+        e = cudaMemcpy(&res, worst, 8, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(worst);
+    cudaFree(tmp_rp);
+    cudaFree(tmp_ci);
+    if (e != cudaSuccess) return fail(e, "csr check");
+    if (res == ~0ull) return 0;
+    if (bad_row_out) *bad_row_out = (int32_t)(res >> 8);
+    return (int)(res & 0xff);
+}
+
+int rvsp_cuda_csr_check(int32_t rows, int32_t cols, int32_t nnz, const int32_t* rp,
+                        const int32_t* ci, int32_t* bad_row_out) {
+    return csr_check_impl(true, rows, cols, nnz, rp, ci, bad_row_out);
+}
+
+int rvsp_cuda_csr_validate(int32_t rows, int32_t cols, int32_t nnz, const int32_t* rp,
+                           const int32_t* ci) {
+    if (!rp || (nnz > 0 && !ci)) return RVSP_ERROR_NULL_POINTER;
+    if (rows <= 0 || cols <= 0 || nnz < 0) return RVSP_ERROR_INVALID_ARGUMENT;
+    int32_t last = 0;
+    cudaError_t e = is_dev(rp) ? cudaMemcpy(&last, rp + rows, 4, cudaMemcpyDeviceToHost)
+                               : (last = rp[rows], cudaSuccess);
+    if (e != cudaSuccess) return fail(e, "csr validate");
+    if (last != nnz) return RVSP_ERROR_INVALID_CSR;
+    const int st = csr_check_impl(false, rows, cols, nnz, rp, ci, nullptr);
+    if (st < 0) return st;
+    return st == 0 ? RVSP_SUCCESS : RVSP_ERROR_INVALID_CSR;
+}
+
+}  // extern "C"

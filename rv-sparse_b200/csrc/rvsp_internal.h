@@ -1,0 +1,110 @@
+// Internal state shared by the C-ABI translation units of the B200 backend.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+
+#include "spgemm_types.cuh"
+
+namespace rvsp {
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+    template <class T>
+    T* as() const {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
+// Small device-side block of counters and flags of one plan.
+struct Misc {
+    int32_t hist[NUM_BINS];    // rows per bin
+    int32_t cursor[NUM_BINS];  // bin scatter cursors
+    int64_t totals[2];         // heavy items, products
+    int32_t item_cursor;
+    int32_t overflow;          // a 32-bit row pointer would overflow
+    int64_t scan_total;        // nnz(C)
+    int64_t scan_total2;       // heavy item total / learned capacity total
+    int32_t n_overflow_rows;   // learned path: rows that outgrew their capacity
+    int32_t pad;
+    int64_t overflow_ub;       // learned path: sum of upper bounds of those rows
+    int32_t err;               // ERR_* bits raised by kernels
+    int32_t pad2;
+};
+
+// Output pointers of a row-kernel launch.
+struct RowOut {
+    int32_t* cnt;
+    const int32_t* c_rp;
+    int32_t* c_ci;
+    float* c_v;
+    int32_t* err;
+};
+
+extern thread_local std::string g_err;
+extern std::atomic<long long> g_launches;
+
+int fail(cudaError_t e, const char* what);
+bool is_dev(const void* p);
+void init_kernel_attributes();
+
+}  // namespace rvsp
+
+struct rvsp_cuda_plan {
+    int algo = 4;
+    int async = 0;
+    cudaStream_t stream = nullptr;
+    bool analysed = false;
+    bool capturing = false;
+    int32_t a_rows = 0, a_cols = 0, a_nnz = 0, b_rows = 0, b_cols = 0, b_nnz = 0;
+
+    // staging copies of host-resident operands; key[] holds the host
+    // pointers of the staged index arrays (a_rp, a_ci, b_rp, b_ci)
+    rvsp::DevBuf s_arp, s_aci, s_av, s_brp, s_bci, s_bv;
+    const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    // analysed structure
+    rvsp::DevBuf ops, ub, bin, chunk_lo, nchunks, feat, cnt, c_rp, bin_rows;
+    rvsp::DevBuf items, item_cnt, item_scan, scan_tmp, misc;
+    int32_t bin_count[rvsp::NUM_BINS] = {};
+    rvsp::BinOffsets offs = {};
+    int32_t n_items = 0;
+    int64_t c_nnz = 0;
+    int64_t products = 0;
+    rvsp::Misc host_misc = {};
+
+    // device staging of a host-resident C; filled_host is the host col_idx
+    // whose structure the staging currently holds
+    rvsp::DevBuf s_cci, s_cv;
+    const int32_t* filled = nullptr;
+    const int32_t* filled_host = nullptr;
+
+    // learned path
+    rvsp::DevBuf pred_cap, slot_off, tmp_ci, tmp_v, row_flag;
+
+    // numeric-only CUDA graph
+    cudaGraphExec_t gexec = nullptr;
+    const void* gkey[8] = {};
+    int graph_kernels = 0;
+};
+
+namespace rvsp {
+int stage_operands(rvsp_cuda_plan* plan, const int32_t* a_rp, const int32_t* a_ci,
+                   const float* a_v, const int32_t* b_rp, const int32_t* b_ci, const float* b_v,
+                   bool cache_index, CsrView* A, CsrView* B);
+int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool features);
+int count_exact(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B);
+void run_rows(rvsp_cuda_plan* plan, int mode, const CsrView& A, const CsrView& B,
+              const RowOut& o);
+int scan_counts(rvsp_cuda_plan* plan, const int32_t* in, int64_t n, int64_t* out64,
+                int32_t* out32, int64_t* total_dev);
+void note_launch(rvsp_cuda_plan* plan, int n);
+void reset_graph(rvsp_cuda_plan* plan);
+}  // namespace rvsp

@@ -1,0 +1,745 @@
+// Device kernels of the B200 CSR SpGEMM backend (C = A * B, FP32).
+//
+// Gustavson row-wise product, as in rv-sparse
+// src/kernels/spgemm/gustavson_core_f32.inc:18-64 (numeric) and
+// src/kernels/spgemm/rvsp_symbolic.c:13-137 (symbolic count and fill),
+// restructured for the GPU:
+//
+//   k_analyze      per-row op count (rvsp_symbolic.c:41), upper bound on the
+//                  row's distinct columns, learned-model features, bin id
+//   k_bin_scatter  rows grouped by bin; heavy rows expanded into
+//                  (row, column-chunk) work items
+//   k_tiny<MODE>   thread per row, rows with <= 32 products
+//   k_warp<CAP,..> warp per row, shared-memory hash table of CAP slots
+//   k_heavy<..>    warp per (row, column chunk), dense shared-memory
+//                  accumulator + occupancy bitmap over CW columns
+//   k_scan_*       exclusive scan of row counts into C's row pointer
+//
+// Each row kernel runs in one of three modes:
+//   COUNT  distinct output columns per row (rvsp_symbolic_count)
+//   FILL   sorted column indices and values (rvsp_symbolic_fill + numeric)
+//   REUSE  values only, on a known sorted pattern (descriptor reuse)
+//
+// Order of operations. The reference adds, per output column, the FP32
+// products a*b in A-row order starting from +0.0f, with no FMA contraction
+// (accum_scalar_f32.c:69 under -std=c11). Every kernel here reproduces that
+// order exactly: products are formed with __fmul_rn and added with
+// __fadd_rn; a thread or warp owns a whole row (or a whole column chunk of a
+// row); when one warp step holds several products of the same column, they
+// are combined in lane order, which is A-row order (ordered_add below).
+// Values are therefore bit-identical to the reference scalar kernel.
+
+#pragma once
+
+#include "spgemm_types.cuh"
+
+namespace rvsp {
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// Row range [*s, *e) of row r of M. Rows outside the matrix or offsets outside
+// [0, nnz] flag ERR_STRUCTURE and read as empty, so a malformed operand can
+// never send a kernel outside its arrays.
+__device__ __forceinline__ void row_range(const CsrView& M, int r, int* s, int* e,
+                                          int32_t* err) {
+    if ((unsigned)r >= (unsigned)M.rows) {
+        *s = *e = 0;
+        atomicOr(err, ERR_STRUCTURE);
+        return;
+    }
+    const int a = M.rp[r], b = M.rp[r + 1];
+    if (a < 0 || b < a || b > M.nnz) {
+        *s = *e = 0;
+        atomicOr(err, ERR_STRUCTURE);
+        return;
+    }
+    *s = a;
+    *e = b;
+}
+
+__device__ __forceinline__ int warp_incl_scan(int x) {
+    const int lane = lane_id();
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+__device__ __forceinline__ uint32_t hash_slot(int32_t col, int log2cap) {
+    return ((uint32_t)col * 0x9E3779B1u) >> (32 - log2cap);
+}
+
+// First index in [lo, hi) with a[idx] >= target (hi if none); a sorted
+// ascending. Warp-cooperative 32-ary search; all lanes get the result.
+__device__ __forceinline__ int warp_lower_bound(const int32_t* __restrict__ a, int lo, int hi,
+                                                int target) {
+    const int lane = lane_id();
+    while (hi - lo > 32) {
+        const int n = hi - lo;
+        const int stride = (n + 31) >> 5;
+        const int idx = lo + lane * stride;
+        const bool pred = idx < hi && a[idx] < target;
+        const int c = __popc(__ballot_sync(FULL, pred));
+        if (c == 0) return lo;
+        const int nlo = lo + (c - 1) * stride + 1;
+        const int nhi = min(lo + c * stride, hi);
+        lo = nlo;
+        hi = nhi;
+    }
+    const int idx = lo + lane;
+    const bool pred = idx < hi && a[idx] < target;
+    return lo + __popc(__ballot_sync(FULL, pred));
+}
+
+// Position of col in the sorted smem array keys[0, n) (col must be present).
+__device__ __forceinline__ int smem_lower_bound(const int32_t* keys, int n, int32_t col) {
+    int pos = 0;
+    int step = 1;
+    while ((step << 1) <= n) step <<= 1;
+    for (; step > 0; step >>= 1)
+        if (pos + step <= n && keys[pos + step - 1] < col) pos += step;
+    return pos;
+}
+
+// vals[slot] += prod for every active lane, in lane order when several lanes
+// share a slot. Lanes hold consecutive products of the row's flattened
+// (A entry, B entry) sequence, so lane order is the reference's order.
+__device__ __forceinline__ void ordered_add(float* vals, int slot, bool active, float prod) {
+    const int lane = lane_id();
+    const int key = active ? slot : (0x40000000 | lane);
+    const unsigned peers = __match_any_sync(FULL, key);
+    const int n = __popc(peers);
+    const int maxn = __reduce_max_sync(FULL, (unsigned)n);
+    if (maxn == 1) {
+        if (active) vals[slot] = __fadd_rn(vals[slot], prod);
+        return;
+    }
+    const int leader = __ffs(peers) - 1;
+    const bool lead = active && lane == leader;
+    float acc = lead ? vals[slot] : 0.0f;
+    unsigned m = peers;
+    for (int r = 0; r < maxn; ++r) {
+        const int src = m ? (__ffs(m) - 1) : lane;
+        const float v = __shfl_sync(FULL, prod, src);
+        if (lead && m) acc = __fadd_rn(acc, v);
+        m &= m - 1;
+    }
+    if (lead) vals[slot] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// Analysis: one CTA per tile of AN_TILE rows; threads stride over the tile's
+// A entries (a contiguous range of col_idx) so long rows are shared.
+// ---------------------------------------------------------------------------
+constexpr int AN_TILE = 256;
+
+struct AnalyzeOut {
+    int64_t* ops;        // [rows] intermediate products per row
+    int32_t* ub;         // [rows] min(ops, b_cols)
+    uint8_t* bin;        // [rows]
+    int32_t* chunk_lo;   // [rows] first heavy column chunk
+    int32_t* nchunks;    // [rows] heavy column chunks (0 for other bins)
+    float4* feat;        // [rows] learned-model features (optional)
+    int32_t* hist;       // [NUM_BINS] rows per bin
+    int64_t* totals;     // [0] heavy items, [1] products
+    int32_t* err;        // ERR_* bits
+};
+
+__global__ void __launch_bounds__(AN_TILE) k_analyze(CsrView A, CsrView B, AnalyzeOut out) {
+    __shared__ int32_t s_rp[AN_TILE + 1];
+    __shared__ unsigned long long s_ops[AN_TILE];
+    __shared__ int32_t s_maxlen[AN_TILE];
+    __shared__ int32_t s_minc[AN_TILE];
+    __shared__ int32_t s_maxc[AN_TILE];
+    __shared__ int32_t s_hist[NUM_BINS];
+    __shared__ unsigned long long s_items, s_prod;
+
+    const int r0 = blockIdx.x * AN_TILE;
+    const int nr = min(AN_TILE, A.rows - r0);
+    const int t = threadIdx.x;
+    for (int i = t; i <= nr; i += blockDim.x) s_rp[i] = A.rp[r0 + i];
+    for (int i = t; i < nr; i += blockDim.x) {
+        s_ops[i] = 0;
+        s_maxlen[i] = 0;
+        s_minc[i] = INT_MAX;
+        s_maxc[i] = -1;
+    }
+    if (t < NUM_BINS) s_hist[t] = 0;
+    if (t == 0) {
+        s_items = 0;
+        s_prod = 0;
+    }
+    __syncthreads();
+    const int p0 = max(s_rp[0], 0), p1 = min(s_rp[nr], A.nnz);
+    if (t < nr && (s_rp[t] > s_rp[t + 1] || s_rp[t] < 0 || s_rp[t + 1] > A.nnz))
+        atomicOr(out.err, ERR_STRUCTURE);
+    for (int p = p0 + t; p < p1; p += blockDim.x) {
+        int lo = 0, hi = nr;  // largest i with s_rp[i] <= p
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_rp[mid] <= p) lo = mid; else hi = mid;
+        }
+        int bs, be;
+        row_range(B, A.ci[p], &bs, &be, out.err);
+        const int len = be - bs;
+        if (len > 0) {
+            const int first = B.ci[bs], last = B.ci[be - 1];
+            if (first < 0 || last >= B.cols || last < first) {
+                atomicOr(out.err, ERR_STRUCTURE);
+                continue;
+            }
+            atomicAdd(&s_ops[lo], (unsigned long long)len);
+            atomicMax(&s_maxlen[lo], len);
+            atomicMin(&s_minc[lo], first);
+            atomicMax(&s_maxc[lo], last);
+        }
+    }
+    __syncthreads();
+    for (int i = t; i < nr; i += blockDim.x) {
+        const int row = r0 + i;
+        const int64_t ops = (int64_t)s_ops[i];
+        const int32_t ub = (int32_t)min(ops, (int64_t)B.cols);
+        const int b = bin_of(ops, ub);
+        out.ops[row] = ops;
+        out.ub[row] = ub;
+        out.bin[row] = (uint8_t)b;
+        int nch = 0, clo = 0;
+        if (b == BIN_HEAVY) {
+            clo = s_minc[i] / HEAVY_CW;
+            nch = s_maxc[i] / HEAVY_CW - clo + 1;
+            atomicAdd(&s_items, (unsigned long long)nch);
+        }
+        out.chunk_lo[row] = clo;
+        out.nchunks[row] = nch;
+        if (out.feat) {
+            const int anz = s_rp[i + 1] - s_rp[i];
+            const int span = ops > 0 ? s_maxc[i] - s_minc[i] + 1 : 0;
+            out.feat[row] = make_float4((float)anz, (float)ops, (float)s_maxlen[i], (float)span);
+        }
+        atomicAdd(&s_hist[b], 1);
+        atomicAdd(&s_prod, (unsigned long long)ops);
+    }
+    __syncthreads();
+    if (t < NUM_BINS && s_hist[t]) atomicAdd(&out.hist[t], s_hist[t]);
+    if (t == 0) {
+        if (s_items) atomicAdd((unsigned long long*)&out.totals[0], s_items);
+        atomicAdd((unsigned long long*)&out.totals[1], s_prod);
+    }
+}
+
+// Rows grouped by bin (order within a bin is arbitrary; rows are
+// independent). Heavy rows reserve a block of consecutive work items.
+__global__ void k_bin_scatter(int32_t rows, const uint8_t* __restrict__ bin,
+                              const int32_t* __restrict__ chunk_lo,
+                              const int32_t* __restrict__ nchunks, BinOffsets offs,
+                              int32_t* __restrict__ cursor, int32_t* __restrict__ bin_rows,
+                              int32_t* __restrict__ item_cursor, HeavyItem* __restrict__ items) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = lane_id();
+    const int b = row < rows ? (int)bin[row] : -1;
+    const unsigned peers = __match_any_sync(FULL, b);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader && b > BIN_EMPTY) base = atomicAdd(&cursor[b], __popc(peers));
+    base = __shfl_sync(FULL, base, leader);
+    if (b <= BIN_EMPTY) return;
+    const int rank = __popc(peers & ((1u << lane) - 1));
+    bin_rows[offs.off[b] + base + rank] = row;
+    if (b == BIN_HEAVY) {
+        const int n = nchunks[row];
+        const int first = atomicAdd(item_cursor, n);
+        const int lo = chunk_lo[row];
+        for (int c = 0; c < n; ++c) items[first + c] = HeavyItem{row, lo + c, first, 0};
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tiny rows (ops <= 32): one thread per row, the reference loop verbatim.
+// Per-thread scratch is interleaved (element x of thread t at x*TPB + t) so
+// lanes touching the same element index never share a bank.
+// ---------------------------------------------------------------------------
+constexpr int TINY_TPB = 128;
+
+template <int MODE>
+__global__ void __launch_bounds__(TINY_TPB)
+    k_tiny(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
+           int32_t* __restrict__ cnt, const int32_t* __restrict__ c_rp,
+           int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err) {
+    __shared__ int32_t s_col[TINY_CAP * TINY_TPB];
+    __shared__ float s_val[(MODE == COUNT ? 1 : TINY_CAP) * TINY_TPB];
+    const int t = threadIdx.x;
+    const int i = blockIdx.x * TINY_TPB + t;
+    if (i >= nrows) return;
+    const int row = rows[i];
+#define COL(x) s_col[(x) * TINY_TPB + t]
+#define VAL(x) s_val[(x) * TINY_TPB + t]
+    int a0, a1;
+    row_range(A, row, &a0, &a1, err);
+    int n = 0;
+    if (MODE == REUSE) {
+        const int c0 = c_rp[row];
+        n = min(c_rp[row + 1] - c0, TINY_CAP);
+        for (int x = 0; x < n; ++x) COL(x) = c_ci[c0 + x];
+    } else {
+        for (int p = a0; p < a1; ++p) {
+            int q0, q1;
+            row_range(B, A.ci[p], &q0, &q1, err);
+            for (int q = q0; q < q1 && n < TINY_CAP; ++q) COL(n++) = B.ci[q];
+        }
+        for (int x = 1; x < n; ++x) {  // insertion sort
+            const int key = COL(x);
+            int y = x - 1;
+            while (y >= 0 && COL(y) > key) {
+                COL(y + 1) = COL(y);
+                --y;
+            }
+            COL(y + 1) = key;
+        }
+        int m = 0;  // unique
+        for (int x = 0; x < n; ++x) {
+            const int c = COL(x);
+            if (m == 0 || COL(m - 1) != c) COL(m++) = c;
+        }
+        n = m;
+        if (MODE == COUNT) {
+            cnt[row] = n;
+            return;
+        }
+        const int c0 = c_rp[row];
+        for (int x = 0; x < n; ++x) c_ci[c0 + x] = COL(x);
+    }
+    if constexpr (MODE != COUNT) {
+        for (int x = 0; x < n; ++x) VAL(x) = 0.0f;
+        for (int p = a0; p < a1; ++p) {
+            const float a = A.v[p];
+            int q0, q1;
+            row_range(B, A.ci[p], &q0, &q1, err);
+            for (int q = q0; q < q1; ++q) {
+                const int col = B.ci[q];
+                int pos = 0, step = 1;
+                while ((step << 1) <= n) step <<= 1;
+                for (; step > 0; step >>= 1)
+                    if (pos + step <= n && COL(pos + step - 1) < col) pos += step;
+                if (pos < n) VAL(pos) = __fadd_rn(VAL(pos), __fmul_rn(a, B.v[q]));
+            }
+        }
+        const int c0 = c_rp[row];
+        for (int x = 0; x < n; ++x) c_v[c0 + x] = VAL(x);
+    }
+#undef COL
+#undef VAL
+}
+
+// ---------------------------------------------------------------------------
+// Medium rows: one warp per row, CAP-slot shared-memory table per warp.
+// The row's products are processed 32 at a time in flattened
+// (A entry, B entry) order; each lane locates its A entry with a 5-step
+// search over the warp's inclusive scan of B-row lengths.
+// ---------------------------------------------------------------------------
+template <int CAP, int MODE>
+__host__ __device__ constexpr int warp_smem_bytes() {
+    return (MODE == COUNT ? 4 : 8) * CAP;
+}
+
+template <int CAP, int WARPS, int MODE>
+__global__ void __launch_bounds__(WARPS * 32)
+    k_warp(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
+           int32_t* __restrict__ cnt, const int32_t* __restrict__ c_rp,
+           int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int LOG2CAP = __builtin_ctz(CAP);
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    int32_t* keys = reinterpret_cast<int32_t*>(smem + warp * warp_smem_bytes<CAP, MODE>());
+    float* vals = reinterpret_cast<float*>(keys + CAP);
+    volatile int32_t* vkeys = keys;
+
+    for (int w = blockIdx.x * WARPS + warp; w < nrows; w += gridDim.x * WARPS) {
+        const int row = rows[w];
+        int L = 0, c0 = 0;
+        if (MODE == REUSE) {
+            c0 = c_rp[row];
+            L = min(c_rp[row + 1] - c0, CAP);
+            for (int x = lane; x < L; x += 32) {
+                keys[x] = c_ci[c0 + x];
+                vals[x] = 0.0f;
+            }
+        } else {
+            for (int x = lane; x < CAP; x += 32) {
+                keys[x] = -1;
+                if (MODE == FILL) vals[x] = 0.0f;
+            }
+        }
+        __syncwarp();
+        int count = 0;
+        int a0, a1;
+        row_range(A, row, &a0, &a1, err);
+        for (int base = a0; base < a1; base += 32) {
+            const int j = base + lane;
+            int bs = 0, bl = 0;
+            float av = 0.0f;
+            if (j < a1) {
+                int be;
+                row_range(B, A.ci[j], &bs, &be, err);
+                bl = be - bs;
+                if (MODE != COUNT) av = A.v[j];
+            }
+            const int incl = warp_incl_scan(bl);
+            const int total = __shfl_sync(FULL, incl, 31);
+            for (int f = 0; f < total; f += 32) {
+                const int p = f + lane;
+                const bool pv = p < total;
+                int e = 0;
+#pragma unroll
+                for (int s = 16; s >= 1; s >>= 1) {
+                    const int cand = __shfl_sync(FULL, incl, e + s - 1);
+                    if (cand <= p) e += s;
+                }
+                e = min(e, 31);
+                const int e_incl = __shfl_sync(FULL, incl, e);
+                const int e_bl = __shfl_sync(FULL, bl, e);
+                const int e_bs = __shfl_sync(FULL, bs, e);
+                const float e_av = __shfl_sync(FULL, av, e);
+                int col = -1;
+                float bv = 0.0f;
+                if (pv) {
+                    const int q = e_bs + (p - (e_incl - e_bl));
+                    col = B.ci[q];
+                    if (MODE != COUNT) bv = B.v[q];
+                }
+                int slot = -1;
+                bool ok = pv;
+                if (MODE == REUSE) {
+                    if (pv) {
+                        slot = smem_lower_bound(keys, L, col);
+                        ok = slot < L;
+                    }
+                } else {
+                    bool inserted = false;
+                    if (pv) {
+                        // at most CAP probes: a table can only fill up when an
+                        // operand breaks the column-range contract
+                        uint32_t h = hash_slot(col, LOG2CAP);
+                        ok = false;
+                        for (int probe = 0; probe < CAP; ++probe) {
+                            const int cur = vkeys[h];
+                            if (cur == col) {
+                                ok = true;
+                                break;
+                            }
+                            if (cur == -1) {
+                                const int old = atomicCAS(&keys[h], -1, col);
+                                if (old == -1 || old == col) {
+                                    inserted = old == -1;
+                                    ok = true;
+                                    break;
+                                }
+                            }
+                            h = (h + 1) & (CAP - 1);
+                        }
+                        if (!ok) atomicOr(err, ERR_STRUCTURE);
+                        slot = (int)h;
+                    }
+                    count += __popc(__ballot_sync(FULL, inserted));
+                }
+                if (MODE != COUNT) ordered_add(vals, slot, ok, __fmul_rn(e_av, bv));
+                __syncwarp();
+            }
+        }
+        __syncwarp();
+        if (MODE == COUNT) {
+            if (lane == 0) cnt[row] = count;
+        } else if (MODE == REUSE) {
+            for (int x = lane; x < L; x += 32) c_v[c0 + x] = vals[x];
+        } else {
+            // compact occupied slots to the front (left moves only)
+            int out = 0;
+            for (int b0 = 0; b0 < CAP; b0 += 32) {
+                const int key = keys[b0 + lane];
+                const float val = vals[b0 + lane];
+                const bool ok = key != -1;
+                const unsigned m = __ballot_sync(FULL, ok);
+                __syncwarp();
+                if (ok) {
+                    const int pos = out + __popc(m & ((1u << lane) - 1));
+                    keys[pos] = key;
+                    vals[pos] = val;
+                }
+                out += __popc(m);
+                __syncwarp();
+            }
+            const int n = out;
+            int P = 1;
+            while (P < n) P <<= 1;
+            for (int x = n + lane; x < P; x += 32) keys[x] = INT_MAX;
+            __syncwarp();
+            for (int k = 2; k <= P; k <<= 1) {  // bitonic sort of (key, val)
+                for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                    for (int i = lane; i < P; i += 32) {
+                        const int ixj = i ^ jj;
+                        if (ixj > i) {
+                            const int ki = keys[i], kj = keys[ixj];
+                            const bool up = (i & k) == 0;
+                            if ((ki > kj) == up) {
+                                keys[i] = kj;
+                                keys[ixj] = ki;
+                                const float t0 = vals[i];
+                                vals[i] = vals[ixj];
+                                vals[ixj] = t0;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            const int o = c_rp[row];
+            for (int x = lane; x < n; x += 32) {
+                c_ci[o + x] = keys[x];
+                c_v[o + x] = vals[x];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Heavy rows: one warp per (row, chunk of HEAVY_CW columns). The warp walks
+// the row's A entries in order; for each B row that reaches the chunk it
+// locates the chunk's sub-range and adds the products into a dense
+// accumulator (distinct columns within one B row, so no two lanes collide).
+// ---------------------------------------------------------------------------
+template <int MODE>
+__host__ __device__ constexpr int heavy_smem_bytes() {
+    return (MODE == COUNT ? 0 : 4 * HEAVY_CW) + (MODE == REUSE ? 0 : HEAVY_CW / 8);
+}
+
+template <int WARPS, int MODE>
+__global__ void __launch_bounds__(WARPS * 32)
+    k_heavy(CsrView A, CsrView B, const HeavyItem* __restrict__ items, int nitems,
+            int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
+            const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
+            int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int NW = HEAVY_CW / 32;
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    unsigned char* mine = smem + warp * heavy_smem_bytes<MODE>();
+    float* acc = reinterpret_cast<float*>(mine);
+    unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * HEAVY_CW));
+
+    for (int w = blockIdx.x * WARPS + warp; w < nitems; w += gridDim.x * WARPS) {
+        const HeavyItem it = items[w];
+        const int row = it.row;
+        const int lo = it.chunk * HEAVY_CW;
+        const int hi = min(lo + HEAVY_CW, B.cols);
+        if (MODE != COUNT)
+            for (int x = lane; x < HEAVY_CW; x += 32) acc[x] = 0.0f;
+        if (MODE != REUSE)
+            for (int x = lane; x < NW; x += 32) bits[x] = 0u;
+        __syncwarp();
+        int a0, a1;
+        row_range(A, row, &a0, &a1, err);
+        for (int base = a0; base < a1; base += 32) {
+            const int j = base + lane;
+            int bs = 0, be = 0;
+            float av = 0.0f;
+            bool hit = false;
+            if (j < a1) {
+                row_range(B, A.ci[j], &bs, &be, err);
+                if (MODE != COUNT) av = A.v[j];
+                hit = be > bs && B.ci[be - 1] >= lo && B.ci[bs] < hi;
+            }
+            unsigned hm = __ballot_sync(FULL, hit);
+            while (hm) {
+                const int e = __ffs(hm) - 1;
+                hm &= hm - 1;
+                const int ebs = __shfl_sync(FULL, bs, e);
+                const int ebe = __shfl_sync(FULL, be, e);
+                const float eav = __shfl_sync(FULL, av, e);
+                const int s = warp_lower_bound(B.ci, ebs, ebe, lo);
+                const int t = warp_lower_bound(B.ci, s, ebe, hi);
+                for (int q = s + lane; q < t; q += 32) {
+                    const int col = B.ci[q] - lo;
+                    if ((unsigned)col >= (unsigned)HEAVY_CW) {
+                        atomicOr(err, ERR_STRUCTURE);
+                        continue;
+                    }
+                    if (MODE != REUSE) atomicOr(&bits[col >> 5], 1u << (col & 31));
+                    if (MODE != COUNT) acc[col] = __fadd_rn(acc[col], __fmul_rn(eav, B.v[q]));
+                }
+                __syncwarp();
+            }
+        }
+        __syncwarp();
+        if (MODE == COUNT) {
+            int c = 0;
+            for (int x = lane; x < NW; x += 32) c += __popc(bits[x]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+            if (lane == 0) {
+                item_cnt[w] = c;
+                if (c) atomicAdd(&row_cnt[row], c);
+            }
+        } else if (MODE == FILL) {
+            int64_t out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
+            for (int x0 = 0; x0 < NW; x0 += 32) {
+                unsigned word = bits[x0 + lane];
+                const int pc = __popc(word);
+                const int incl = warp_incl_scan(pc);
+                int64_t pos = out + (incl - pc);
+                while (word) {
+                    const int b = __ffs(word) - 1;
+                    word &= word - 1;
+                    const int col = (x0 + lane) * 32 + b;
+                    c_ci[pos] = lo + col;
+                    c_v[pos] = acc[col];
+                    ++pos;
+                }
+                out += __shfl_sync(FULL, incl, 31);
+            }
+        } else {
+            const int r0 = c_rp[row], r1 = c_rp[row + 1];
+            const int s = warp_lower_bound(c_ci, r0, r1, lo);
+            const int t = warp_lower_bound(c_ci, s, r1, hi);
+            for (int q = s + lane; q < t; q += 32) {
+                const int col = c_ci[q] - lo;
+                c_v[q] = (unsigned)col < (unsigned)HEAVY_CW ? acc[col] : 0.0f;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan of int32 counts (reduce -> scan tile sums -> apply).
+// ---------------------------------------------------------------------------
+constexpr int SCAN_TPB = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_TPB * SCAN_ITEMS;
+
+__device__ __forceinline__ int64_t block_excl_scan64(int64_t x, int64_t* total) {
+    __shared__ int64_t s_warp[SCAN_TPB / 32];
+    const int lane = lane_id(), warp = threadIdx.x >> 5;
+    int64_t incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const int64_t v = lane < SCAN_TPB / 32 ? s_warp[lane] : 0;
+        int64_t vi = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(FULL, vi, o);
+            if (lane >= o) vi += y;
+        }
+        if (lane < SCAN_TPB / 32) s_warp[lane] = vi - v;
+        if (lane == SCAN_TPB / 32 - 1) *total = vi;
+    }
+    __syncthreads();
+    const int64_t r = s_warp[warp] + incl - x;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(SCAN_TPB)
+    k_scan_reduce(const int32_t* __restrict__ in, int64_t n, int64_t* __restrict__ tile_sums) {
+    __shared__ int64_t s_total;
+    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    int64_t s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i)
+        if (base + i < n) s += in[base + i];
+    block_excl_scan64(s, &s_total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = s_total;
+}
+
+// One CTA: exclusive scan of the tile sums in place; total to *total.
+__global__ void __launch_bounds__(SCAN_TPB)
+    k_scan_tiles(int64_t* __restrict__ tile_sums, int64_t ntiles, int64_t* __restrict__ total) {
+    __shared__ int64_t s_total;
+    int64_t carry = 0;
+    for (int64_t b0 = 0; b0 < ntiles; b0 += SCAN_TPB) {
+        const int64_t i = b0 + threadIdx.x;
+        const int64_t v = i < ntiles ? tile_sums[i] : 0;
+        const int64_t ex = block_excl_scan64(v, &s_total);
+        if (i < ntiles) tile_sums[i] = carry + ex;
+        carry += s_total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// out64[i] / out32[i] = exclusive prefix; out[n] = total. Sets *overflow
+// when a 32-bit output would exceed INT32_MAX.
+__global__ void __launch_bounds__(SCAN_TPB)
+    k_scan_apply(const int32_t* __restrict__ in, int64_t n, const int64_t* __restrict__ tile_sums,
+                 const int64_t* __restrict__ total, int64_t* __restrict__ out64,
+                 int32_t* __restrict__ out32, int32_t* __restrict__ overflow) {
+    __shared__ int64_t s_total;
+    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    int32_t v[SCAN_ITEMS];
+    int64_t s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        v[i] = base + i < n ? in[base + i] : 0;
+        s += v[i];
+    }
+    int64_t run = tile_sums[blockIdx.x] + block_excl_scan64(s, &s_total);
+    bool ovf = false;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        if (base + i < n) {
+            if (out64) out64[base + i] = run;
+            if (out32) {
+                out32[base + i] = (int32_t)run;
+                ovf |= run > INT32_MAX;
+            }
+        }
+        run += v[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int64_t tot = *total;
+        if (out64) out64[n] = tot;
+        if (out32) {
+            out32[n] = (int32_t)tot;
+            ovf |= tot > INT32_MAX;
+        }
+    }
+    if (ovf) atomicExch(overflow, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Canonical CSR check (rv-sparse src/kernels/spgemm/rvsp_support.c:37-127):
+// thread per row; the lowest failing row wins. Row offsets outside [0, nnz]
+// are reported as a bad row pointer before any column is read.
+// ---------------------------------------------------------------------------
+// With CANONICAL == false only the row pointer and the column range are
+// checked (rv-sparse src/core/matrix.c:51-90, rvsp_csr_validate).
+template <bool CANONICAL>
+__global__ void k_csr_check(int32_t rows, int32_t cols, int32_t nnz,
+                            const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                            unsigned long long* __restrict__ worst) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    const int s = rp[r], e = rp[r + 1];
+    int code = 0;
+    if (e < s || s < 0 || e > nnz) {
+        code = 1;
+    } else {
+        int last = -1;
+        for (int p = s; p < e && !code; ++p) {
+            const int c = ci[p];
+            if (c < 0 || c >= cols) code = 2;
+            else if (CANONICAL && c == last) code = 4;
+            else if (CANONICAL && c < last) code = 3;
+            last = c;
+        }
+    }
+    if (code) atomicMin(worst, ((unsigned long long)(uint32_t)r << 8) | (unsigned)code);
+}
+
+}  // namespace rvsp

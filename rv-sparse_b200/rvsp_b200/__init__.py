@@ -1,0 +1,240 @@
+"""ctypes binding of librvsp_b200.so (the rv-sparse C API on the B200 backend).
+
+The library is the product; this module only loads it and mirrors its C
+declarations (include/rv_sparse.h, include/rv_sparse_types.h,
+include/rvsp_cuda.h) so tests and benchmarks can drive it from Python. It
+never computes a product itself: when the shared library is missing every
+entry point raises instead of falling back to anything.
+
+Array arguments accept numpy arrays (host memory) or objects exposing a
+device pointer via ``data_ptr()`` (e.g. CUDA tensors), matching the library's
+per-pointer residency rule.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "librvsp_b200.so")
+
+# rv_sparse_types.h
+RVSP_SUCCESS = 0
+RVSP_ERROR_NULL_POINTER = -1
+RVSP_ERROR_INVALID_ARGUMENT = -2
+RVSP_ERROR_INVALID_CSR = -3
+RVSP_ERROR_UNSUPPORTED_DTYPE = -4
+RVSP_ERROR_UNSUPPORTED_BACKEND = -5
+RVSP_ERROR_ALLOCATION_FAILED = -6
+RVSP_ERROR_DEVICE_FAILURE = -7
+
+RVSP_DTYPE_INT8, RVSP_DTYPE_INT32, RVSP_DTYPE_BF16, RVSP_DTYPE_FP32, RVSP_DTYPE_FP64 = range(5)
+RVSP_FORMAT_CSR = 0
+(RVSP_BACKEND_SCALAR, RVSP_BACKEND_SCALAR_UNROLL4, RVSP_BACKEND_RVV_INTRINSICS,
+ RVSP_BACKEND_CUDA, RVSP_BACKEND_CUDA_LEARNED) = range(5)
+(RVSP_SPGEMM_ALGO_DEFAULT, RVSP_SPGEMM_ALGO_RVV, RVSP_SPGEMM_ALGO_CONTIG,
+ RVSP_SPGEMM_ALGO_ADAPTIVE, RVSP_SPGEMM_ALGO_CUDA, RVSP_SPGEMM_ALGO_CUDA_LEARNED) = range(6)
+RVSP_OWNS_HOST = 1
+RVSP_OWNS_DEVICE = 2
+RVSP_CUDA_ALGO_EXACT = 4
+RVSP_CUDA_ALGO_LEARNED = 5
+
+
+class CsrMatrix(C.Structure):
+    """rvsp_csr_matrix_t"""
+    _fields_ = [("rows", C.c_int32), ("cols", C.c_int32), ("nnz", C.c_int32),
+                ("row_ptr", C.c_void_p), ("col_idx", C.c_void_p), ("values", C.c_void_p),
+                ("dtype", C.c_int), ("format", C.c_int), ("owns_data", C.c_int)]
+
+
+class SpgemmOptions(C.Structure):
+    """rvsp_spgemm_options_t"""
+    _fields_ = [("backend", C.c_int), ("input_dtype", C.c_int), ("output_dtype", C.c_int)]
+
+
+class RvspError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"{what}: status {status} ({status_string(status)}) {last_error()}")
+
+
+_lib = None
+
+_VP = C.c_void_p
+_I32 = C.c_int32
+_I64 = C.c_int64
+
+_PROTOS = {
+    # rv_sparse.h
+    "rvsp_get_version": (C.c_char_p, []),
+    "rvsp_status_to_string": (C.c_char_p, [C.c_int]),
+    "rvsp_csr_create": (C.c_int, [C.POINTER(CsrMatrix), _I32, _I32, _I32, _VP, _VP, _VP, C.c_int]),
+    "rvsp_csr_validate": (C.c_int, [C.POINTER(CsrMatrix)]),
+    "rvsp_csr_destroy": (None, [C.POINTER(CsrMatrix)]),
+    "rvsp_spgemm_csr": (C.c_int, [C.POINTER(CsrMatrix), C.POINTER(CsrMatrix), C.POINTER(CsrMatrix),
+                                  C.POINTER(SpgemmOptions)]),
+    "rvsp_spgemm_descr_create": (C.c_int, [C.POINTER(_VP)]),
+    "rvsp_spgemm_descr_destroy": (None, [_VP]),
+    "rvsp_spgemm_set_algo": (C.c_int, [_VP, C.c_int]),
+    "rvsp_spgemm_work_estimation": (C.c_int, [_VP, C.POINTER(CsrMatrix), C.POINTER(CsrMatrix),
+                                              C.POINTER(C.c_size_t), C.POINTER(_I32)]),
+    "rvsp_spgemm_compute": (C.c_int, [_VP, C.POINTER(CsrMatrix), C.POINTER(CsrMatrix),
+                                      C.POINTER(CsrMatrix), _VP]),
+    "rvsp_spgemm_get_op_counts": (C.c_int, [_VP, _VP, _I32]),
+    "rvsp_spgemm_invalidate_structure": (None, [_VP]),
+    # rvsp_cuda.h
+    "rvsp_cuda_device_count": (C.c_int, []),
+    "rvsp_cuda_last_error": (C.c_char_p, []),
+    "rvsp_cuda_is_device_pointer": (C.c_int, [_VP]),
+    "rvsp_cuda_free": (None, [_VP]),
+    "rvsp_cuda_plan_create": (C.c_int, [C.POINTER(_VP), C.c_int]),
+    "rvsp_cuda_plan_destroy": (None, [_VP]),
+    "rvsp_cuda_plan_set_async": (C.c_int, [_VP, C.c_int]),
+    "rvsp_cuda_plan_stream": (_VP, [_VP]),
+    "rvsp_cuda_symbolic": (C.c_int, [_VP, _I32, _I32, _I32, _VP, _VP, _I32, _I32, _I32, _VP, _VP,
+                                     C.POINTER(_I64), C.POINTER(C.c_size_t)]),
+    "rvsp_cuda_numeric": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, C.c_int, _VP]),
+    "rvsp_cuda_op_counts": (C.c_int, [_VP, _VP, _I32]),
+    "rvsp_cuda_spgemm_f32": (C.c_int, [C.c_int, _I32, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP,
+                                       C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
+                                       C.POINTER(_I32), _VP]),
+    "rvsp_cuda_csr_check": (C.c_int, [_I32, _I32, _I32, _VP, _VP, C.POINTER(_I32)]),
+    "rvsp_cuda_csr_validate": (C.c_int, [_I32, _I32, _I32, _VP, _VP]),
+    "rvsp_cuda_launch_count": (_I64, []),
+}
+
+
+def build() -> None:
+    """Compile the library in-tree for sm_100a (make -C rv-sparse_b200)."""
+    subprocess.run(["make", "-s", "-j8", "-C", PKG_DIR], check=True)
+
+
+def lib():
+    """The loaded librvsp_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: run `make -C {PKG_DIR}`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _PROTOS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def status_string(st: int) -> str:
+    return lib().rvsp_status_to_string(st).decode()
+
+
+def last_error() -> str:
+    return lib().rvsp_cuda_last_error().decode()
+
+
+def device_count() -> int:
+    return lib().rvsp_cuda_device_count()
+
+
+def launch_count() -> int:
+    return lib().rvsp_cuda_launch_count()
+
+
+def ptr(a) -> int | None:
+    """Address of a numpy array or of a device tensor (data_ptr())."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data if a.size else _EMPTY.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return int(a)
+
+
+_EMPTY = np.zeros(4, np.int32)
+
+
+def check(st: int, what: str = "") -> None:
+    if st != RVSP_SUCCESS:
+        raise RvspError(st, what)
+
+
+def csr_struct(rows, cols, nnz, row_ptr, col_idx, values, dtype=RVSP_DTYPE_FP32) -> CsrMatrix:
+    M = CsrMatrix()
+    M.rows, M.cols, M.nnz = rows, cols, nnz
+    M.row_ptr, M.col_idx, M.values = ptr(row_ptr), ptr(col_idx), ptr(values)
+    M.dtype, M.format, M.owns_data = dtype, RVSP_FORMAT_CSR, 0
+    return M
+
+
+def from_csr(M) -> CsrMatrix:
+    """rvsp_csr_matrix_t view of an object with rows, cols, row_ptr, col_idx, values."""
+    return csr_struct(M.rows, M.cols, int(M.row_ptr[-1]) if isinstance(M.row_ptr, np.ndarray)
+                      else int(M.nnz), M.row_ptr, M.col_idx, M.values)
+
+
+def spgemm(A, B, backend=RVSP_BACKEND_CUDA):
+    """One-shot C = A * B on host numpy CSR through rvsp_spgemm_csr.
+
+    Returns (row_ptr, col_idx, values) as numpy arrays (copies); C is
+    released with rvsp_csr_destroy.
+    """
+    L = lib()
+    a, b = from_csr(A), from_csr(B)
+    c = CsrMatrix()
+    opts = SpgemmOptions(backend, RVSP_DTYPE_FP32, RVSP_DTYPE_FP32)
+    check(L.rvsp_spgemm_csr(C.byref(a), C.byref(b), C.byref(c), C.byref(opts)), "rvsp_spgemm_csr")
+    try:
+        n = c.nnz
+        rp = np.ctypeslib.as_array(C.cast(c.row_ptr, C.POINTER(C.c_int32)), (A.rows + 1,)).copy()
+        ci = (np.ctypeslib.as_array(C.cast(c.col_idx, C.POINTER(C.c_int32)), (n,)).copy()
+              if n else np.zeros(0, np.int32))
+        v = (np.ctypeslib.as_array(C.cast(c.values, C.POINTER(C.c_float)), (n,)).copy()
+             if n else np.zeros(0, np.float32))
+    finally:
+        L.rvsp_csr_destroy(C.byref(c))
+    return rp, ci, v
+
+
+class Descriptor:
+    """rvsp_spgemm_descr_t with its create / set_algo / estimate / compute cycle."""
+
+    def __init__(self, algo=RVSP_SPGEMM_ALGO_CUDA):
+        self.L = lib()
+        self.h = C.c_void_p()
+        check(self.L.rvsp_spgemm_descr_create(C.byref(self.h)), "descr_create")
+        if algo is not None:
+            check(self.L.rvsp_spgemm_set_algo(self.h, algo), "set_algo")
+
+    def close(self):
+        if self.h:
+            self.L.rvsp_spgemm_descr_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def work_estimation(self, a: CsrMatrix, b: CsrMatrix):
+        ws = C.c_size_t(0)
+        nnz = C.c_int32(0)
+        st = self.L.rvsp_spgemm_work_estimation(self.h, C.byref(a), C.byref(b), C.byref(ws),
+                                                C.byref(nnz))
+        return st, ws.value, nnz.value
+
+    def compute(self, a: CsrMatrix, b: CsrMatrix, c: CsrMatrix, ws) -> int:
+        return self.L.rvsp_spgemm_compute(self.h, C.byref(a), C.byref(b), C.byref(c), ptr(ws))
+
+    def op_counts(self, n):
+        out = np.zeros(max(n, 1), np.int64)
+        st = self.L.rvsp_spgemm_get_op_counts(self.h, out.ctypes.data, n)
+        return st, out[:n]
+
+    def invalidate(self):
+        self.L.rvsp_spgemm_invalidate_structure(self.h)

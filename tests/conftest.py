@@ -1,0 +1,93 @@
+"""Shared test setup: import paths, the gpu marker, golden fixtures.
+
+Tests marked ``gpu`` need a CUDA device and the built librvsp_b200.so; the
+rest run on CPU (oracle checks, host-side logic, symbol exports).
+"""
+
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "rv-sparse_b200"))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
+
+
+class Mat:
+    """Plain CSR holder for fixtures (rows, cols, row_ptr, col_idx, values)."""
+
+    def __init__(self, rows, cols, row_ptr, col_idx, values):
+        self.rows, self.cols = int(rows), int(cols)
+        self.row_ptr = np.ascontiguousarray(row_ptr, np.int32)
+        self.col_idx = np.ascontiguousarray(col_idx, np.int32)
+        self.values = np.ascontiguousarray(values, np.float32)
+
+    @property
+    def nnz(self):
+        return int(self.row_ptr[-1])
+
+
+def load_fixtures():
+    """The six hand-computed triples of rv-sparse tests/csr_fixtures.h."""
+    with open(os.path.join(GOLDEN, "csr_fixtures.json")) as f:
+        data = json.load(f)["pairs"]
+    out = []
+    for p in data:
+        mk = lambda d: Mat(d["rows"], d["cols"], d["row_ptr"], d["col_idx"], d["values"])  # noqa: E731
+        out.append((p["name"], mk(p["a"]), mk(p["b"]), mk(p["c"])))
+    return out
+
+
+def load_ref_cases():
+    """Seeded products with the reference scalar kernel's outputs."""
+    meta = json.load(open(os.path.join(GOLDEN, "ref_outputs.json")))
+    z = np.load(os.path.join(GOLDEN, "ref_outputs.npz"))
+    out = []
+    for name, info in meta["cases"].items():
+        A = Mat(info["a"][0], info["a"][1], z[f"{name}.a.row_ptr"], z[f"{name}.a.col_idx"],
+                z[f"{name}.a.values"])
+        B = Mat(info["b"][0], info["b"][1], z[f"{name}.b.row_ptr"], z[f"{name}.b.col_idx"],
+                z[f"{name}.b.values"])
+        Cc = (z[f"{name}.c.row_ptr"], z[f"{name}.c.col_idx"], z[f"{name}.c.values"])
+        out.append((name, A, B, Cc, z[f"{name}.ops"]))
+    return out
+
+
+def ref_digests():
+    return json.load(open(os.path.join(GOLDEN, "ref_outputs.json")))["digests"]
+
+
+@pytest.fixture(scope="session")
+def fixtures():
+    return load_fixtures()
+
+
+@pytest.fixture(scope="session")
+def ref_cases():
+    return load_ref_cases()
+
+
+def have_gpu():
+    try:
+        import rvsp_b200
+        return os.path.exists(rvsp_b200.LIB_PATH) and rvsp_b200.device_count() > 0
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="session")
+def gpu_lib():
+    import rvsp_b200
+    if not os.path.exists(rvsp_b200.LIB_PATH):
+        pytest.fail("librvsp_b200.so not built (make -C rv-sparse_b200)")
+    if rvsp_b200.device_count() == 0:
+        pytest.skip("no CUDA device")
+    return rvsp_b200
