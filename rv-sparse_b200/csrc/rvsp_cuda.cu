@@ -82,11 +82,23 @@ constexpr int heavy_warps() {
     return MODE == COUNT ? 8 : 2;
 }
 
+// warps per CTA of the map-replay reuse kernel (a float per slot)
+template <int CAP>
+constexpr int map_warps() {
+    constexpr int w = 65536 / (4 * CAP);
+    return w > 8 ? 8 : (w < 1 ? 1 : w);
+}
+
 template <int CAP, int MODE>
 static void set_warp_attr() {
     constexpr int W = warps_for<CAP, MODE>();
     cudaFuncSetAttribute(k_warp<CAP, W, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          W * warp_smem_bytes<CAP, MODE>());
+    if (MODE == REUSE) {
+        constexpr int WM = map_warps<CAP>();
+        cudaFuncSetAttribute(k_warp_reuse_map<CAP, WM>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, WM * 4 * CAP);
+    }
 }
 
 template <int MODE>
@@ -121,12 +133,23 @@ void note_launch(rvsp_cuda_plan* plan, int n) {
 }
 
 template <int CAP, int MODE>
-static void launch_warp(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B,
-                        const int32_t* rows, int n, const RowOut& o) {
-    constexpr int W = warps_for<CAP, MODE>();
-    const int grid = (n + W - 1) / W;
-    k_warp<CAP, W, MODE><<<grid, W * 32, W * warp_smem_bytes<CAP, MODE>(), plan->stream>>>(
-        A, B, rows, n, o.cnt, o.c_rp, o.c_ci, o.c_v, o.err);
+static void launch_warp(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, int b,
+                        const RowOut& o) {
+    const int n = plan->bin_count[b];
+    const int32_t* rows = plan->bin_rows.as<int32_t>() + plan->offs.off[b];
+    const int32_t* lo = plan->list_off.as<int32_t>() + plan->offs.off[b];
+    uint16_t* pm = plan->pm16.as<uint16_t>() + plan->pm16_base[b];
+    if (MODE == REUSE && o.maps) {
+        constexpr int WM = map_warps<CAP>();
+        k_warp_reuse_map<CAP, WM><<<(n + WM - 1) / WM, WM * 32, WM * 4 * CAP, plan->stream>>>(
+            A, B, rows, n, o.c_rp, o.c_v, lo, pm, o.err);
+    } else {
+        constexpr int W = warps_for<CAP, MODE>();
+        k_warp<CAP, W, MODE><<<(n + W - 1) / W, W * 32, W * warp_smem_bytes<CAP, MODE>(),
+                               plan->stream>>>(A, B, rows, n, o.cnt, o.c_rp, o.c_ci, o.c_v,
+                                               o.maps ? lo : nullptr, o.maps ? pm : nullptr,
+                                               o.err);
+    }
     note_launch(plan, 1);
 }
 
@@ -139,18 +162,25 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
         if (n == 0) continue;
         const int32_t* r = rows + plan->offs.off[b];
         if (b == BIN_TINY) {
-            k_tiny<MODE><<<(n + TINY_TPB - 1) / TINY_TPB, TINY_TPB, 0, plan->stream>>>(
-                A, B, r, n, o.cnt, o.c_rp, o.c_ci, o.c_v, o.err);
+            const int32_t* lo = plan->list_off.as<int32_t>() + plan->offs.off[b];
+            const int grid = (n + TINY_TPB - 1) / TINY_TPB;
+            if (MODE == REUSE && o.maps)
+                k_tiny_reuse_map<<<grid, TINY_TPB, 0, plan->stream>>>(
+                    A, B, r, n, o.c_rp, o.c_v, lo, plan->pm8.as<uint8_t>(), o.err);
+            else
+                k_tiny<MODE><<<grid, TINY_TPB, 0, plan->stream>>>(
+                    A, B, r, n, o.cnt, o.c_rp, o.c_ci, o.c_v, o.maps ? lo : nullptr,
+                    o.maps ? plan->pm8.as<uint8_t>() : nullptr, o.err);
             note_launch(plan, 1);
         } else if (b < BIN_HEAVY) {
             switch (WARP_CAP_MIN << (b - BIN_WARP0)) {
-                case 64: launch_warp<64, MODE>(plan, A, B, r, n, o); break;
-                case 128: launch_warp<128, MODE>(plan, A, B, r, n, o); break;
-                case 256: launch_warp<256, MODE>(plan, A, B, r, n, o); break;
-                case 512: launch_warp<512, MODE>(plan, A, B, r, n, o); break;
-                case 1024: launch_warp<1024, MODE>(plan, A, B, r, n, o); break;
-                case 2048: launch_warp<2048, MODE>(plan, A, B, r, n, o); break;
-                default: launch_warp<4096, MODE>(plan, A, B, r, n, o); break;
+                case 64: launch_warp<64, MODE>(plan, A, B, b, o); break;
+                case 128: launch_warp<128, MODE>(plan, A, B, b, o); break;
+                case 256: launch_warp<256, MODE>(plan, A, B, b, o); break;
+                case 512: launch_warp<512, MODE>(plan, A, B, b, o); break;
+                case 1024: launch_warp<1024, MODE>(plan, A, B, b, o); break;
+                case 2048: launch_warp<2048, MODE>(plan, A, B, b, o); break;
+                default: launch_warp<4096, MODE>(plan, A, B, b, o); break;
             }
         } else if (plan->n_items > 0) {
             constexpr int W = heavy_warps<MODE>();
@@ -261,16 +291,22 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     ENS(plan->c_rp, (M + 1) * 4);
     ENS(plan->bin_rows, M * 4);
     ENS(plan->misc, sizeof(Misc));
+    const int64_t tiles = (M + AN_TILE - 1) / AN_TILE;
+    ENS(plan->tile_hist, NUM_BINS * tiles * 4);
+    ENS(plan->tile_off, (NUM_BINS * tiles + 1) * 4);
     if (features) ENS(plan->feat, M * 16);
     Misc* misc = plan->misc.as<Misc>();
     if ((e = cudaMemsetAsync(misc, 0, sizeof(Misc), plan->stream)) != cudaSuccess)
         return fail(e, "memset");
     AnalyzeOut out{plan->ops.as<int64_t>(), plan->ub.as<int32_t>(), plan->bin.as<uint8_t>(),
                    plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
-                   features ? plan->feat.as<float4>() : nullptr, misc->hist, misc->totals,
-                   &misc->err};
-    k_analyze<<<(unsigned)((M + AN_TILE - 1) / AN_TILE), AN_TILE, 0, plan->stream>>>(A, B, out);
+                   features ? plan->feat.as<float4>() : nullptr, misc->hist,
+                   plan->tile_hist.as<int32_t>(), misc->totals, misc->bin_prod, &misc->err};
+    k_analyze<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(A, B, out);
     note_launch(plan, 1);
+    int st = scan_counts(plan, plan->tile_hist.as<int32_t>(), NUM_BINS * tiles, nullptr,
+                         plan->tile_off.as<int32_t>(), &misc->tile_total);
+    if (st) return st;
     if ((e = cudaMemcpyAsync(&plan->host_misc, misc, sizeof(Misc), cudaMemcpyDeviceToHost,
                              plan->stream)) != cudaSuccess)
         return fail(e, "histogram read");
@@ -283,7 +319,7 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     for (int b = 0; b < NUM_BINS; ++b) {
         plan->bin_count[b] = plan->host_misc.hist[b];
         plan->offs.off[b] = acc;
-        if (b != BIN_EMPTY) acc += plan->bin_count[b];
+        acc += plan->bin_count[b];
     }
     plan->n_items = (int32_t)plan->host_misc.totals[0];
     plan->products = plan->host_misc.totals[1];
@@ -291,9 +327,9 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     ENS(plan->item_cnt, (size_t)plan->n_items * 4);
     ENS(plan->item_scan, ((size_t)plan->n_items + 1) * 8);
 #undef ENS
-    k_bin_scatter<<<(unsigned)((M + 255) / 256), 256, 0, plan->stream>>>(
-        (int32_t)M, plan->bin.as<uint8_t>(), plan->chunk_lo.as<int32_t>(),
-        plan->nchunks.as<int32_t>(), plan->offs, misc->cursor, plan->bin_rows.as<int32_t>(),
+    k_bin_scatter<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(
+        (int32_t)M, plan->bin.as<uint8_t>(), plan->tile_off.as<int32_t>(),
+        plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(), plan->bin_rows.as<int32_t>(),
         &misc->item_cursor, plan->items.as<HeavyItem>());
     note_launch(plan, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "analysis launch");
@@ -307,7 +343,7 @@ int count_exact(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
     if ((e = cudaMemsetAsync(plan->cnt.p, 0, M * 4, plan->stream)) != cudaSuccess)
         return fail(e, "memset");
     Misc* misc = plan->misc.as<Misc>();
-    RowOut o{plan->cnt.as<int32_t>(), nullptr, nullptr, nullptr, &misc->err};
+    RowOut o{plan->cnt.as<int32_t>(), nullptr, nullptr, nullptr, &misc->err, false};
     run_rows(plan, COUNT, A, B, o);
     int st = scan_counts(plan, plan->cnt.as<int32_t>(), M, nullptr, plan->c_rp.as<int32_t>(),
                          &misc->scan_total);
@@ -334,6 +370,43 @@ int count_exact(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
     return RVSP_SUCCESS;
 }
 
+// Allocates the position maps and their offsets (an exclusive scan of the
+// per-row product counts in bin-list order) when the plan records them and
+// they fit: total products below 2^31 and map bytes within a quarter of the
+// device memory currently free. Returns whether the next FILL records them.
+bool prepare_maps(rvsp_cuda_plan* plan) {
+    plan->maps_ready = false;
+    if (!plan->map_policy || plan->products <= 0 || plan->products >= INT32_MAX) return false;
+    int64_t p8 = plan->host_misc.bin_prod[BIN_TINY], p16 = 0;
+    for (int b = BIN_WARP0; b < BIN_HEAVY; ++b) {
+        plan->pm16_base[b] = p16;
+        p16 += plan->host_misc.bin_prod[b];
+    }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const int64_t M = plan->a_rows;
+    const size_t need = (size_t)p8 + 2 * (size_t)p16 + 8 * (size_t)(M + 1);
+    if (need > free_b / 4) return false;
+    if (plan->pm8.ensure((size_t)p8) != cudaSuccess || plan->pm16.ensure(2 * (size_t)p16) != cudaSuccess ||
+        plan->list_ops.ensure(4 * (size_t)M) != cudaSuccess ||
+        plan->list_off.ensure(4 * (size_t)(M + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    Misc* misc = plan->misc.as<Misc>();
+    k_list_ops<<<(unsigned)((M + 255) / 256), 256, 0, plan->stream>>>(
+        plan->bin_rows.as<int32_t>(), (int32_t)M, plan->ops.as<int64_t>(),
+        plan->list_ops.as<int32_t>(), &misc->overflow);
+    note_launch(plan, 1);
+    if (scan_counts(plan, plan->list_ops.as<int32_t>(), M, nullptr, plan->list_off.as<int32_t>(),
+                    &misc->list_total) != RVSP_SUCCESS)
+        return false;
+    return cudaGetLastError() == cudaSuccess;
+}
+
 void reset_graph(rvsp_cuda_plan* plan) {
     if (plan->gexec) cudaGraphExecDestroy(plan->gexec);
     plan->gexec = nullptr;
@@ -355,7 +428,7 @@ int reuse_numeric(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, cons
             return fail(e, "begin capture");
         plan->capturing = true;
         RowOut o{nullptr, plan->c_rp.as<int32_t>(), const_cast<int32_t*>(c_ci), c_v,
-                 &plan->misc.as<Misc>()->err};
+                 &plan->misc.as<Misc>()->err, plan->maps_ready};
         run_rows(plan, REUSE, A, B, o);
         plan->capturing = false;
         e = cudaStreamEndCapture(plan->stream, &g);
@@ -433,7 +506,9 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
                       &p->ops, &p->ub, &p->bin, &p->chunk_lo, &p->nchunks, &p->feat,
                       &p->cnt, &p->c_rp, &p->bin_rows, &p->items, &p->item_cnt,
                       &p->item_scan, &p->scan_tmp, &p->misc, &p->s_cci, &p->s_cv,
-                      &p->pred_cap, &p->slot_off, &p->tmp_ci, &p->tmp_v, &p->row_flag};
+                      &p->pred_cap, &p->slot_off, &p->tmp_ci, &p->tmp_v, &p->row_flag,
+                      &p->tile_hist, &p->tile_off, &p->pm8, &p->pm16, &p->list_ops,
+                      &p->list_off};
     for (DevBuf* b : bufs) b->release();
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;
@@ -457,6 +532,7 @@ int rvsp_cuda_symbolic(rvsp_cuda_plan_t plan, int32_t a_rows, int32_t a_cols, in
         return RVSP_ERROR_INVALID_ARGUMENT;
     if (a_cols != b_rows) return RVSP_ERROR_INVALID_ARGUMENT;
     plan->analysed = false;
+    plan->maps_ready = false;
     plan->filled = nullptr;
     plan->filled_host = nullptr;
     reset_graph(plan);
@@ -509,8 +585,14 @@ int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t*
     }
     if (nnz > 0) {
         if (fill_structure) {
-            RowOut o{nullptr, plan->c_rp.as<int32_t>(), d_ci, d_v, &plan->misc.as<Misc>()->err};
+            const bool maps = prepare_maps(plan);
+            RowOut o{nullptr, plan->c_rp.as<int32_t>(), d_ci, d_v, &plan->misc.as<Misc>()->err,
+                     maps};
             run_rows(plan, FILL, A, B, o);
+            if (maps) {
+                plan->maps_ready = true;
+                reset_graph(plan);
+            }
             if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "fill launch");
             if (!dev_ci) {
                 if ((e = cudaMemcpyAsync(c_ci, d_ci, (size_t)nnz * 4, cudaMemcpyDeviceToHost,

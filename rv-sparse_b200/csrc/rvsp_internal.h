@@ -37,6 +37,9 @@ struct Misc {
     int64_t overflow_ub;       // learned path: sum of upper bounds of those rows
     int32_t err;               // ERR_* bits raised by kernels
     int32_t pad2;
+    int64_t bin_prod[NUM_BINS];  // products per bin
+    int64_t tile_total;        // scratch total of the tile-histogram scan
+    int64_t list_total;        // scratch total of the product-offset scan
 };
 
 // Output pointers of a row-kernel launch.
@@ -46,6 +49,7 @@ struct RowOut {
     int32_t* c_ci;
     float* c_v;
     int32_t* err;
+    bool maps;  // FILL: record position maps; REUSE: replay them
 };
 
 extern thread_local std::string g_err;
@@ -71,7 +75,7 @@ struct rvsp_cuda_plan {
     const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
 
     // analysed structure
-    rvsp::DevBuf ops, ub, bin, chunk_lo, nchunks, feat, cnt, c_rp, bin_rows;
+    rvsp::DevBuf ops, ub, bin, chunk_lo, nchunks, feat, cnt, c_rp, bin_rows, tile_hist, tile_off;
     rvsp::DevBuf items, item_cnt, item_scan, scan_tmp, misc;
     int32_t bin_count[rvsp::NUM_BINS] = {};
     rvsp::BinOffsets offs = {};
@@ -85,6 +89,14 @@ struct rvsp_cuda_plan {
     rvsp::DevBuf s_cci, s_cv;
     const int32_t* filled = nullptr;
     const int32_t* filled_host = nullptr;
+
+    // per-product output positions, recorded by the first fill and replayed by
+    // numeric-only reuse (uint8 for tiny rows, uint16 for warp-bin rows);
+    // list_off is the product offset of every entry of bin_rows
+    int map_policy = 1;   // 0: never record (one-shot plans)
+    bool maps_ready = false;
+    rvsp::DevBuf pm8, pm16, list_ops, list_off;
+    int64_t pm16_base[rvsp::NUM_BINS] = {};
 
     // learned path
     rvsp::DevBuf pred_cap, slot_off, tmp_ci, tmp_v, row_flag;

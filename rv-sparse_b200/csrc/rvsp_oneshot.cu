@@ -83,7 +83,10 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
     if ((st = read_i32(a_rp + a_rows, &a_nnz))) return st;
     if ((st = read_i32(b_rp + a_cols, &b_nnz))) return st;
     rvsp_cuda_plan_t& plan = t_plan[algo == RVSP_CUDA_ALGO_LEARNED ? 1 : 0];
-    if (!plan && (st = rvsp_cuda_plan_create(&plan, algo))) return st;
+    if (!plan) {
+        if ((st = rvsp_cuda_plan_create(&plan, algo))) return st;
+        plan->map_policy = 0;  // a one-shot product is never reused
+    }
     const bool dev = is_dev(a_rp);
     keep_pool_memory();
 

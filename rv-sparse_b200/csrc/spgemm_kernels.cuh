@@ -128,7 +128,6 @@ __device__ __forceinline__ void ordered_add(float* vals, int slot, bool active, 
     }
     if (lead) vals[slot] = acc;
 }
-
 // ---------------------------------------------------------------------------
 // Analysis: one CTA per tile of AN_TILE rows; threads stride over the tile's
 // A entries (a contiguous range of col_idx) so long rows are shared.
@@ -143,7 +142,9 @@ struct AnalyzeOut {
     int32_t* nchunks;    // [rows] heavy column chunks (0 for other bins)
     float4* feat;        // [rows] learned-model features (optional)
     int32_t* hist;       // [NUM_BINS] rows per bin
+    int32_t* tile_hist;  // [NUM_BINS][tiles] rows per bin per tile (stable binning)
     int64_t* totals;     // [0] heavy items, [1] products
+    int64_t* bin_prod;   // [NUM_BINS] products per bin
     int32_t* err;        // ERR_* bits
 };
 
@@ -154,6 +155,7 @@ __global__ void __launch_bounds__(AN_TILE) k_analyze(CsrView A, CsrView B, Analy
     __shared__ int32_t s_minc[AN_TILE];
     __shared__ int32_t s_maxc[AN_TILE];
     __shared__ int32_t s_hist[NUM_BINS];
+    __shared__ unsigned long long s_bprod[NUM_BINS];
     __shared__ unsigned long long s_items, s_prod;
 
     const int r0 = blockIdx.x * AN_TILE;
@@ -166,7 +168,10 @@ __global__ void __launch_bounds__(AN_TILE) k_analyze(CsrView A, CsrView B, Analy
         s_minc[i] = INT_MAX;
         s_maxc[i] = -1;
     }
-    if (t < NUM_BINS) s_hist[t] = 0;
+    if (t < NUM_BINS) {
+        s_hist[t] = 0;
+        s_bprod[t] = 0;
+    }
     if (t == 0) {
         s_items = 0;
         s_prod = 0;
@@ -219,34 +224,45 @@ __global__ void __launch_bounds__(AN_TILE) k_analyze(CsrView A, CsrView B, Analy
             out.feat[row] = make_float4((float)anz, (float)ops, (float)s_maxlen[i], (float)span);
         }
         atomicAdd(&s_hist[b], 1);
+        atomicAdd(&s_bprod[b], (unsigned long long)ops);
         atomicAdd(&s_prod, (unsigned long long)ops);
     }
     __syncthreads();
-    if (t < NUM_BINS && s_hist[t]) atomicAdd(&out.hist[t], s_hist[t]);
+    if (t < NUM_BINS) {
+        out.tile_hist[t * gridDim.x + blockIdx.x] = s_hist[t];
+        if (s_hist[t]) atomicAdd(&out.hist[t], s_hist[t]);
+        if (s_bprod[t]) atomicAdd((unsigned long long*)&out.bin_prod[t], s_bprod[t]);
+    }
     if (t == 0) {
         if (s_items) atomicAdd((unsigned long long*)&out.totals[0], s_items);
         atomicAdd((unsigned long long*)&out.totals[1], s_prod);
     }
 }
 
-// Rows grouped by bin (order within a bin is arbitrary; rows are
-// independent). Heavy rows reserve a block of consecutive work items.
-__global__ void k_bin_scatter(int32_t rows, const uint8_t* __restrict__ bin,
-                              const int32_t* __restrict__ chunk_lo,
-                              const int32_t* __restrict__ nchunks, BinOffsets offs,
-                              int32_t* __restrict__ cursor, int32_t* __restrict__ bin_rows,
-                              int32_t* __restrict__ item_cursor, HeavyItem* __restrict__ items) {
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = lane_id();
-    const int b = row < rows ? (int)bin[row] : -1;
+// Stable partition of rows by bin: tile_off[b * tiles + tile] is where the
+// tile's rows of bin b start in bin_rows (an exclusive scan of tile_hist), so
+// every bin lists its rows in ascending order. Heavy rows reserve a block of
+// consecutive work items.
+__global__ void __launch_bounds__(AN_TILE)
+    k_bin_scatter(int32_t rows, const uint8_t* __restrict__ bin,
+                  const int32_t* __restrict__ tile_off, const int32_t* __restrict__ chunk_lo,
+                  const int32_t* __restrict__ nchunks, int32_t* __restrict__ bin_rows,
+                  int32_t* __restrict__ item_cursor, HeavyItem* __restrict__ items) {
+    __shared__ int32_t s_wc[AN_TILE / 32][NUM_BINS];
+    const int t = threadIdx.x, lane = lane_id(), warp = t >> 5;
+    const int row = blockIdx.x * AN_TILE + t;
+    const int b = row < rows ? (int)bin[row] : NUM_BINS;
+    for (int i = t; i < (AN_TILE / 32) * NUM_BINS; i += blockDim.x) (&s_wc[0][0])[i] = 0;
+    __syncthreads();
     const unsigned peers = __match_any_sync(FULL, b);
-    const int leader = __ffs(peers) - 1;
-    int base = 0;
-    if (lane == leader && b > BIN_EMPTY) base = atomicAdd(&cursor[b], __popc(peers));
-    base = __shfl_sync(FULL, base, leader);
-    if (b <= BIN_EMPTY) return;
-    const int rank = __popc(peers & ((1u << lane) - 1));
-    bin_rows[offs.off[b] + base + rank] = row;
+    if (b < NUM_BINS && lane == __ffs(peers) - 1) s_wc[warp][b] = __popc(peers);
+    __syncthreads();
+    if (b >= NUM_BINS) return;
+    int before = 0;
+    for (int w = 0; w < warp; ++w) before += s_wc[w][b];
+    const int pos = tile_off[b * gridDim.x + blockIdx.x] + before +
+                    __popc(peers & ((1u << lane) - 1));
+    bin_rows[pos] = row;
     if (b == BIN_HEAVY) {
         const int n = nchunks[row];
         const int first = atomicAdd(item_cursor, n);
@@ -255,81 +271,150 @@ __global__ void k_bin_scatter(int32_t rows, const uint8_t* __restrict__ bin,
     }
 }
 
+// Per-row product counts in bin-list order (int32; rows beyond INT32_MAX
+// products flag *overflow), the input of the position-map offsets.
+__global__ void k_list_ops(const int32_t* __restrict__ bin_rows, int32_t n,
+                           const int64_t* __restrict__ ops, int32_t* __restrict__ out,
+                           int32_t* __restrict__ overflow) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t v = ops[bin_rows[i]];
+    if (v > INT32_MAX) atomicExch(overflow, 1);
+    out[i] = (int32_t)min(v, (int64_t)INT32_MAX);
+}
+
 // ---------------------------------------------------------------------------
 // Tiny rows (ops <= 32): one thread per row, the reference loop verbatim.
-// Per-thread scratch is interleaved (element x of thread t at x*TPB + t) so
-// lanes touching the same element index never share a bank.
+// Per-thread scratch is interleaved with a padded stride (element x of thread
+// t at x*TINY_LD + t): threads touching the same element never share a bank,
+// and neither do lanes reading one thread's elements during the coalesced
+// write-out, where each warp stores its 32 rows one row at a time.
+//
+// FILL mode can also record, for every product in reference order, the
+// position of its column within the output row (pm, one byte per product;
+// rows start at list_off[i] - list_off[0]), which the reuse kernel replays.
 // ---------------------------------------------------------------------------
 constexpr int TINY_TPB = 128;
+constexpr int TINY_LD = TINY_TPB + 1;
 
 template <int MODE>
 __global__ void __launch_bounds__(TINY_TPB)
     k_tiny(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
            int32_t* __restrict__ cnt, const int32_t* __restrict__ c_rp,
-           int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err) {
-    __shared__ int32_t s_col[TINY_CAP * TINY_TPB];
-    __shared__ float s_val[(MODE == COUNT ? 1 : TINY_CAP) * TINY_TPB];
-    const int t = threadIdx.x;
+           int32_t* __restrict__ c_ci, float* __restrict__ c_v,
+           const int32_t* __restrict__ list_off, uint8_t* __restrict__ pm,
+           int32_t* __restrict__ err) {
+    __shared__ int32_t s_col[TINY_CAP * TINY_LD];
+    __shared__ float s_val[(MODE == COUNT ? 1 : TINY_CAP) * TINY_LD];
+    const int t = threadIdx.x, lane = lane_id(), wbase = t & ~31;
     const int i = blockIdx.x * TINY_TPB + t;
-    if (i >= nrows) return;
-    const int row = rows[i];
-#define COL(x) s_col[(x) * TINY_TPB + t]
-#define VAL(x) s_val[(x) * TINY_TPB + t]
-    int a0, a1;
-    row_range(A, row, &a0, &a1, err);
-    int n = 0;
-    if (MODE == REUSE) {
-        const int c0 = c_rp[row];
-        n = min(c_rp[row + 1] - c0, TINY_CAP);
-        for (int x = 0; x < n; ++x) COL(x) = c_ci[c0 + x];
-    } else {
-        for (int p = a0; p < a1; ++p) {
-            int q0, q1;
-            row_range(B, A.ci[p], &q0, &q1, err);
-            for (int q = q0; q < q1 && n < TINY_CAP; ++q) COL(n++) = B.ci[q];
-        }
-        for (int x = 1; x < n; ++x) {  // insertion sort
-            const int key = COL(x);
-            int y = x - 1;
-            while (y >= 0 && COL(y) > key) {
-                COL(y + 1) = COL(y);
-                --y;
+    const bool live = i < nrows;
+#define COL(x) s_col[(x) * TINY_LD + t]
+#define VAL(x) s_val[(x) * TINY_LD + t]
+    int row = 0, n = 0, c0 = 0;
+    if (live) {
+        row = rows[i];
+        int a0, a1;
+        row_range(A, row, &a0, &a1, err);
+        if (MODE == REUSE) {
+            c0 = c_rp[row];
+            n = min(c_rp[row + 1] - c0, TINY_CAP);
+            for (int x = 0; x < n; ++x) COL(x) = c_ci[c0 + x];
+        } else {
+            for (int p = a0; p < a1; ++p) {
+                int q0, q1;
+                row_range(B, A.ci[p], &q0, &q1, err);
+                for (int q = q0; q < q1 && n < TINY_CAP; ++q) COL(n++) = B.ci[q];
             }
-            COL(y + 1) = key;
+            for (int x = 1; x < n; ++x) {  // insertion sort
+                const int key = COL(x);
+                int y = x - 1;
+                while (y >= 0 && COL(y) > key) {
+                    COL(y + 1) = COL(y);
+                    --y;
+                }
+                COL(y + 1) = key;
+            }
+            int m = 0;  // unique
+            for (int x = 0; x < n; ++x) {
+                const int c = COL(x);
+                if (m == 0 || COL(m - 1) != c) COL(m++) = c;
+            }
+            n = m;
+            if (MODE == COUNT) cnt[row] = n;
+            else c0 = c_rp[row];
         }
-        int m = 0;  // unique
-        for (int x = 0; x < n; ++x) {
-            const int c = COL(x);
-            if (m == 0 || COL(m - 1) != c) COL(m++) = c;
+        if (MODE != COUNT) {
+            uint8_t* pp = pm ? pm + (list_off[i] - list_off[0]) : nullptr;
+            for (int x = 0; x < n; ++x) VAL(x) = 0.0f;
+            for (int p = a0; p < a1; ++p) {
+                const float a = A.v[p];
+                int q0, q1;
+                row_range(B, A.ci[p], &q0, &q1, err);
+                for (int q = q0; q < q1; ++q) {
+                    const int col = B.ci[q];
+                    int pos = 0, step = 16;
+                    for (; step > 0; step >>= 1)
+                        if (pos + step <= n && COL(pos + step - 1) < col) pos += step;
+                    if (pp) *pp++ = (uint8_t)pos;
+                    if (pos < n) VAL(pos) = __fadd_rn(VAL(pos), __fmul_rn(a, B.v[q]));
+                }
+            }
         }
-        n = m;
-        if (MODE == COUNT) {
-            cnt[row] = n;
-            return;
-        }
-        const int c0 = c_rp[row];
-        for (int x = 0; x < n; ++x) c_ci[c0 + x] = COL(x);
     }
-    if constexpr (MODE != COUNT) {
-        for (int x = 0; x < n; ++x) VAL(x) = 0.0f;
+    if (MODE == COUNT) return;
+    __syncwarp();
+    for (int j = 0; j < 32; ++j) {  // coalesced write-out, one row per step
+        const int cj = __shfl_sync(FULL, c0, j);
+        const int nj = __shfl_sync(FULL, n, j);
+        if (lane < nj) {
+            if (MODE == FILL) c_ci[cj + lane] = s_col[lane * TINY_LD + wbase + j];
+            c_v[cj + lane] = s_val[lane * TINY_LD + wbase + j];
+        }
+    }
+#undef COL
+#undef VAL
+}
+
+// Reuse with a position map: the numeric loop of the reference with the
+// output position of every product read from pm instead of searched for.
+// Neither B's nor C's column indices are read.
+__global__ void __launch_bounds__(TINY_TPB)
+    k_tiny_reuse_map(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
+                     const int32_t* __restrict__ c_rp, float* __restrict__ c_v,
+                     const int32_t* __restrict__ list_off, const uint8_t* __restrict__ pm,
+                     int32_t* __restrict__ err) {
+    __shared__ float s_val[TINY_CAP * TINY_LD];
+    const int t = threadIdx.x, lane = lane_id(), wbase = t & ~31;
+    const int i = blockIdx.x * TINY_TPB + t;
+    int n = 0, c0 = 0;
+    if (i < nrows) {
+        const int row = rows[i];
+        c0 = c_rp[row];
+        n = min(c_rp[row + 1] - c0, TINY_CAP);
+        for (int x = 0; x < n; ++x) s_val[x * TINY_LD + t] = 0.0f;
+        int a0, a1;
+        row_range(A, row, &a0, &a1, err);
+        const uint8_t* pp = pm + (list_off[i] - list_off[0]);
         for (int p = a0; p < a1; ++p) {
             const float a = A.v[p];
             int q0, q1;
             row_range(B, A.ci[p], &q0, &q1, err);
             for (int q = q0; q < q1; ++q) {
-                const int col = B.ci[q];
-                int pos = 0, step = 1;
-                while ((step << 1) <= n) step <<= 1;
-                for (; step > 0; step >>= 1)
-                    if (pos + step <= n && COL(pos + step - 1) < col) pos += step;
-                if (pos < n) VAL(pos) = __fadd_rn(VAL(pos), __fmul_rn(a, B.v[q]));
+                const int x = *pp++;
+                if (x < n) {
+                    float* s = &s_val[x * TINY_LD + t];
+                    *s = __fadd_rn(*s, __fmul_rn(a, B.v[q]));
+                }
             }
         }
-        const int c0 = c_rp[row];
-        for (int x = 0; x < n; ++x) c_v[c0 + x] = VAL(x);
     }
-#undef COL
-#undef VAL
+    __syncwarp();
+    for (int j = 0; j < 32; ++j) {
+        const int cj = __shfl_sync(FULL, c0, j);
+        const int nj = __shfl_sync(FULL, n, j);
+        if (lane < nj) c_v[cj + lane] = s_val[lane * TINY_LD + wbase + j];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -337,17 +422,43 @@ __global__ void __launch_bounds__(TINY_TPB)
 // The row's products are processed 32 at a time in flattened
 // (A entry, B entry) order; each lane locates its A entry with a 5-step
 // search over the warp's inclusive scan of B-row lengths.
+// FILL mode can record each product's output position (pm, uint16, rows
+// starting at list_off[w] - list_off[0]) for the reuse kernel.
 // ---------------------------------------------------------------------------
 template <int CAP, int MODE>
 __host__ __device__ constexpr int warp_smem_bytes() {
     return (MODE == COUNT ? 4 : 8) * CAP;
 }
 
+// Lane's product p of the current 32-entry A chunk: its B position and the
+// A value. incl is the warp's inclusive scan of the chunk's B-row lengths.
+struct ProductRef {
+    int q;
+    float a;
+};
+
+__device__ __forceinline__ ProductRef locate_product(int p, int incl, int bl, int bs, float av) {
+    int e = 0;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const int cand = __shfl_sync(FULL, incl, e + s - 1);
+        if (cand <= p) e += s;
+    }
+    e = min(e, 31);
+    const int e_incl = __shfl_sync(FULL, incl, e);
+    const int e_bl = __shfl_sync(FULL, bl, e);
+    const int e_bs = __shfl_sync(FULL, bs, e);
+    const float e_av = __shfl_sync(FULL, av, e);
+    return ProductRef{e_bs + (p - (e_incl - e_bl)), e_av};
+}
+
 template <int CAP, int WARPS, int MODE>
 __global__ void __launch_bounds__(WARPS * 32)
     k_warp(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
            int32_t* __restrict__ cnt, const int32_t* __restrict__ c_rp,
-           int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err) {
+           int32_t* __restrict__ c_ci, float* __restrict__ c_v,
+           const int32_t* __restrict__ list_off, uint16_t* __restrict__ pm,
+           int32_t* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int LOG2CAP = __builtin_ctz(CAP);
     const int warp = threadIdx.x >> 5, lane = lane_id();
@@ -390,23 +501,12 @@ __global__ void __launch_bounds__(WARPS * 32)
             for (int f = 0; f < total; f += 32) {
                 const int p = f + lane;
                 const bool pv = p < total;
-                int e = 0;
-#pragma unroll
-                for (int s = 16; s >= 1; s >>= 1) {
-                    const int cand = __shfl_sync(FULL, incl, e + s - 1);
-                    if (cand <= p) e += s;
-                }
-                e = min(e, 31);
-                const int e_incl = __shfl_sync(FULL, incl, e);
-                const int e_bl = __shfl_sync(FULL, bl, e);
-                const int e_bs = __shfl_sync(FULL, bs, e);
-                const float e_av = __shfl_sync(FULL, av, e);
+                const ProductRef pr = locate_product(p, incl, bl, bs, av);
                 int col = -1;
                 float bv = 0.0f;
                 if (pv) {
-                    const int q = e_bs + (p - (e_incl - e_bl));
-                    col = B.ci[q];
-                    if (MODE != COUNT) bv = B.v[q];
+                    col = B.ci[pr.q];
+                    if (MODE != COUNT) bv = B.v[pr.q];
                 }
                 int slot = -1;
                 bool ok = pv;
@@ -443,7 +543,7 @@ __global__ void __launch_bounds__(WARPS * 32)
                     }
                     count += __popc(__ballot_sync(FULL, inserted));
                 }
-                if (MODE != COUNT) ordered_add(vals, slot, ok, __fmul_rn(e_av, bv));
+                if (MODE != COUNT) ordered_add(vals, slot, ok, __fmul_rn(pr.a, bv));
                 __syncwarp();
             }
         }
@@ -498,7 +598,81 @@ __global__ void __launch_bounds__(WARPS * 32)
                 c_ci[o + x] = keys[x];
                 c_v[o + x] = vals[x];
             }
+            if (pm) {  // second walk: position of every product in the sorted row
+                uint16_t* pp = pm + (list_off[w] - list_off[0]);
+                for (int base = a0; base < a1; base += 32) {
+                    const int j = base + lane;
+                    int bs = 0, bl = 0;
+                    if (j < a1) {
+                        int be;
+                        row_range(B, A.ci[j], &bs, &be, err);
+                        bl = be - bs;
+                    }
+                    const int incl = warp_incl_scan(bl);
+                    const int total = __shfl_sync(FULL, incl, 31);
+                    for (int f = 0; f < total; f += 32) {
+                        const int p = f + lane;
+                        const ProductRef pr = locate_product(p, incl, bl, bs, 0.0f);
+                        if (p < total) pp[p] = (uint16_t)smem_lower_bound(keys, n, B.ci[pr.q]);
+                    }
+                    pp += total;
+                }
+            }
         }
+        __syncwarp();
+    }
+}
+
+// Reuse with a position map: like REUSE, but every product's slot comes
+// from pm, so B's and C's column indices are not read and no search runs.
+template <int CAP, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32)
+    k_warp_reuse_map(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
+                     const int32_t* __restrict__ c_rp, float* __restrict__ c_v,
+                     const int32_t* __restrict__ list_off, const uint16_t* __restrict__ pm,
+                     int32_t* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    float* vals = reinterpret_cast<float*>(smem) + warp * CAP;
+    for (int w = blockIdx.x * WARPS + warp; w < nrows; w += gridDim.x * WARPS) {
+        const int row = rows[w];
+        const int c0 = c_rp[row];
+        const int L = min(c_rp[row + 1] - c0, CAP);
+        for (int x = lane; x < L; x += 32) vals[x] = 0.0f;
+        __syncwarp();
+        const uint16_t* pp = pm + (list_off[w] - list_off[0]);
+        int a0, a1;
+        row_range(A, row, &a0, &a1, err);
+        for (int base = a0; base < a1; base += 32) {
+            const int j = base + lane;
+            int bs = 0, bl = 0;
+            float av = 0.0f;
+            if (j < a1) {
+                int be;
+                row_range(B, A.ci[j], &bs, &be, err);
+                bl = be - bs;
+                av = A.v[j];
+            }
+            const int incl = warp_incl_scan(bl);
+            const int total = __shfl_sync(FULL, incl, 31);
+            for (int f = 0; f < total; f += 32) {
+                const int p = f + lane;
+                const bool pv = p < total;
+                const ProductRef pr = locate_product(p, incl, bl, bs, av);
+                int slot = -1;
+                float bv = 0.0f;
+                if (pv) {
+                    slot = pp[p];
+                    bv = B.v[pr.q];
+                }
+                const bool ok = pv && slot < L;
+                ordered_add(vals, slot, ok, __fmul_rn(pr.a, bv));
+                __syncwarp();
+            }
+            pp += total;
+        }
+        __syncwarp();
+        for (int x = lane; x < L; x += 32) c_v[c0 + x] = vals[x];
         __syncwarp();
     }
 }

@@ -313,3 +313,46 @@ def test_launch_counter_advances(gpu_lib):
     A = gen.uniform_fixed(128, 128, 8, seed=9)
     oneshot(A, A)
     assert rv.launch_count() > before
+
+
+@pytest.mark.parametrize("device", [True, False])
+def test_descriptor_reuse_all_bins(gpu_lib, device):
+    """Reuse across tiny, warp-table and heavy rows: the position maps recorded
+    by the first fill replay bit-exactly with new values in A and B."""
+    A, B = _bin_sweep_matrix(7)
+    rng = np.random.default_rng(11)
+    d = rv.Descriptor(rv.RVSP_SPGEMM_ALGO_CUDA)
+    av, bvals = A.values.copy(), B.values.copy()
+    if device:
+        dA, dB = DevCSR(A), DevCSR(B)
+        a, b = dA.struct(), dB.struct()
+    else:
+        a = rv.csr_struct(A.rows, A.cols, A.nnz, A.row_ptr, A.col_idx, av)
+        b = rv.csr_struct(B.rows, B.cols, B.nnz, B.row_ptr, B.col_idx, bvals)
+    st, ws, nnz = d.work_estimation(a, b)
+    rv.check(st)
+    wrp, wci, _ = oracle.spgemm_f32(A, B)
+    if device:
+        crp, cci, cv = dev(np.zeros(A.rows + 1, np.int32)), dev(np.zeros(nnz, np.int32)), \
+            dev(np.zeros(nnz, np.float32))
+    else:
+        crp, cci, cv = np.zeros(A.rows + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz, np.float32)
+    c = rv.csr_struct(A.rows, B.cols, nnz, crp, cci, cv)
+    wsb = np.zeros(max(ws, 4), np.uint8)
+    for rep in range(3):
+        na = (A.values * rng.uniform(0.5, 1.5, A.nnz)).astype(np.float32)
+        nb = (B.values * rng.uniform(0.5, 1.5, B.nnz)).astype(np.float32)
+        if device:
+            dA.values.copy_(dev(na))
+            dB.values.copy_(dev(nb))
+        else:
+            av[:] = na
+            bvals[:] = nb
+        rv.check(d.compute(a, b, c, wsb), f"compute {rep}")
+        want = oracle.numeric_f32(Mat(A.rows, A.cols, A.row_ptr, A.col_idx, na),
+                                  Mat(B.rows, B.cols, B.row_ptr, B.col_idx, nb), wrp, wci)
+        got_v = cv.cpu().numpy() if device else cv
+        got_ci = cci.cpu().numpy() if device else cci
+        assert np.array_equal(got_ci, wci)
+        assert np.array_equal(bits(got_v), bits(want)), rep
+    d.close()
