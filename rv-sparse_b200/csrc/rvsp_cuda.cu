@@ -165,8 +165,9 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
             const int32_t* lo = plan->list_off.as<int32_t>() + plan->offs.off[b];
             const int grid = (n + TINY_TPB - 1) / TINY_TPB;
             if (MODE == REUSE && o.maps)
-                k_tiny_reuse_map<<<grid, TINY_TPB, 0, plan->stream>>>(
-                    A, B, r, n, o.c_rp, o.c_v, lo, plan->pm8.as<uint8_t>(), o.err);
+                k_tiny_reuse_map<<<(n + 32 * TRM_WARPS - 1) / (32 * TRM_WARPS), 32 * TRM_WARPS, 0,
+                                   plan->stream>>>(A, B, r, n, o.c_rp, o.c_v, lo,
+                                                   plan->pm8.as<uint8_t>(), o.err);
             else
                 k_tiny<MODE><<<grid, TINY_TPB, 0, plan->stream>>>(
                     A, B, r, n, o.cnt, o.c_rp, o.c_ci, o.c_v, o.maps ? lo : nullptr,

@@ -379,41 +379,112 @@ __global__ void __launch_bounds__(TINY_TPB)
 // Reuse with a position map: the numeric loop of the reference with the
 // output position of every product read from pm instead of searched for.
 // Neither B's nor C's column indices are read.
-__global__ void __launch_bounds__(TINY_TPB)
+//
+// One thread per row, as in the reference loop, organised so each thread
+// keeps many independent loads in flight: A entries are taken 8 at a time
+// (their column indices, values and B-row ranges loaded as two batches), and
+// each B row's values and positions are loaded 8 at a time before they are
+// accumulated. Values accumulate in a per-warp buffer laid out in C order, so
+// a warp whose 32 rows are consecutive writes C back as one contiguous range.
+// (Staging the warp's map bytes and A entries in shared memory first halves
+// the L1 sectors but costs more in instructions and occupancy than it saves.)
+constexpr int TRM_WARPS = 4;
+constexpr int TRM_CCAP = 32 * TINY_CAP;  // C entries of one warp's rows
+
+__global__ void __launch_bounds__(TRM_WARPS * 32)
     k_tiny_reuse_map(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
                      const int32_t* __restrict__ c_rp, float* __restrict__ c_v,
                      const int32_t* __restrict__ list_off, const uint8_t* __restrict__ pm,
                      int32_t* __restrict__ err) {
-    __shared__ float s_val[TINY_CAP * TINY_LD];
-    const int t = threadIdx.x, lane = lane_id(), wbase = t & ~31;
-    const int i = blockIdx.x * TINY_TPB + t;
-    int n = 0, c0 = 0;
-    if (i < nrows) {
-        const int row = rows[i];
+    __shared__ float s_acc[TRM_WARPS][TRM_CCAP];
+    const int w = threadIdx.x >> 5, lane = lane_id();
+    const int i = (blockIdx.x * TRM_WARPS + w) * 32 + lane;
+    if ((blockIdx.x * TRM_WARPS + w) * 32 >= nrows) return;  // whole warp idle
+    const bool live = i < nrows;
+    int row = -1, c0 = 0, c1 = 0, a0 = 0, a1 = 0, pb = 0;
+    if (live) {
+        row = rows[i];
         c0 = c_rp[row];
-        n = min(c_rp[row + 1] - c0, TINY_CAP);
-        for (int x = 0; x < n; ++x) s_val[x * TINY_LD + t] = 0.0f;
-        int a0, a1;
+        c1 = c_rp[row + 1];
         row_range(A, row, &a0, &a1, err);
-        const uint8_t* pp = pm + (list_off[i] - list_off[0]);
-        for (int p = a0; p < a1; ++p) {
-            const float a = A.v[p];
-            int q0, q1;
-            row_range(B, A.ci[p], &q0, &q1, err);
-            for (int q = q0; q < q1; ++q) {
-                const int x = *pp++;
-                if (x < n) {
-                    float* s = &s_val[x * TINY_LD + t];
-                    *s = __fadd_rn(*s, __fmul_rn(a, B.v[q]));
+        pb = list_off[i] - list_off[0];
+    }
+    const int n = min(c1 - c0, TINY_CAP);
+    const int last = __popc(__ballot_sync(FULL, live)) - 1;  // live lanes are a prefix
+    const int row_first = __shfl_sync(FULL, row, 0), row_last = __shfl_sync(FULL, row, last);
+    const int cbase = __shfl_sync(FULL, c0, 0), cend = __shfl_sync(FULL, c1, last);
+    const bool contig = row_last - row_first == last && cend - cbase <= TRM_CCAP;
+    int coff, ctotal;
+    if (contig) {
+        coff = c0 - cbase;
+        ctotal = cend - cbase;
+    } else {
+        const int incl = warp_incl_scan(n);
+        coff = incl - n;
+        ctotal = __shfl_sync(FULL, incl, 31);
+    }
+    float* acc = s_acc[w];
+    for (int e = lane; e < ctotal; e += 32) acc[e] = 0.0f;
+    __syncwarp();
+    if (live) {
+        const uint8_t* sp = pm + pb;
+        float* mine = acc + coff;
+        for (int p0 = a0; p0 < a1; p0 += 8) {
+            int k[8];
+            float a[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                k[u] = p0 + u < a1 ? A.ci[p0 + u] : -1;
+                a[u] = p0 + u < a1 ? A.v[p0 + u] : 0.0f;
+            }
+            int q0[8], q1[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                q0[u] = q1[u] = 0;
+                if (p0 + u < a1) {
+                    if ((unsigned)k[u] < (unsigned)B.rows) {
+                        q0[u] = B.rp[k[u]];
+                        q1[u] = B.rp[k[u] + 1];
+                    } else {
+                        atomicOr(err, ERR_STRUCTURE);
+                    }
                 }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (q0[u] < 0 || q1[u] < q0[u] || q1[u] > B.nnz) {
+                    atomicOr(err, ERR_STRUCTURE);
+                    q1[u] = q0[u] = 0;
+                }
+                const float* src = B.v + q0[u];
+                const int len = q1[u] - q0[u];
+                for (int m0 = 0; m0 < len; m0 += 8) {
+                    float v[8];
+                    int x[8];
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const bool in = m0 + t < len;
+                        v[t] = in ? __ldg(src + m0 + t) : 0.0f;
+                        x[t] = in ? (int)__ldg(sp + m0 + t) : TINY_CAP;
+                    }
+#pragma unroll
+                    for (int t = 0; t < 8; ++t)
+                        if (x[t] < n) mine[x[t]] = __fadd_rn(mine[x[t]], __fmul_rn(a[u], v[t]));
+                }
+                sp += len;
             }
         }
     }
     __syncwarp();
-    for (int j = 0; j < 32; ++j) {
-        const int cj = __shfl_sync(FULL, c0, j);
-        const int nj = __shfl_sync(FULL, n, j);
-        if (lane < nj) c_v[cj + lane] = s_val[lane * TINY_LD + wbase + j];
+    if (contig) {
+        for (int e = lane; e < ctotal; e += 32) c_v[cbase + e] = acc[e];
+    } else {
+        for (int j = 0; j <= last; ++j) {
+            const int cj = __shfl_sync(FULL, c0, j);
+            const int nj = __shfl_sync(FULL, n, j);
+            const int oj = __shfl_sync(FULL, coff, j);
+            if (lane < nj) c_v[cj + lane] = acc[oj + lane];
+        }
     }
 }
 
