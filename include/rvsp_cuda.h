@@ -144,6 +144,62 @@ RVSP_CUDA_API int rvsp_cuda_csr_check(int32_t rows, int32_t cols, int32_t nnz,
 RVSP_CUDA_API int rvsp_cuda_csr_validate(int32_t rows, int32_t cols, int32_t nnz,
                            const int32_t *row_ptr, const int32_t *col_idx);
 
+/* ------------------------------------------------------------------------
+ * Learned row-size predictor (no counterpart in the reference).
+ *
+ * A 4-32-32-2 MLP over per-row features (A-row nnz, sum and max of the
+ * referenced B-row lengths, column span) predicts each output row's nnz; the
+ * learned path (RVSP_CUDA_ALGO_LEARNED) sizes hash tables and output slots
+ * from it, sweeps the products once, and re-runs rows that outgrow their
+ * prediction on the exact kernels, so results stay bit-identical.
+ * A model is the float vector [mean(4), inv_std(4), z, params(1282)]
+ * (RVSP_CUDA_MLP_FLOATS floats); a checkpoint file holds it with a magic,
+ * version and checksum. The default checkpoint is $RVSP_MLP_WEIGHTS or
+ * weights/row_mlp_v1.bin beside the library's directory.
+ * ------------------------------------------------------------------------ */
+#define RVSP_CUDA_MLP_PARAMS 1282
+#define RVSP_CUDA_MLP_FLOATS 1291
+
+/* 1 when a model is loaded (the default checkpoint is tried once). */
+RVSP_CUDA_API int rvsp_cuda_learned_available(void);
+RVSP_CUDA_API int rvsp_cuda_mlp_load(const char *path);
+RVSP_CUDA_API int rvsp_cuda_mlp_set(const float *model, int32_t nfloats);
+RVSP_CUDA_API int rvsp_cuda_mlp_get(float *model_out, int32_t nfloats);
+RVSP_CUDA_API int rvsp_cuda_mlp_save(const char *path, const float *model, int32_t nfloats);
+
+/* Mean loss and its gradient over n samples on the GPU (the training
+ * kernel's forward/backward pass, one batch). X is [n][4] normalised
+ * features, y = log2(1 + nnz), w optional per-sample weights. */
+RVSP_CUDA_API int rvsp_cuda_mlp_grad(const float *params, const float *X, const float *y,
+                                     const float *w, int32_t n, float *loss_out,
+                                     float *grad_out);
+
+/* Adam training on the GPU, params updated in place (host arrays).
+ * epoch_loss_out (optional) gets the mean batch loss of every epoch. */
+RVSP_CUDA_API int rvsp_cuda_mlp_train(float *params, const float *X, const float *y,
+                                      const float *w, int32_t n, int32_t epochs, int32_t batch,
+                                      float lr, uint64_t seed, float *epoch_loss_out);
+
+/* Inference kernel on raw features [n][4]: mu, sigma and the capacity
+ * ceil(2^(mu + z sigma) - 1) clamped to [1, ub] (0 when ub <= 0). */
+RVSP_CUDA_API int rvsp_cuda_mlp_infer(const float *model, int32_t nfloats, const float *feat,
+                                      const int32_t *ub, int32_t n, float *mu_out,
+                                      float *sigma_out, int32_t *cap_out);
+
+/* Analysis of this plan also records the per-row model features. */
+RVSP_CUDA_API int rvsp_cuda_plan_collect_features(rvsp_cuda_plan_t plan, int on);
+
+/* Per-row features [n][4], exact output counts and upper bounds
+ * min(products, cols(B)) of the last analysis (any pointer may be NULL). */
+RVSP_CUDA_API int rvsp_cuda_plan_row_stats(rvsp_cuda_plan_t plan, float *feat_out,
+                                           int32_t *cnt_out, int32_t *ub_out, int32_t n);
+
+/* Learned-path statistics of the last analysis: [0] rows sized by the
+ * prediction, [1] of those, rows that outgrew it, [2] rows too large for a
+ * table (exact path), [3] sum of the counts and [4] sum of the capacities of
+ * predicted rows that fit, [5] rows finished by the exact path. */
+RVSP_CUDA_API int rvsp_cuda_plan_learned_stats(rvsp_cuda_plan_t plan, int64_t *out, int32_t n);
+
 /* Number of kernels this library has launched in this process (graph
  * replays count each kernel node), for launch accounting in benchmarks. */
 RVSP_CUDA_API int64_t rvsp_cuda_launch_count(void);

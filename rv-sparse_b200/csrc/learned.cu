@@ -1,0 +1,418 @@
+// Learned-capacity SpGEMM path (RVSP_CUDA_ALGO_LEARNED).
+//
+// The exact path sweeps every product twice: once to count each row's
+// distinct columns into tables sized by the row's upper bound
+// ub = min(products, cols(B)), once to fill. Here the row-size predictor
+// (mlp.cuh) sizes each row instead, and one fused sweep fills C:
+//
+//   analysis       k_analyze with features; k_mlp_infer on rows whose bound
+//                  exceeds the tiny bin; k_learned_bins assigns each row a
+//                  capacity (tiny rows: their product count, exact; others:
+//                  the prediction) and a hash-table class, stable-partitioned
+//   fused fill     the FILL kernels write every row's sorted columns and
+//                  values into its slot of an over-allocated buffer and record
+//                  its count; a row whose table fills up or whose count passes
+//                  its capacity is flagged (count -1) instead
+//   exact re-run   flagged rows and rows too large for a table (k_need) are
+//                  counted by the exact kernels under a row mask
+//   C              scan of all counts -> row pointer; flagged rows are filled
+//                  in place by the exact FILL kernels, the rest are copied from
+//                  their slots (k_compact)
+//
+// Every row is computed by the same order-preserving kernels as the exact
+// path, so the result is bit-identical to it; a misprediction costs time,
+// never accuracy. The plan records how many rows were predicted, how many
+// overflowed, and how full the slots were.
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "mlp.cuh"
+#include "rv_sparse_types.h"
+#include "rvsp_cuda.h"
+#include "rvsp_internal.h"
+#include "spgemm_types.cuh"
+
+namespace rvsp {
+
+bool current_model(MlpModel* out);
+void launch_mlp_infer(const MlpModel& m, const float4* feat, const int32_t* ub, const uint8_t* bin,
+                      int32_t n, int32_t* cap, cudaStream_t st);
+
+constexpr int LBIN_EXACT = BIN_HEAVY;  // predicted bin of rows left to the exact path
+
+struct LearnedBinsOut {
+    uint8_t* lbin;
+    int32_t* lcap;
+    int32_t* tile_hist;  // [NUM_BINS][tiles]
+    int32_t* hist;       // [NUM_BINS]
+    int64_t* slot_total;
+};
+
+__global__ void __launch_bounds__(AN_TILE)
+    k_learned_bins(int32_t rows, const uint8_t* __restrict__ bin, const int64_t* __restrict__ ops,
+                   const int32_t* __restrict__ cap_pred, LearnedBinsOut out) {
+    __shared__ int32_t s_hist[NUM_BINS];
+    __shared__ unsigned long long s_slots;
+    const int t = threadIdx.x;
+    if (t < NUM_BINS) s_hist[t] = 0;
+    if (t == 0) s_slots = 0;
+    __syncthreads();
+    const int row = blockIdx.x * AN_TILE + t;
+    if (row < rows) {
+        const int b = bin[row];
+        int lb, cap;
+        if (b == BIN_EMPTY) {
+            lb = BIN_EMPTY;
+            cap = 0;
+        } else if (b == BIN_TINY) {
+            lb = BIN_TINY;
+            cap = (int)ops[row];
+        } else {
+            const int c = max(cap_pred[row], 1);
+            const int64_t need = (int64_t)c + (c >> 2);
+            int tcap = WARP_CAP_MIN;
+            lb = BIN_WARP0;
+            while (tcap < need && lb < BIN_HEAVY) {
+                tcap <<= 1;
+                ++lb;
+            }
+            cap = lb == BIN_HEAVY ? 0 : c;  // BIN_HEAVY here means LBIN_EXACT
+        }
+        out.lbin[row] = (uint8_t)lb;
+        out.lcap[row] = cap;
+        atomicAdd(&s_hist[lb], 1);
+        if (cap) atomicAdd(&s_slots, (unsigned long long)cap);
+    }
+    __syncthreads();
+    if (t < NUM_BINS) {
+        out.tile_hist[t * gridDim.x + blockIdx.x] = s_hist[t];
+        if (s_hist[t]) atomicAdd(&out.hist[t], s_hist[t]);
+    }
+    if (t == 0 && s_slots) atomicAdd((unsigned long long*)out.slot_total, s_slots);
+}
+
+// Rows the fused sweep could not finish: predicted too large for a table, or
+// overflowed. Their counts are reset for the exact count kernels.
+// stats: [0] predicted rows that overflowed, [1] rows exact by size,
+//        [2] sum of counts of predicted rows that fit, [3] their capacity
+__global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
+                       const int32_t* __restrict__ lcap, int32_t* __restrict__ cnt,
+                       uint8_t* __restrict__ need, int32_t* __restrict__ n_need,
+                       int64_t* __restrict__ stats) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    bool nd = false, ovf = false, big = false;
+    int64_t fitc = 0, fitcap = 0;
+    if (row < rows) {
+        const int lb = lbin[row];
+        big = lb == LBIN_EXACT;
+        ovf = lb >= BIN_WARP0 && lb < LBIN_EXACT && cnt[row] < 0;
+        nd = big || ovf;
+        if (lb >= BIN_WARP0 && lb < LBIN_EXACT && !ovf) {
+            fitc = cnt[row];
+            fitcap = lcap[row];
+        }
+        need[row] = nd ? 1 : 0;
+        if (nd) cnt[row] = 0;
+    }
+    const unsigned mn = __ballot_sync(FULL, nd), mo = __ballot_sync(FULL, ovf),
+                   mb = __ballot_sync(FULL, big);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        fitc += __shfl_xor_sync(FULL, fitc, o);
+        fitcap += __shfl_xor_sync(FULL, fitcap, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (mn) atomicAdd(n_need, __popc(mn));
+        if (mo) atomicAdd((unsigned long long*)&stats[0], (unsigned long long)__popc(mo));
+        if (mb) atomicAdd((unsigned long long*)&stats[1], (unsigned long long)__popc(mb));
+        if (fitc) atomicAdd((unsigned long long*)&stats[2], (unsigned long long)fitc);
+        if (fitcap) atomicAdd((unsigned long long*)&stats[3], (unsigned long long)fitcap);
+    }
+}
+
+// Copy finished rows from their slots into C, G lanes per row.
+template <int G>
+__global__ void k_compact(const int32_t* __restrict__ rows, int32_t n,
+                          const uint8_t* __restrict__ need, const int32_t* __restrict__ cnt,
+                          const int64_t* __restrict__ slot_off, const int32_t* __restrict__ c_rp,
+                          const int32_t* __restrict__ tmp_ci, const float* __restrict__ tmp_v,
+                          int32_t* __restrict__ c_ci, float* __restrict__ c_v) {
+    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t grp = gid / G;
+    const int sub = (int)(gid % G);
+    if (grp >= n) return;
+    const int row = rows[grp];
+    if (need[row]) return;
+    const int k = cnt[row];
+    const int64_t src = slot_off[row];
+    const int dst = c_rp[row];
+    for (int x = sub; x < k; x += G) {
+        c_ci[dst + x] = tmp_ci[src + x];
+        c_v[dst + x] = tmp_v[src + x];
+    }
+}
+
+// Enqueued by analyze() before its host synchronisation: prediction and
+// predicted-capacity bins, so one round trip returns both histograms.
+static int learned_pre_sync(rvsp_cuda_plan* plan) {
+    MlpModel model;
+    if (!current_model(&model)) {
+        g_err = "no row-size model loaded";
+        return RVSP_ERROR_UNSUPPORTED_BACKEND;
+    }
+    const int64_t M = plan->a_rows;
+    const int64_t tiles = (M + AN_TILE - 1) / AN_TILE;
+    cudaError_t e;
+#define ENS(buf, bytes) \
+    if ((e = (buf).ensure(bytes)) != cudaSuccess) return fail(e, "learned alloc " #buf)
+    ENS(plan->pred_cap, M * 4);
+    ENS(plan->lbin, M);
+    ENS(plan->lcap, M * 4);
+    ENS(plan->ltile_hist, NUM_BINS * tiles * 4);
+    ENS(plan->ltile_off, (NUM_BINS * tiles + 1) * 4);
+    ENS(plan->lbin_rows, M * 4);
+    ENS(plan->need, M);
+    ENS(plan->row_flag, M);
+#undef ENS
+    Misc* misc = plan->misc.as<Misc>();
+    launch_mlp_infer(model, plan->feat.as<float4>(), plan->ub.as<int32_t>(), plan->bin.as<uint8_t>(),
+                     (int32_t)M, plan->pred_cap.as<int32_t>(), plan->stream);
+    note_launch(plan, 1);
+    LearnedBinsOut lo{plan->lbin.as<uint8_t>(), plan->lcap.as<int32_t>(),
+                      plan->ltile_hist.as<int32_t>(), misc->lhist, &misc->slot_total};
+    k_learned_bins<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(
+        (int32_t)M, plan->bin.as<uint8_t>(), plan->ops.as<int64_t>(), plan->pred_cap.as<int32_t>(),
+        lo);
+    note_launch(plan, 1);
+    return scan_counts(plan, plan->ltile_hist.as<int32_t>(), NUM_BINS * tiles, nullptr,
+                       plan->ltile_off.as<int32_t>(), &misc->ltile_total);
+}
+
+// Learned analysis, one sweep over the predicted-capacity bins, exact counts
+// of the rows that sweep could not finish. On return the plan holds the exact
+// row pointer of C (plan->c_rp, plan->c_nnz) and the mask of rows finished by
+// the exact path (plan->need). With fused, the sweep is the FILL kernels and
+// every other row's columns and values wait in its slot (tmp_ci / tmp_v at
+// slot_off) for learned_finish; without, the sweep is the COUNT kernels with
+// tables sized by the prediction (the descriptor's structure analysis).
+int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool fused) {
+    int st = analyze(plan, A, B, true, learned_pre_sync);
+    if (st) return st;
+    const int64_t M = plan->a_rows;
+    Misc* misc = plan->misc.as<Misc>();
+    int32_t acc = 0;
+    for (int b = 0; b < NUM_BINS; ++b) {
+        plan->lcount[b] = plan->host_misc.lhist[b];
+        plan->loffs.off[b] = acc;
+        acc += plan->lcount[b];
+    }
+    plan->slot_total = plan->host_misc.slot_total;
+    cudaError_t e;
+    size_t free_b = 0, total_b = 0;
+    if ((e = cudaMemGetInfo(&free_b, &total_b)) != cudaSuccess) return fail(e, "mem info");
+    if (fused) {
+        if ((size_t)plan->slot_total * 8 > free_b / 2) {
+            g_err = "predicted capacity exceeds the memory budget";
+            return RVSP_ERROR_ALLOCATION_FAILED;
+        }
+        if ((e = plan->slot_off.ensure(((size_t)M + 1) * 8)) != cudaSuccess)
+            return fail(e, "slots");
+        if ((e = plan->tmp_ci.ensure((size_t)plan->slot_total * 4)) != cudaSuccess)
+            return fail(e, "slots");
+        if ((e = plan->tmp_v.ensure((size_t)plan->slot_total * 4)) != cudaSuccess)
+            return fail(e, "slots");
+    }
+    launch_bin_scatter(plan, plan->lbin.as<uint8_t>(), plan->ltile_off.as<int32_t>(),
+                       plan->lbin_rows.as<int32_t>(), false);
+    if (fused && (st = scan_counts(plan, plan->lcap.as<int32_t>(), M, plan->slot_off.as<int64_t>(),
+                                   nullptr, &misc->scan_total2)))
+        return st;
+    if ((e = cudaMemsetAsync(plan->cnt.p, 0, M * 4, plan->stream)) != cudaSuccess)
+        return fail(e, "memset");
+    if (plan->n_items > 0 &&
+        (e = cudaMemsetAsync(plan->item_cnt.p, 0, (size_t)plan->n_items * 4, plan->stream)) !=
+            cudaSuccess)
+        return fail(e, "memset");
+    // one sweep over the predicted-capacity bins
+    RowOut fo{plan->cnt.as<int32_t>(), nullptr, plan->tmp_ci.as<int32_t>(), plan->tmp_v.as<float>(),
+              &misc->err, false};
+    fo.ctl.slot_off = fused ? plan->slot_off.as<int64_t>() : nullptr;
+    fo.ctl.learned = 1;
+    fo.learned_bins = true;
+    run_rows(plan, fused ? FILL : COUNT, A, B, fo);
+    k_need<<<(unsigned)((M + 255) / 256), 256, 0, plan->stream>>>(
+        (int32_t)M, plan->lbin.as<uint8_t>(), plan->lcap.as<int32_t>(), plan->cnt.as<int32_t>(),
+        plan->need.as<uint8_t>(), &misc->n_need, misc->lstats);
+    note_launch(plan, 1);
+    // exact counts of the rows the sweep could not finish (tiny rows never overflow)
+    RowOut co{plan->cnt.as<int32_t>(), nullptr, nullptr, nullptr, &misc->err, false};
+    co.ctl.only = plan->need.as<uint8_t>();
+    const int32_t tiny = plan->bin_count[BIN_TINY];
+    plan->bin_count[BIN_TINY] = 0;
+    run_rows(plan, COUNT, A, B, co);
+    plan->bin_count[BIN_TINY] = tiny;
+    if ((st = scan_counts(plan, plan->cnt.as<int32_t>(), M, nullptr, plan->c_rp.as<int32_t>(),
+                          &misc->scan_total)))
+        return st;
+    if (plan->n_items > 0 &&
+        (st = scan_counts(plan, plan->item_cnt.as<int32_t>(), plan->n_items,
+                          plan->item_scan.as<int64_t>(), nullptr, &misc->tile_total)))
+        return st;
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "learned launch");
+    if ((e = cudaMemcpyAsync(&plan->host_misc, misc, sizeof(Misc), cudaMemcpyDeviceToHost,
+                             plan->stream)) != cudaSuccess)
+        return fail(e, "learned read");
+    if ((e = cudaStreamSynchronize(plan->stream)) != cudaSuccess) return fail(e, "learned sweep");
+    if (plan->host_misc.err) {
+        g_err = "operand structure out of range (row_ptr or col_idx)";
+        return RVSP_ERROR_INVALID_CSR;
+    }
+    if (plan->host_misc.overflow || plan->host_misc.scan_total > INT32_MAX) {
+        g_err = "nnz(C) exceeds INT32_MAX";
+        return RVSP_ERROR_ALLOCATION_FAILED;
+    }
+    plan->c_nnz = plan->host_misc.scan_total;
+    // heavy rows sized by the prediction were never counted by column chunk
+    plan->items_counted = plan->n_items == 0 || fused;
+    int64_t predicted = 0;
+    for (int b = BIN_WARP0; b < LBIN_EXACT; ++b) predicted += plan->lcount[b];
+    plan->lstats[0] = predicted;
+    plan->lstats[1] = plan->host_misc.lstats[0];
+    plan->lstats[2] = plan->host_misc.lstats[1];
+    plan->lstats[3] = plan->host_misc.lstats[2];
+    plan->lstats[4] = plan->host_misc.lstats[3];
+    plan->lstats[5] = plan->host_misc.n_need;
+    return RVSP_SUCCESS;
+}
+
+// C from the learned sweep: exact fill of the masked rows in place, copy of
+// the rest from their slots. c_ci / c_v are device arrays of nnz entries.
+int learned_finish(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, int32_t* c_ci,
+                   float* c_v) {
+    Misc* misc = plan->misc.as<Misc>();
+    if (plan->host_misc.n_need > 0) {
+        RowOut fo{nullptr, plan->c_rp.as<int32_t>(), c_ci, c_v, &misc->err, false};
+        fo.ctl.only = plan->need.as<uint8_t>();
+        const int32_t tiny = plan->bin_count[BIN_TINY];
+        plan->bin_count[BIN_TINY] = 0;
+        run_rows(plan, FILL, A, B, fo);
+        plan->bin_count[BIN_TINY] = tiny;
+    }
+    const int32_t* lrows = plan->lbin_rows.as<int32_t>();
+    const int32_t nt = plan->lcount[BIN_TINY];
+    if (nt > 0) {
+        k_compact<8><<<(unsigned)(((int64_t)nt * 8 + 255) / 256), 256, 0, plan->stream>>>(
+            lrows + plan->loffs.off[BIN_TINY], nt, plan->need.as<uint8_t>(), plan->cnt.as<int32_t>(),
+            plan->slot_off.as<int64_t>(), plan->c_rp.as<int32_t>(), plan->tmp_ci.as<int32_t>(),
+            plan->tmp_v.as<float>(), c_ci, c_v);
+        note_launch(plan, 1);
+    }
+    int32_t nw = 0;
+    for (int b = BIN_WARP0; b < LBIN_EXACT; ++b) nw += plan->lcount[b];
+    if (nw > 0) {
+        k_compact<32><<<(unsigned)(((int64_t)nw * 32 + 255) / 256), 256, 0, plan->stream>>>(
+            lrows + plan->loffs.off[BIN_WARP0], nw, plan->need.as<uint8_t>(),
+            plan->cnt.as<int32_t>(), plan->slot_off.as<int64_t>(), plan->c_rp.as<int32_t>(),
+            plan->tmp_ci.as<int32_t>(), plan->tmp_v.as<float>(), c_ci, c_v);
+        note_launch(plan, 1);
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? RVSP_SUCCESS : fail(e, "learned finish");
+}
+
+// Product through the learned path; C arrays allocated like rvsp_cuda_spgemm_f32.
+int learned_spgemm(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t a_nnz,
+                   const int32_t* a_rp, const int32_t* a_ci, const float* a_v, int32_t b_rows,
+                   int32_t b_cols, int32_t b_nnz, const int32_t* b_rp, const int32_t* b_ci,
+                   const float* b_v, int device_out, int32_t** c_rp_out, int32_t** c_ci_out,
+                   float** c_v_out, int32_t* c_nnz_out) {
+    plan->analysed = false;
+    plan->maps_ready = false;
+    plan->filled_host = nullptr;
+    reset_graph(plan);
+    plan->a_rows = a_rows;
+    plan->a_cols = a_cols;
+    plan->a_nnz = a_nnz;
+    plan->b_rows = b_rows;
+    plan->b_cols = b_cols;
+    plan->b_nnz = b_nnz;
+    memset(plan->key, 0, sizeof(plan->key));
+    CsrView A, B;
+    int st = stage_operands(plan, a_rp, a_ci, a_v, b_rp, b_ci, b_v, false, &A, &B);
+    if (st) return st;
+    if ((st = learned_symbolic(plan, A, B, true))) return st;
+    plan->analysed = true;
+    const int64_t nnz = plan->c_nnz;
+    const size_t alloc = nnz > 0 ? (size_t)nnz : 1;
+    int32_t *rp = nullptr, *ci = nullptr;
+    float* v = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&rp, ((size_t)a_rows + 1) * 4, plan->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&ci, alloc * 4, plan->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&v, alloc * 4, plan->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(rp, plan->c_rp.p, ((size_t)a_rows + 1) * 4, cudaMemcpyDeviceToDevice,
+                            plan->stream);
+    if (e == cudaSuccess && nnz > 0) {
+        st = learned_finish(plan, A, B, ci, v);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && st == RVSP_SUCCESS) e = cudaStreamSynchronize(plan->stream);
+    if (e != cudaSuccess || st) {
+        cudaFree(rp);
+        cudaFree(ci);
+        cudaFree(v);
+        return st ? st : fail(e, "learned product");
+    }
+    if (!device_out) {  // host inputs: hand back malloc'd host arrays
+        int32_t* hrp = (int32_t*)malloc(((size_t)a_rows + 1) * 4);
+        int32_t* hci = (int32_t*)malloc(alloc * 4);
+        float* hv = (float*)malloc(alloc * 4);
+        if (!hrp || !hci || !hv) {
+            free(hrp);
+            free(hci);
+            free(hv);
+            cudaFree(rp);
+            cudaFree(ci);
+            cudaFree(v);
+            return RVSP_ERROR_ALLOCATION_FAILED;
+        }
+        e = cudaMemcpy(hrp, rp, ((size_t)a_rows + 1) * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(hci, ci, (size_t)nnz * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(hv, v, (size_t)nnz * 4, cudaMemcpyDeviceToHost);
+        cudaFree(rp);
+        cudaFree(ci);
+        cudaFree(v);
+        if (e != cudaSuccess) {
+            free(hrp);
+            free(hci);
+            free(hv);
+            return fail(e, "learned copy-out");
+        }
+        rp = hrp;
+        ci = hci;
+        v = hv;
+    }
+    *c_rp_out = rp;
+    *c_ci_out = ci;
+    *c_v_out = v;
+    *c_nnz_out = (int32_t)nnz;
+    return RVSP_SUCCESS;
+}
+
+}  // namespace rvsp
+
+using namespace rvsp;
+
+extern "C" {
+
+int rvsp_cuda_plan_learned_stats(rvsp_cuda_plan_t plan, int64_t* out, int32_t n) {
+    if (!plan || !out) return RVSP_ERROR_NULL_POINTER;
+    if (n < 6) return RVSP_ERROR_INVALID_ARGUMENT;
+    if (plan->algo != RVSP_CUDA_ALGO_LEARNED || !plan->analysed) return RVSP_ERROR_INVALID_ARGUMENT;
+    memcpy(out, plan->lstats, sizeof(plan->lstats));
+    return RVSP_SUCCESS;
+}
+
+}  // extern "C"

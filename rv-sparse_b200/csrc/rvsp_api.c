@@ -235,7 +235,10 @@ static int algo_available(rvsp_spgemm_algo_t algo)
 {
     if (algo != RVSP_SPGEMM_ALGO_CUDA && algo != RVSP_SPGEMM_ALGO_CUDA_LEARNED)
         return 0;
-    return rvsp_cuda_device_count() > 0;
+    if (rvsp_cuda_device_count() == 0)
+        return 0;
+    /* the learned strategy needs a row-size model (the shipped checkpoint) */
+    return algo != RVSP_SPGEMM_ALGO_CUDA_LEARNED || rvsp_cuda_learned_available();
 }
 
 rvsp_status_t rvsp_spgemm_descr_create(rvsp_spgemm_descr_t *descr)

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "rv_sparse_types.h"
 #include "rvsp_cuda.h"
@@ -135,8 +136,9 @@ void note_launch(rvsp_cuda_plan* plan, int n) {
 template <int CAP, int MODE>
 static void launch_warp(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, int b,
                         const RowOut& o) {
-    const int n = plan->bin_count[b];
-    const int32_t* rows = plan->bin_rows.as<int32_t>() + plan->offs.off[b];
+    const int n = o.learned_bins ? plan->lcount[b] : plan->bin_count[b];
+    const int32_t* rows = o.learned_bins ? plan->lbin_rows.as<int32_t>() + plan->loffs.off[b]
+                                         : plan->bin_rows.as<int32_t>() + plan->offs.off[b];
     const int32_t* lo = plan->list_off.as<int32_t>() + plan->offs.off[b];
     uint16_t* pm = plan->pm16.as<uint16_t>() + plan->pm16_base[b];
     if (MODE == REUSE && o.maps) {
@@ -148,7 +150,7 @@ static void launch_warp(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
         k_warp<CAP, W, MODE><<<(n + W - 1) / W, W * 32, W * warp_smem_bytes<CAP, MODE>(),
                                plan->stream>>>(A, B, rows, n, o.cnt, o.c_rp, o.c_ci, o.c_v,
                                                o.maps ? lo : nullptr, o.maps ? pm : nullptr,
-                                               o.err);
+                                               o.err, o.ctl);
     }
     note_launch(plan, 1);
 }
@@ -156,11 +158,12 @@ static void launch_warp(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
 template <int MODE>
 static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B,
                         const RowOut& o) {
-    const int32_t* rows = plan->bin_rows.as<int32_t>();
+    const int32_t* rows = o.learned_bins ? plan->lbin_rows.as<int32_t>() : plan->bin_rows.as<int32_t>();
     for (int b = BIN_TINY; b < NUM_BINS; ++b) {
-        const int n = plan->bin_count[b];
+        const int n = o.learned_bins ? plan->lcount[b] : plan->bin_count[b];
         if (n == 0) continue;
-        const int32_t* r = rows + plan->offs.off[b];
+        if (o.learned_bins && b == BIN_HEAVY) continue;  // left to the exact path
+        const int32_t* r = rows + (o.learned_bins ? plan->loffs.off[b] : plan->offs.off[b]);
         if (b == BIN_TINY) {
             const int32_t* lo = plan->list_off.as<int32_t>() + plan->offs.off[b];
             const int grid = (n + TINY_TPB - 1) / TINY_TPB;
@@ -171,7 +174,7 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
             else
                 k_tiny<MODE><<<grid, TINY_TPB, 0, plan->stream>>>(
                     A, B, r, n, o.cnt, o.c_rp, o.c_ci, o.c_v, o.maps ? lo : nullptr,
-                    o.maps ? plan->pm8.as<uint8_t>() : nullptr, o.err);
+                    o.maps ? plan->pm8.as<uint8_t>() : nullptr, o.err, o.ctl);
             note_launch(plan, 1);
         } else if (b < BIN_HEAVY) {
             switch (WARP_CAP_MIN << (b - BIN_WARP0)) {
@@ -188,7 +191,7 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
             const int grid = (plan->n_items + W - 1) / W;
             k_heavy<W, MODE><<<grid, W * 32, W * heavy_smem_bytes<MODE>(), plan->stream>>>(
                 A, B, plan->items.as<HeavyItem>(), plan->n_items, plan->item_cnt.as<int32_t>(),
-                o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err);
+                o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, o.ctl);
             note_launch(plan, 1);
         }
     }
@@ -278,7 +281,8 @@ int stage_operands(rvsp_cuda_plan* plan, const int32_t* a_rp, const int32_t* a_c
 
 // Analysis + binning. Leaves per-row op counts, bins and heavy items in the
 // plan; one device->host read of the bin histogram.
-int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool features) {
+int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool features,
+            int (*pre_sync)(rvsp_cuda_plan*)) {
     const int64_t M = plan->a_rows;
     cudaError_t e;
 #define ENS(buf, bytes)                                        \
@@ -308,6 +312,7 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     int st = scan_counts(plan, plan->tile_hist.as<int32_t>(), NUM_BINS * tiles, nullptr,
                          plan->tile_off.as<int32_t>(), &misc->tile_total);
     if (st) return st;
+    if (pre_sync && (st = pre_sync(plan))) return st;
     if ((e = cudaMemcpyAsync(&plan->host_misc, misc, sizeof(Misc), cudaMemcpyDeviceToHost,
                              plan->stream)) != cudaSuccess)
         return fail(e, "histogram read");
@@ -328,13 +333,22 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     ENS(plan->item_cnt, (size_t)plan->n_items * 4);
     ENS(plan->item_scan, ((size_t)plan->n_items + 1) * 8);
 #undef ENS
-    k_bin_scatter<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(
-        (int32_t)M, plan->bin.as<uint8_t>(), plan->tile_off.as<int32_t>(),
-        plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(), plan->bin_rows.as<int32_t>(),
-        &misc->item_cursor, plan->items.as<HeavyItem>());
-    note_launch(plan, 1);
+    launch_bin_scatter(plan, plan->bin.as<uint8_t>(), plan->tile_off.as<int32_t>(),
+                       plan->bin_rows.as<int32_t>(), true);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "analysis launch");
     return RVSP_SUCCESS;
+}
+
+// Stable partition of the plan's rows by bin (k_bin_scatter); with
+// heavy_items the heavy rows also get their column-chunk work items.
+void launch_bin_scatter(rvsp_cuda_plan* plan, const uint8_t* bin, const int32_t* tile_off,
+                        int32_t* bin_rows, bool heavy_items) {
+    const int64_t M = plan->a_rows;
+    Misc* misc = plan->misc.as<Misc>();
+    k_bin_scatter<<<(unsigned)((M + AN_TILE - 1) / AN_TILE), AN_TILE, 0, plan->stream>>>(
+        (int32_t)M, bin, tile_off, plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
+        bin_rows, &misc->item_cursor, heavy_items ? plan->items.as<HeavyItem>() : nullptr);
+    note_launch(plan, 1);
 }
 
 // Exact count + scan: C's row pointer in plan->c_rp, nnz in plan->c_nnz.
@@ -354,6 +368,7 @@ int count_exact(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
                          plan->item_scan.as<int64_t>(), nullptr, &misc->scan_total2);
         if (st) return st;
     }
+    plan->items_counted = true;
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "count launch");
     if ((e = cudaMemcpyAsync(&plan->host_misc, misc, sizeof(Misc), cudaMemcpyDeviceToHost,
                              plan->stream)) != cudaSuccess)
@@ -509,7 +524,8 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
                       &p->item_scan, &p->scan_tmp, &p->misc, &p->s_cci, &p->s_cv,
                       &p->pred_cap, &p->slot_off, &p->tmp_ci, &p->tmp_v, &p->row_flag,
                       &p->tile_hist, &p->tile_off, &p->pm8, &p->pm16, &p->list_ops,
-                      &p->list_off};
+                      &p->list_off, &p->lbin, &p->lcap, &p->ltile_hist, &p->ltile_off,
+                      &p->lbin_rows, &p->need};
     for (DevBuf* b : bufs) b->release();
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;
@@ -547,8 +563,12 @@ int rvsp_cuda_symbolic(rvsp_cuda_plan_t plan, int32_t a_rows, int32_t a_cols, in
     CsrView A, B;
     int st = stage_operands(plan, a_rp, a_ci, nullptr, b_rp, b_ci, nullptr, false, &A, &B);
     if (st) return st;
-    if ((st = analyze(plan, A, B, plan->algo == RVSP_CUDA_ALGO_LEARNED))) return st;
-    if ((st = count_exact(plan, A, B))) return st;
+    if (plan->algo == RVSP_CUDA_ALGO_LEARNED) {
+        if ((st = learned_symbolic(plan, A, B, false))) return st;
+    } else {
+        if ((st = analyze(plan, A, B, plan->features))) return st;
+        if ((st = count_exact(plan, A, B))) return st;
+    }
     plan->analysed = true;
     *c_nnz_out = plan->c_nnz;
     *ws_bytes_out = 256;
@@ -586,6 +606,26 @@ int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t*
     }
     if (nnz > 0) {
         if (fill_structure) {
+            if (!plan->items_counted && plan->n_items > 0) {
+                // heavy rows the learned analysis sized by prediction: count
+                // their column chunks now so the chunk fills know their offsets
+                k_heavy_uncounted<<<(unsigned)((M + 255) / 256), 256, 0, plan->stream>>>(
+                    (int32_t)M, plan->bin.as<uint8_t>(), plan->need.as<uint8_t>(),
+                    plan->row_flag.as<uint8_t>());
+                RowOut ho{nullptr, nullptr, nullptr, nullptr, &plan->misc.as<Misc>()->err, false};
+                ho.ctl.only = plan->row_flag.as<uint8_t>();
+                const int32_t saved[NUM_BINS - 1] = {};
+                int32_t keep[NUM_BINS];
+                memcpy(keep, plan->bin_count, sizeof(keep));
+                memcpy(plan->bin_count, saved, sizeof(saved));  // heavy bin only
+                run_rows(plan, COUNT, A, B, ho);
+                memcpy(plan->bin_count, keep, sizeof(keep));
+                if ((st = scan_counts(plan, plan->item_cnt.as<int32_t>(), plan->n_items,
+                                      plan->item_scan.as<int64_t>(), nullptr,
+                                      &plan->misc.as<Misc>()->tile_total)))
+                    return st;
+                plan->items_counted = true;
+            }
             const bool maps = prepare_maps(plan);
             RowOut o{nullptr, plan->c_rp.as<int32_t>(), d_ci, d_v, &plan->misc.as<Misc>()->err,
                      maps};
@@ -712,6 +752,45 @@ int rvsp_cuda_csr_validate(int32_t rows, int32_t cols, int32_t nnz, const int32_
     const int st = csr_check_impl(false, rows, cols, nnz, rp, ci, nullptr);
     if (st < 0) return st;
     return st == 0 ? RVSP_SUCCESS : RVSP_ERROR_INVALID_CSR;
+}
+
+int rvsp_cuda_plan_collect_features(rvsp_cuda_plan_t plan, int on) {
+    if (!plan) return RVSP_ERROR_NULL_POINTER;
+    plan->features = on != 0;
+    return RVSP_SUCCESS;
+}
+
+int rvsp_cuda_plan_row_stats(rvsp_cuda_plan_t plan, float* feat_out, int32_t* cnt_out,
+                             int32_t* ub_out, int32_t n) {
+    if (!plan) return RVSP_ERROR_NULL_POINTER;
+    if (!plan->analysed || n < plan->a_rows) return RVSP_ERROR_INVALID_ARGUMENT;
+    const bool have_feat = plan->features || plan->algo == RVSP_CUDA_ALGO_LEARNED;
+    if (feat_out && !have_feat) return RVSP_ERROR_INVALID_ARGUMENT;
+    const size_t M = (size_t)plan->a_rows;
+    cudaError_t e = cudaSuccess;
+    auto kind = [](const void* p) {
+        return is_dev(p) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    };
+    if (feat_out) e = cudaMemcpyAsync(feat_out, plan->feat.p, M * 16, kind(feat_out), plan->stream);
+    // exact counts: C's row pointer differences are exact on every path
+    if (e == cudaSuccess && cnt_out) {
+        std::vector<int32_t> rp(M + 1);
+        e = cudaMemcpyAsync(rp.data(), plan->c_rp.p, (M + 1) * 4, cudaMemcpyDeviceToHost,
+                            plan->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(plan->stream);
+        if (e == cudaSuccess) {
+            std::vector<int32_t> c(M);
+            for (size_t i = 0; i < M; ++i) c[i] = rp[i + 1] - rp[i];
+            e = cudaMemcpyAsync(cnt_out, c.data(), M * 4,
+                                is_dev(cnt_out) ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost,
+                                plan->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(plan->stream);
+        }
+    }
+    if (e == cudaSuccess && ub_out)
+        e = cudaMemcpyAsync(ub_out, plan->ub.p, M * 4, kind(ub_out), plan->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(plan->stream);
+    return e == cudaSuccess ? RVSP_SUCCESS : fail(e, "row stats");
 }
 
 }  // extern "C"

@@ -40,6 +40,12 @@ struct Misc {
     int64_t bin_prod[NUM_BINS];  // products per bin
     int64_t tile_total;        // scratch total of the tile-histogram scan
     int64_t list_total;        // scratch total of the product-offset scan
+    int32_t lhist[NUM_BINS];   // learned path: rows per predicted-capacity bin
+    int32_t n_need;            // learned path: rows sent to the exact path
+    int32_t pad3;
+    int64_t slot_total;        // learned path: sum of predicted capacities
+    int64_t lstats[6];         // learned path statistics (see rvsp_cuda_plan_learned_stats)
+    int64_t ltile_total;
 };
 
 // Output pointers of a row-kernel launch.
@@ -49,7 +55,9 @@ struct RowOut {
     int32_t* c_ci;
     float* c_v;
     int32_t* err;
-    bool maps;  // FILL: record position maps; REUSE: replay them
+    bool maps;           // FILL: record position maps; REUSE: replay them
+    RowCtl ctl = {nullptr, nullptr, 0};
+    bool learned_bins = false;  // iterate the predicted-capacity bins instead
 };
 
 extern thread_local std::string g_err;
@@ -94,11 +102,20 @@ struct rvsp_cuda_plan {
     // numeric-only reuse (uint8 for tiny rows, uint16 for warp-bin rows);
     // list_off is the product offset of every entry of bin_rows
     int map_policy = 1;   // 0: never record (one-shot plans)
+    bool features = false;  // analysis also writes the per-row model features
+    bool items_counted = true;  // every heavy work item's count (item_scan) is valid
     bool maps_ready = false;
     rvsp::DevBuf pm8, pm16, list_ops, list_off;
     int64_t pm16_base[rvsp::NUM_BINS] = {};
 
-    // learned path
+    // learned path: predicted capacities, their bins (stable partition like
+    // the exact bins), slot offsets of the over-allocated output, the mask of
+    // rows sent back to the exact path
+    rvsp::DevBuf lbin, lcap, ltile_hist, ltile_off, lbin_rows, need;
+    int32_t lcount[rvsp::NUM_BINS] = {};
+    rvsp::BinOffsets loffs = {};
+    int64_t slot_total = 0;
+    int64_t lstats[6] = {};   // predicted rows, overflowed, exact by size, sum nnz / sum cap of predicted, exact rows
     rvsp::DevBuf pred_cap, slot_off, tmp_ci, tmp_v, row_flag;
 
     // numeric-only CUDA graph
@@ -111,7 +128,8 @@ namespace rvsp {
 int stage_operands(rvsp_cuda_plan* plan, const int32_t* a_rp, const int32_t* a_ci,
                    const float* a_v, const int32_t* b_rp, const int32_t* b_ci, const float* b_v,
                    bool cache_index, CsrView* A, CsrView* B);
-int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool features);
+int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool features,
+            int (*pre_sync)(rvsp_cuda_plan*) = nullptr);
 int count_exact(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B);
 void run_rows(rvsp_cuda_plan* plan, int mode, const CsrView& A, const CsrView& B,
               const RowOut& o);
@@ -119,4 +137,14 @@ int scan_counts(rvsp_cuda_plan* plan, const int32_t* in, int64_t n, int64_t* out
                 int32_t* out32, int64_t* total_dev);
 void note_launch(rvsp_cuda_plan* plan, int n);
 void reset_graph(rvsp_cuda_plan* plan);
+void launch_bin_scatter(rvsp_cuda_plan* plan, const uint8_t* bin, const int32_t* tile_off,
+                        int32_t* bin_rows, bool heavy_items);
+int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool fused);
+int learned_finish(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, int32_t* c_ci,
+                   float* c_v);
+int learned_spgemm(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t a_nnz,
+                   const int32_t* a_rp, const int32_t* a_ci, const float* a_v, int32_t b_rows,
+                   int32_t b_cols, int32_t b_nnz, const int32_t* b_rp, const int32_t* b_ci,
+                   const float* b_v, int device_out, int32_t** c_rp_out, int32_t** c_ci_out,
+                   float** c_v_out, int32_t* c_nnz_out);
 }  // namespace rvsp

@@ -73,7 +73,8 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
     if (a_rows <= 0 || a_cols <= 0 || b_cols <= 0) return RVSP_ERROR_INVALID_ARGUMENT;
     if (algo != RVSP_CUDA_ALGO_EXACT && algo != RVSP_CUDA_ALGO_LEARNED)
         return RVSP_ERROR_UNSUPPORTED_BACKEND;
-    if (algo == RVSP_CUDA_ALGO_LEARNED) return RVSP_ERROR_UNSUPPORTED_BACKEND;
+    if (algo == RVSP_CUDA_ALGO_LEARNED && !rvsp_cuda_learned_available())
+        return RVSP_ERROR_UNSUPPORTED_BACKEND;
     *c_rp_out = nullptr;
     *c_ci_out = nullptr;
     *c_v_out = nullptr;
@@ -90,7 +91,11 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
     const bool dev = is_dev(a_rp);
     keep_pool_memory();
 
-    {
+    if (algo == RVSP_CUDA_ALGO_LEARNED) {
+        st = learned_spgemm(plan, a_rows, a_cols, a_nnz, a_rp, a_ci, a_v, a_cols, b_cols,
+                            b_nnz, b_rp, b_ci, b_v, dev ? 1 : 0, c_rp_out, c_ci_out, c_v_out,
+                            c_nnz_out);
+    } else {
         int64_t nnz = 0;
         size_t ws = 0;
         st = rvsp_cuda_symbolic(plan, a_rows, a_cols, a_nnz, a_rp, a_ci, a_cols, b_cols, b_nnz,

@@ -132,7 +132,6 @@ __device__ __forceinline__ void ordered_add(float* vals, int slot, bool active, 
 // Analysis: one CTA per tile of AN_TILE rows; threads stride over the tile's
 // A entries (a contiguous range of col_idx) so long rows are shared.
 // ---------------------------------------------------------------------------
-constexpr int AN_TILE = 256;
 
 struct AnalyzeOut {
     int64_t* ops;        // [rows] intermediate products per row
@@ -263,7 +262,7 @@ __global__ void __launch_bounds__(AN_TILE)
     const int pos = tile_off[b * gridDim.x + blockIdx.x] + before +
                     __popc(peers & ((1u << lane) - 1));
     bin_rows[pos] = row;
-    if (b == BIN_HEAVY) {
+    if (b == BIN_HEAVY && items) {
         const int n = nchunks[row];
         const int first = atomicAdd(item_cursor, n);
         const int lo = chunk_lo[row];
@@ -303,22 +302,23 @@ __global__ void __launch_bounds__(TINY_TPB)
            int32_t* __restrict__ cnt, const int32_t* __restrict__ c_rp,
            int32_t* __restrict__ c_ci, float* __restrict__ c_v,
            const int32_t* __restrict__ list_off, uint8_t* __restrict__ pm,
-           int32_t* __restrict__ err) {
+           int32_t* __restrict__ err, RowCtl ctl) {
     __shared__ int32_t s_col[TINY_CAP * TINY_LD];
     __shared__ float s_val[(MODE == COUNT ? 1 : TINY_CAP) * TINY_LD];
     const int t = threadIdx.x, lane = lane_id(), wbase = t & ~31;
     const int i = blockIdx.x * TINY_TPB + t;
-    const bool live = i < nrows;
+    int row = i < nrows ? rows[i] : 0;
+    const bool live = i < nrows && !(ctl.only && !ctl.only[row]);
 #define COL(x) s_col[(x) * TINY_LD + t]
 #define VAL(x) s_val[(x) * TINY_LD + t]
-    int row = 0, n = 0, c0 = 0;
+    int n = 0;
+    int64_t c0 = 0;
     if (live) {
-        row = rows[i];
         int a0, a1;
         row_range(A, row, &a0, &a1, err);
         if (MODE == REUSE) {
             c0 = c_rp[row];
-            n = min(c_rp[row + 1] - c0, TINY_CAP);
+            n = min((int)(c_rp[row + 1] - c0), TINY_CAP);
             for (int x = 0; x < n; ++x) COL(x) = c_ci[c0 + x];
         } else {
             for (int p = a0; p < a1; ++p) {
@@ -341,8 +341,14 @@ __global__ void __launch_bounds__(TINY_TPB)
                 if (m == 0 || COL(m - 1) != c) COL(m++) = c;
             }
             n = m;
-            if (MODE == COUNT) cnt[row] = n;
-            else c0 = c_rp[row];
+            if (MODE == COUNT) {
+                cnt[row] = n;
+            } else if (ctl.slot_off) {
+                c0 = ctl.slot_off[row];
+                cnt[row] = n;
+            } else {
+                c0 = c_rp[row];
+            }
         }
         if (MODE != COUNT) {
             uint8_t* pp = pm ? pm + (list_off[i] - list_off[0]) : nullptr;
@@ -365,7 +371,7 @@ __global__ void __launch_bounds__(TINY_TPB)
     if (MODE == COUNT) return;
     __syncwarp();
     for (int j = 0; j < 32; ++j) {  // coalesced write-out, one row per step
-        const int cj = __shfl_sync(FULL, c0, j);
+        const int64_t cj = __shfl_sync(FULL, (long long)c0, j);
         const int nj = __shfl_sync(FULL, n, j);
         if (lane < nj) {
             if (MODE == FILL) c_ci[cj + lane] = s_col[lane * TINY_LD + wbase + j];
@@ -529,7 +535,7 @@ __global__ void __launch_bounds__(WARPS * 32)
            int32_t* __restrict__ cnt, const int32_t* __restrict__ c_rp,
            int32_t* __restrict__ c_ci, float* __restrict__ c_v,
            const int32_t* __restrict__ list_off, uint16_t* __restrict__ pm,
-           int32_t* __restrict__ err) {
+           int32_t* __restrict__ err, RowCtl ctl) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int LOG2CAP = __builtin_ctz(CAP);
     const int warp = threadIdx.x >> 5, lane = lane_id();
@@ -537,9 +543,14 @@ __global__ void __launch_bounds__(WARPS * 32)
     float* vals = reinterpret_cast<float*>(keys + CAP);
     volatile int32_t* vkeys = keys;
 
+    // learned FILL: a table that fills up means the row outgrew its predicted
+    // capacity; the row is flagged for the exact path instead of an error
+    const bool learned = MODE != REUSE && ctl.learned;
     for (int w = blockIdx.x * WARPS + warp; w < nrows; w += gridDim.x * WARPS) {
         const int row = rows[w];
+        if (ctl.only && !ctl.only[row]) continue;
         int L = 0, c0 = 0;
+        bool ovf = false;
         if (MODE == REUSE) {
             c0 = c_rp[row];
             L = min(c_rp[row + 1] - c0, CAP);
@@ -557,7 +568,7 @@ __global__ void __launch_bounds__(WARPS * 32)
         int count = 0;
         int a0, a1;
         row_range(A, row, &a0, &a1, err);
-        for (int base = a0; base < a1; base += 32) {
+        for (int base = a0; base < a1 && !ovf; base += 32) {
             const int j = base + lane;
             int bs = 0, bl = 0;
             float av = 0.0f;
@@ -569,7 +580,7 @@ __global__ void __launch_bounds__(WARPS * 32)
             }
             const int incl = warp_incl_scan(bl);
             const int total = __shfl_sync(FULL, incl, 31);
-            for (int f = 0; f < total; f += 32) {
+            for (int f = 0; f < total && !ovf; f += 32) {
                 const int p = f + lane;
                 const bool pv = p < total;
                 const ProductRef pr = locate_product(p, incl, bl, bs, av);
@@ -609,17 +620,20 @@ __global__ void __launch_bounds__(WARPS * 32)
                             }
                             h = (h + 1) & (CAP - 1);
                         }
-                        if (!ok) atomicOr(err, ERR_STRUCTURE);
+                        if (!ok && !learned) atomicOr(err, ERR_STRUCTURE);
                         slot = (int)h;
                     }
                     count += __popc(__ballot_sync(FULL, inserted));
+                    if (learned) ovf = __any_sync(FULL, pv && !ok);
                 }
                 if (MODE != COUNT) ordered_add(vals, slot, ok, __fmul_rn(pr.a, bv));
                 __syncwarp();
             }
         }
         __syncwarp();
-        if (MODE == COUNT) {
+        if (learned && (ovf || (MODE == FILL && count > ctl.slot_off[row + 1] - ctl.slot_off[row]))) {
+            if (lane == 0) cnt[row] = -1;
+        } else if (MODE == COUNT) {
             if (lane == 0) cnt[row] = count;
         } else if (MODE == REUSE) {
             for (int x = lane; x < L; x += 32) c_v[c0 + x] = vals[x];
@@ -664,11 +678,12 @@ __global__ void __launch_bounds__(WARPS * 32)
                     __syncwarp();
                 }
             }
-            const int o = c_rp[row];
+            const int64_t o = learned ? ctl.slot_off[row] : (int64_t)c_rp[row];
             for (int x = lane; x < n; x += 32) {
                 c_ci[o + x] = keys[x];
                 c_v[o + x] = vals[x];
             }
+            if (learned && lane == 0) cnt[row] = n;
             if (pm) {  // second walk: position of every product in the sorted row
                 uint16_t* pp = pm + (list_off[w] - list_off[0]);
                 for (int base = a0; base < a1; base += 32) {
@@ -764,7 +779,8 @@ __global__ void __launch_bounds__(WARPS * 32)
     k_heavy(CsrView A, CsrView B, const HeavyItem* __restrict__ items, int nitems,
             int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
             const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
-            int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err) {
+            int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err,
+            RowCtl ctl) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int NW = HEAVY_CW / 32;
     const int warp = threadIdx.x >> 5, lane = lane_id();
@@ -775,6 +791,7 @@ __global__ void __launch_bounds__(WARPS * 32)
     for (int w = blockIdx.x * WARPS + warp; w < nitems; w += gridDim.x * WARPS) {
         const HeavyItem it = items[w];
         const int row = it.row;
+        if (ctl.only && !ctl.only[row]) continue;
         const int lo = it.chunk * HEAVY_CW;
         const int hi = min(lo + HEAVY_CW, B.cols);
         if (MODE != COUNT)
@@ -823,7 +840,7 @@ __global__ void __launch_bounds__(WARPS * 32)
             for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
             if (lane == 0) {
                 item_cnt[w] = c;
-                if (c) atomicAdd(&row_cnt[row], c);
+                if (c && row_cnt) atomicAdd(&row_cnt[row], c);
             }
         } else if (MODE == FILL) {
             int64_t out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
@@ -853,6 +870,14 @@ __global__ void __launch_bounds__(WARPS * 32)
         }
         __syncwarp();
     }
+}
+
+// Heavy rows whose column-chunk counts are still missing (rows the learned
+// structure analysis sized by prediction rather than counting by chunk).
+__global__ void k_heavy_uncounted(int32_t rows, const uint8_t* __restrict__ bin,
+                                  const uint8_t* __restrict__ need, uint8_t* __restrict__ mask) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < rows) mask[r] = bin[r] == BIN_HEAVY && !need[r];
 }
 
 // ---------------------------------------------------------------------------

@@ -39,6 +39,7 @@ constexpr int BIN_WARP0 = 2;
 constexpr int BIN_HEAVY = BIN_WARP0 + NUM_WARP_BINS;
 constexpr int NUM_BINS = BIN_HEAVY + 1;
 constexpr int HEAVY_CW = 8192;  // columns per heavy work item
+constexpr int AN_TILE = 256;    // rows per analysis / binning tile
 
 struct HeavyItem {
     int32_t row;
@@ -49,6 +50,20 @@ struct HeavyItem {
 
 struct BinOffsets {
     int32_t off[NUM_BINS];
+};
+
+// Extra controls of a row-kernel launch, used by the learned path.
+//   slot_off  FILL writes row r at slot_off[r] instead of c_rp[r]; the slot
+//             holds slot_off[r+1] - slot_off[r] entries; the row's count goes
+//             to cnt[r]
+//   only      when set, row r is processed only if only[r] != 0
+//   learned   tables are sized by a prediction: a row whose table fills up
+//             (or, with slot_off, whose count passes its slot) gets cnt[r] = -1
+//             and is left for the exact path instead of raising an error
+struct RowCtl {
+    const int64_t* slot_off;
+    const uint8_t* only;
+    int learned;
 };
 
 __host__ __device__ inline int bin_of(int64_t ops, int32_t ub) {

@@ -105,7 +105,22 @@ _PROTOS = {
     "rvsp_cuda_csr_check": (C.c_int, [_I32, _I32, _I32, _VP, _VP, C.POINTER(_I32)]),
     "rvsp_cuda_csr_validate": (C.c_int, [_I32, _I32, _I32, _VP, _VP]),
     "rvsp_cuda_launch_count": (_I64, []),
+    "rvsp_cuda_learned_available": (C.c_int, []),
+    "rvsp_cuda_mlp_load": (C.c_int, [C.c_char_p]),
+    "rvsp_cuda_mlp_set": (C.c_int, [_VP, _I32]),
+    "rvsp_cuda_mlp_get": (C.c_int, [_VP, _I32]),
+    "rvsp_cuda_mlp_save": (C.c_int, [C.c_char_p, _VP, _I32]),
+    "rvsp_cuda_mlp_grad": (C.c_int, [_VP, _VP, _VP, _VP, _I32, _VP, _VP]),
+    "rvsp_cuda_mlp_train": (C.c_int, [_VP, _VP, _VP, _VP, _I32, _I32, _I32, C.c_float,
+                                      C.c_uint64, _VP]),
+    "rvsp_cuda_mlp_infer": (C.c_int, [_VP, _I32, _VP, _VP, _I32, _VP, _VP, _VP]),
+    "rvsp_cuda_plan_collect_features": (C.c_int, [_VP, C.c_int]),
+    "rvsp_cuda_plan_row_stats": (C.c_int, [_VP, _VP, _VP, _VP, _I32]),
+    "rvsp_cuda_plan_learned_stats": (C.c_int, [_VP, _VP, _I32]),
 }
+
+MLP_PARAMS = 1282
+MLP_FLOATS = 1291  # [mean(4), inv_std(4), z, params(1282)]
 
 
 def build() -> None:
@@ -238,3 +253,91 @@ class Descriptor:
 
     def invalidate(self):
         self.L.rvsp_spgemm_invalidate_structure(self.h)
+
+
+class Plan:
+    """rvsp_cuda_plan_t: the device-side half of a descriptor, driven directly."""
+
+    def __init__(self, algo=RVSP_CUDA_ALGO_EXACT, features=False):
+        self.L = lib()
+        self.h = C.c_void_p()
+        check(self.L.rvsp_cuda_plan_create(C.byref(self.h), algo), "plan_create")
+        if features:
+            check(self.L.rvsp_cuda_plan_collect_features(self.h, 1))
+        self.rows = 0
+
+    def close(self):
+        if self.h:
+            self.L.rvsp_cuda_plan_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def symbolic(self, A, B, a_nnz=None, b_nnz=None):
+        """A, B: objects with rows, cols, row_ptr, col_idx (numpy or device tensors)."""
+        nnz = C.c_int64()
+        ws = C.c_size_t()
+        a_nnz = int(A.row_ptr[-1]) if a_nnz is None else a_nnz
+        b_nnz = int(B.row_ptr[-1]) if b_nnz is None else b_nnz
+        st = self.L.rvsp_cuda_symbolic(self.h, A.rows, A.cols, a_nnz, ptr(A.row_ptr),
+                                       ptr(A.col_idx), B.rows, B.cols, b_nnz, ptr(B.row_ptr),
+                                       ptr(B.col_idx), C.byref(nnz), C.byref(ws))
+        self.rows = A.rows
+        return st, nnz.value
+
+    def numeric(self, A, B, c_rp, c_ci, c_v, fill=True):
+        return self.L.rvsp_cuda_numeric(self.h, ptr(A.row_ptr), ptr(A.col_idx), ptr(A.values),
+                                        ptr(B.row_ptr), ptr(B.col_idx), ptr(B.values), ptr(c_rp),
+                                        ptr(c_ci), ptr(c_v), 1 if fill else 0, None)
+
+    def row_stats(self):
+        n = self.rows
+        feat = np.zeros((max(n, 1), 4), np.float32)
+        cnt = np.zeros(max(n, 1), np.int32)
+        ub = np.zeros(max(n, 1), np.int32)
+        check(self.L.rvsp_cuda_plan_row_stats(self.h, feat.ctypes.data, cnt.ctypes.data,
+                                              ub.ctypes.data, n), "row_stats")
+        return feat[:n], cnt[:n], ub[:n]
+
+    def learned_stats(self):
+        out = np.zeros(6, np.int64)
+        check(self.L.rvsp_cuda_plan_learned_stats(self.h, out.ctypes.data, 6), "learned_stats")
+        keys = ["predicted_rows", "overflowed_rows", "exact_by_size_rows", "fit_nnz",
+                "fit_capacity", "exact_rows"]
+        return dict(zip(keys, out.tolist()))
+
+
+def model_to_vector(mean, inv_std, z, params):
+    v = np.zeros(MLP_FLOATS, np.float32)
+    v[0:4] = mean
+    v[4:8] = inv_std
+    v[8] = z
+    v[9:] = params
+    return v
+
+
+def model_from_vector(v):
+    v = np.asarray(v, np.float32)
+    return v[0:4].copy(), v[4:8].copy(), float(v[8]), v[9:].copy()
+
+
+def unpack_params(p):
+    """Flat parameter vector -> dict of W1 (32,4) b1 W2 (32,32) b2 W3 (2,32) b3."""
+    p = np.asarray(p)
+    o = 0
+    out = {}
+    for name, shape in (("W1", (32, 4)), ("b1", (32,)), ("W2", (32, 32)), ("b2", (32,)),
+                        ("W3", (2, 32)), ("b3", (2,))):
+        size = int(np.prod(shape))
+        out[name] = p[o:o + size].reshape(shape)
+        o += size
+    return out
+
+
+def pack_params(d):
+    return np.concatenate([np.asarray(d[k], np.float32).ravel()
+                           for k in ("W1", "b1", "W2", "b2", "W3", "b3")])
