@@ -200,6 +200,30 @@ RVSP_CUDA_API int rvsp_cuda_plan_row_stats(rvsp_cuda_plan_t plan, float *feat_ou
  * predicted rows that fit, [5] rows finished by the exact path. */
 RVSP_CUDA_API int rvsp_cuda_plan_learned_stats(rvsp_cuda_plan_t plan, int64_t *out, int32_t n);
 
+/*
+ * Allocation-free row pointer of C from per-row counts. No counterpart in the
+ * reference: this entry point exists for callers that cannot allocate device
+ * memory where they need the prefix sum -- code recording a CUDA graph under
+ * stream capture, latency-critical loops that cannot take the device-wide
+ * synchronisation of cudaFree, hosts whose memory budget another allocator
+ * owns. It calls no cudaMalloc/cudaFree: its scratch is a static ~32 KiB
+ * device array held by every GPU that loads this library until exit.
+ *
+ * counts (n int32, device) -> row_ptr (n + 1 int32, device), exclusive prefix
+ * sum with row_ptr[n] = total; the same values the plan path writes to C's
+ * row pointer. n is limited to 8,388,608 rows (RVSP_ERROR_INVALID_ARGUMENT
+ * beyond). stream is a cudaStream_t (NULL: legacy default stream). With
+ * total_out non-NULL the call synchronises the stream, stores the total and
+ * returns RVSP_ERROR_ALLOCATION_FAILED when it exceeds INT32_MAX; with
+ * total_out NULL it returns once the work is enqueued.
+ * The first call on a device resolves the scratch array's address (once per
+ * device, with that device current), so make it before any stream capture.
+ * All calls on a device share the scratch: calls that overlap on the GPU race
+ * and must be serialised by the caller.
+ */
+RVSP_CUDA_API int rvsp_cuda_row_ptr_noalloc(const int32_t *counts, int32_t n, int32_t *row_ptr,
+                                            int64_t *total_out, void *stream);
+
 /* Number of kernels this library has launched in this process (graph
  * replays count each kernel node), for launch accounting in benchmarks. */
 RVSP_CUDA_API int64_t rvsp_cuda_launch_count(void);

@@ -794,3 +794,104 @@ int rvsp_cuda_plan_row_stats(rvsp_cuda_plan_t plan, float* feat_out, int32_t* cn
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free row pointer from per-row counts.
+//
+// For callers that cannot allocate device memory at the point they need C's
+// row pointer: code recording a CUDA graph under stream capture (cudaMalloc
+// there is illegal or stays out of the graph), latency-critical or real-time
+// loops that cannot afford the device-wide synchronisation cudaFree implies,
+// and hosts where another allocator already owns the device memory budget.
+// The scan's scratch (one int64 partial sum per 2048-row tile, the total and
+// an overflow flag) lives in the file-scope array below instead of a plan.
+//
+// The array is a single static allocation of about 32 KiB that every GPU
+// holding this library keeps until the process exits, so the row count is
+// capped at NOALLOC_MAX_ROWS. All calls on a device share it and it keeps the
+// last call's contents: the overflow flag is cleared at the start of every
+// call (the partial sums and total are fully rewritten), and calls whose work
+// overlaps on the GPU (different streams, no ordering between them) race on
+// it and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t NOALLOC_MAX_TILES = 4096;
+constexpr int64_t NOALLOC_MAX_ROWS = NOALLOC_MAX_TILES * SCAN_TILE;  // 8,388,608 rows
+
+struct NoAllocScratch {
+    int64_t tile_sums[NOALLOC_MAX_TILES];
+    int64_t total;
+    int32_t overflow;
+    int32_t pad;
+};
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+NoAllocScratch* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+
+}  // namespace
+
+extern "C" {
+
+int rvsp_cuda_row_ptr_noalloc(const int32_t* counts, int32_t n, int32_t* row_ptr,
+                              int64_t* total_out, void* stream) {
+    if (!counts || !row_ptr) return RVSP_ERROR_NULL_POINTER;
+    if (n <= 0 || (int64_t)n > NOALLOC_MAX_ROWS) {
+        g_err = "rvsp_cuda_row_ptr_noalloc: n must be in [1, 8388608] (static scratch of 4096 "
+                "tiles x 2048 rows)";
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    }
+    if (!is_dev(counts) || !is_dev(row_ptr)) {
+        g_err = "rvsp_cuda_row_ptr_noalloc: counts and row_ptr must be device memory";
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(e, "rvsp_cuda_row_ptr_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        g_err = "rvsp_cuda_row_ptr_noalloc: device index too large";
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    }
+    NoAllocScratch* scratch = nullptr;
+    {
+        // once per device, with that device current: the host-side name of a
+        // __device__ array is not a device address, so resolve it here
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess)
+                return fail(e, "rvsp_cuda_row_ptr_noalloc: cudaGetSymbolAddress");
+            g_noalloc_addr[dev] = static_cast<NoAllocScratch*>(p);
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t ntiles = ((int64_t)n + SCAN_TILE - 1) / SCAN_TILE;
+    e = cudaMemsetAsync(&scratch->overflow, 0, sizeof(int32_t), st);
+    if (e != cudaSuccess) return fail(e, "rvsp_cuda_row_ptr_noalloc: clear");
+    k_scan_reduce<<<(unsigned)ntiles, SCAN_TPB, 0, st>>>(counts, n, scratch->tile_sums);
+    k_scan_tiles<<<1, SCAN_TPB, 0, st>>>(scratch->tile_sums, ntiles, &scratch->total);
+    k_scan_apply<<<(unsigned)ntiles, SCAN_TPB, 0, st>>>(counts, n, scratch->tile_sums,
+                                                        &scratch->total, nullptr, row_ptr,
+                                                        &scratch->overflow);
+    note_launch(nullptr, 3);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "rvsp_cuda_row_ptr_noalloc");
+    if (total_out) {
+        int64_t host[2] = {0, 0};  // total, then the overflow flag in the low word
+        e = cudaMemcpyAsync(host, &scratch->total, sizeof(host), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail(e, "rvsp_cuda_row_ptr_noalloc: read total");
+        *total_out = host[0];
+        if ((int32_t)(host[1] & 0xffffffff) != 0 || host[0] > INT32_MAX) {
+            g_err = "rvsp_cuda_row_ptr_noalloc: total exceeds INT32_MAX";
+            return RVSP_ERROR_ALLOCATION_FAILED;
+        }
+    }
+    return RVSP_SUCCESS;
+}
+
+}  // extern "C"

@@ -117,6 +117,7 @@ _PROTOS = {
     "rvsp_cuda_plan_collect_features": (C.c_int, [_VP, C.c_int]),
     "rvsp_cuda_plan_row_stats": (C.c_int, [_VP, _VP, _VP, _VP, _I32]),
     "rvsp_cuda_plan_learned_stats": (C.c_int, [_VP, _VP, _I32]),
+    "rvsp_cuda_row_ptr_noalloc": (C.c_int, [_VP, _I32, _VP, C.POINTER(_I64), _VP]),
 }
 
 MLP_PARAMS = 1282
