@@ -2,7 +2,7 @@
 """FP32 CSR SpGEMM benchmark on B200 (one process per GPU).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload poisson_reuse|plain]
+                    [--workload poisson_reuse|plain|batched|tall_skinny]
 
 Default workload (the descriptor-reuse case): C = A * A for the 5-point
 Laplacian on a 1024 x 1024 grid (N = 1,048,576, nnz(A) = 5,238,784,
@@ -377,17 +377,170 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# other BASELINE workloads: exact vs learned (and batched vs sequential)
+# ---------------------------------------------------------------------------
+
+class DevMat:
+    def __init__(self, M, torch):
+        self.rows, self.cols, self.nnz = M.rows, M.cols, M.nnz
+        d = lambda a: torch.from_numpy(np.ascontiguousarray(a if a.size else np.zeros(1, a.dtype))).cuda()  # noqa: E731
+        self.row_ptr, self.col_idx, self.values = d(M.row_ptr), d(M.col_idx), d(M.values)
+
+
+def _oneshot_dev(rv, A, B, algo):
+    import ctypes as C
+    L = rv.lib()
+    prp, pci, pv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    nnz = C.c_int32()
+    st = L.rvsp_cuda_spgemm_f32(algo, A.rows, A.cols, B.cols, A.row_ptr.data_ptr(),
+                                A.col_idx.data_ptr(), A.values.data_ptr(), B.row_ptr.data_ptr(),
+                                B.col_idx.data_ptr(), B.values.data_ptr(), C.byref(prp),
+                                C.byref(pci), C.byref(pv), C.byref(nnz), None)
+    rv.check(st, "rvsp_cuda_spgemm_f32")
+    return (prp.value, pci.value, pv.value), nnz.value
+
+
+def _time(fn, steps, warmup, torch):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    return statistics.median(ts)
+
+
+def _d2h(ptr_, n, dtype, torch):
+    """Copy n elements of a library-owned device array to the host."""
+    import ctypes as C
+    if n == 0:
+        return sha(np.zeros(0, dtype))
+    out = np.empty(n, dtype)
+    cuda = C.CDLL("libcuda.so.1")
+    cuda.cuMemcpyDtoH_v2.argtypes = [C.c_void_p, C.c_uint64, C.c_size_t]
+    assert cuda.cuMemcpyDtoH_v2(out.ctypes.data, ptr_, out.nbytes) == 0
+    return out
+
+
+def run_compare(args):
+    """One-shot exact vs learned (and batched vs sequential) on a BASELINE config."""
+    import torch
+
+    import rvsp_b200 as rv
+    from rvsp_b200 import gen
+    torch.zeros(1, device="cuda")
+    L = rv.lib()
+    res = {}
+    if args.workload in ("plain", "tall_skinny"):
+        if args.workload == "plain":
+            A = gen.uniform_fixed()
+            B = A
+            cfg = {"workload": "plain_4096x4096_16_per_row", "seed": 0}
+        else:
+            A, B = gen.tall_skinny(a_rows=args.ts_rows)
+            cfg = {"workload": f"tall_skinny_{args.ts_rows}x100000_x_100000^2", "a_rows": A.rows,
+                   "nnz_a": A.nnz, "nnz_b": B.nnz}
+        P = gen.products(A, B)
+        dA, dB = DevMat(A, torch), DevMat(B, torch)
+        times = {}
+        outs = {}
+        for name, algo in (("exact", rv.RVSP_CUDA_ALGO_EXACT), ("learned", rv.RVSP_CUDA_ALGO_LEARNED)):
+            def fn(algo=algo):
+                ptrs, n = _oneshot_dev(rv, dA, dB, algo)
+                rv.free_device(*ptrs)
+            times[name] = _time(fn, args.steps, args.warmup, torch)
+            ptrs, n = _oneshot_dev(rv, dA, dB, algo)
+            outs[name] = (_d2h(ptrs[0], A.rows + 1, np.int32, torch),
+                          _d2h(ptrs[1], n, np.int32, torch), _d2h(ptrs[2], n, np.float32, torch))
+            rv.free_device(*ptrs)
+        same = all(np.array_equal(a, b) for a, b in zip(outs["exact"], outs["learned"]))
+        nnz_c = int(outs["exact"][0][-1])
+        res["config"] = dict(cfg, rows=A.rows, products=P, nnz_c=nnz_c)
+        res["exact_gflops"] = 2 * P / times["exact"] / 1e9
+        res["learned_gflops"] = 2 * P / times["learned"] / 1e9
+        res["learned_over_exact"] = times["exact"] / times["learned"]
+        res["learned_bit_identical_to_exact"] = bool(same)
+        res["ms"] = {k: v * 1e3 for k, v in times.items()}
+        b_alg = algorithmic_bytes(A.rows, A.nnz, nnz_c, None if B is A else B.rows,
+                                  None if B is A else B.nnz)
+        res["bytes_alg"] = b_alg
+        res["hbm_frac_learned"] = b_alg / times["learned"] / 1e9 / peaks()[0]
+        # FP64 error of the FP32 result on sampled rows
+        import oracle
+        rng = np.random.default_rng(0)
+        rows = np.sort(rng.choice(A.rows, min(2000, A.rows), replace=False))
+        errs = []
+        rp, ci, v = outs["exact"]
+        for r in rows[:400]:
+            srp, sci, sv = oracle.spgemm_f32(A, B, int(r), int(r) + 1)
+            d = oracle.numeric_f64(A, B, srp, sci, int(r), int(r) + 1)
+            got = v[rp[r]:rp[r + 1]]
+            assert np.array_equal(sci, ci[rp[r]:rp[r + 1]])
+            errs.append(np.abs(got - d) / np.maximum(np.abs(d), 1e-30))
+        e = np.concatenate(errs) if errs else np.zeros(1)
+        res["fp32_vs_fp64_rel_err"] = {"max": float(e.max()), "median": float(np.median(e)),
+                                       "p99": float(np.quantile(e, 0.99)), "rows_sampled": 400}
+    elif args.workload == "batched":
+        pairs = gen.batched_uneven(count=args.batch_count)
+        P = sum(gen.products(A, B) for A, B in pairs)
+        dev_pairs = [(DevMat(A, torch), DevMat(B, torch)) for A, B in pairs]
+        def seq():
+            for dA, dB in dev_pairs:
+                ptrs, n = _oneshot_dev(rv, dA, dB, rv.RVSP_CUDA_ALGO_EXACT)
+                rv.free_device(*ptrs)
+        times = {"sequential_exact": _time(seq, max(1, args.steps // 10), 1, torch)}
+        for name, algo in (("batched_exact", rv.RVSP_CUDA_ALGO_EXACT),
+                           ("batched_learned", rv.RVSP_CUDA_ALGO_LEARNED)):
+            def fn(algo=algo):
+                ptrs, n, offs = rv.spgemm_batched(dev_pairs, algo)
+                rv.free_device(*ptrs)
+            times[name] = _time(fn, args.steps, args.warmup, torch)
+        ptrs, n, offs = rv.spgemm_batched(dev_pairs, rv.RVSP_CUDA_ALGO_LEARNED)
+        crp = _d2h(ptrs[0], int(offs[-1]) + 1, np.int32, torch)
+        cci = _d2h(ptrs[1], n, np.int32, torch)
+        cv = _d2h(ptrs[2], n, np.float32, torch)
+        rv.free_device(*ptrs)
+        # spot-check three products against the oracle
+        import oracle
+        ok = True
+        for i in (0, len(pairs) // 2, len(pairs) - 1):
+            A, B = pairs[i]
+            r0, r1 = int(offs[i]), int(offs[i + 1])
+            wrp, wci, wv = oracle.spgemm_f32(A, B)
+            lrp = crp[r0:r1 + 1] - crp[r0]
+            ok &= np.array_equal(lrp, wrp) and np.array_equal(cci[crp[r0]:crp[r1]], wci) and \
+                np.array_equal(cv[crp[r0]:crp[r1]].view(np.uint32), wv.view(np.uint32))
+        res["config"] = {"workload": f"batched_{len(pairs)}_uneven", "products": P,
+                         "rows": int(offs[-1]), "nnz_c": n}
+        res["gflops"] = {k: 2 * P / t / 1e9 for k, t in times.items()}
+        res["ms"] = {k: t * 1e3 for k, t in times.items()}
+        res["batched_learned_over_sequential"] = times["sequential_exact"] / times["batched_learned"]
+        res["batched_learned_over_batched_exact"] = times["batched_exact"] / times["batched_learned"]
+        res["spot_check_bit_exact_vs_oracle"] = bool(ok)
+    print(json.dumps({"workload": args.workload, **res}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="poisson_reuse",
+                    choices=["poisson_reuse", "plain", "batched", "tall_skinny"])
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--ts-rows", type=int, default=2_000_000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "poisson_reuse":
+        run_compare(args)
     else:
         run_ours(args)
 

@@ -144,6 +144,28 @@ RVSP_CUDA_API int rvsp_cuda_csr_check(int32_t rows, int32_t cols, int32_t nnz,
 RVSP_CUDA_API int rvsp_cuda_csr_validate(int32_t rows, int32_t cols, int32_t nnz,
                            const int32_t *row_ptr, const int32_t *col_idx);
 
+/*
+ * Batched products C_i = A_i * B_i, i < count, in one pipeline (no
+ * counterpart in the reference, whose callers loop over rvsp_spgemm_csr).
+ * Sizes are host arrays [count]; operand arrays are host arrays [count] of
+ * device pointers. The operands are packed on the device into block-stacked
+ * matrices (A_i's columns shifted, B_i's kept) and multiplied as one
+ * product, so every row of every product is binned and launched together.
+ * Output: one packed C (device, callee-allocated, release with
+ * rvsp_cuda_free) whose rows [row_offsets_out[i], row_offsets_out[i+1]) are
+ * C_i, with C_i's own column indices; c_row_ptr is global (subtract
+ * c_row_ptr[row_offsets_out[i]] for C_i's local row pointer).
+ * row_offsets_out is a host array [count + 1]. algo is
+ * RVSP_CUDA_ALGO_EXACT or RVSP_CUDA_ALGO_LEARNED.
+ */
+RVSP_CUDA_API int rvsp_cuda_spgemm_batched_f32(
+    int algo, int32_t count, const int32_t *a_rows, const int32_t *a_cols, const int32_t *b_cols,
+    const int32_t *a_nnz, const int32_t *b_nnz, const int32_t *const *a_row_ptr,
+    const int32_t *const *a_col_idx, const float *const *a_values,
+    const int32_t *const *b_row_ptr, const int32_t *const *b_col_idx,
+    const float *const *b_values, int32_t **c_row_ptr_out, int32_t **c_col_idx_out,
+    float **c_values_out, int64_t *c_nnz_out, int64_t *row_offsets_out);
+
 /* ------------------------------------------------------------------------
  * Learned row-size predictor (no counterpart in the reference).
  *

@@ -118,6 +118,10 @@ _PROTOS = {
     "rvsp_cuda_plan_row_stats": (C.c_int, [_VP, _VP, _VP, _VP, _I32]),
     "rvsp_cuda_plan_learned_stats": (C.c_int, [_VP, _VP, _I32]),
     "rvsp_cuda_row_ptr_noalloc": (C.c_int, [_VP, _I32, _VP, C.POINTER(_I64), _VP]),
+    "rvsp_cuda_spgemm_batched_f32": (C.c_int, [C.c_int, _I32, _VP, _VP, _VP, _VP, _VP,
+                                               _VP, _VP, _VP, _VP, _VP, _VP,
+                                               C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
+                                               C.POINTER(_I64), _VP]),
 }
 
 MLP_PARAMS = 1282
@@ -342,3 +346,37 @@ def unpack_params(p):
 def pack_params(d):
     return np.concatenate([np.asarray(d[k], np.float32).ravel()
                            for k in ("W1", "b1", "W2", "b2", "W3", "b3")])
+
+
+def spgemm_batched(pairs_dev, algo=RVSP_CUDA_ALGO_EXACT):
+    """Batched product of device operand pairs (objects with rows, cols, nnz,
+    row_ptr, col_idx, values as device tensors). Returns the library-owned
+    packed C device pointers (rp, ci, v), nnz and the row offsets; release the
+    pointers with free_device()."""
+    L = lib()
+    n = len(pairs_dev)
+    i32 = lambda xs: np.ascontiguousarray(xs, np.int32)  # noqa: E731
+    vp = lambda xs: (C.c_void_p * n)(*[ptr(x) for x in xs])  # noqa: E731
+    a_rows = i32([a.rows for a, b in pairs_dev])
+    a_cols = i32([a.cols for a, b in pairs_dev])
+    b_cols = i32([b.cols for a, b in pairs_dev])
+    a_nnz = i32([a.nnz for a, b in pairs_dev])
+    b_nnz = i32([b.nnz for a, b in pairs_dev])
+    arrs = [vp([a.row_ptr for a, b in pairs_dev]), vp([a.col_idx for a, b in pairs_dev]),
+            vp([a.values for a, b in pairs_dev]), vp([b.row_ptr for a, b in pairs_dev]),
+            vp([b.col_idx for a, b in pairs_dev]), vp([b.values for a, b in pairs_dev])]
+    prp, pci, pv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    nnz = C.c_int64()
+    offs = np.zeros(n + 1, np.int64)
+    st = L.rvsp_cuda_spgemm_batched_f32(algo, n, a_rows.ctypes.data, a_cols.ctypes.data,
+                                        b_cols.ctypes.data, a_nnz.ctypes.data, b_nnz.ctypes.data,
+                                        *[C.cast(x, C.c_void_p) for x in arrs], C.byref(prp),
+                                        C.byref(pci), C.byref(pv), C.byref(nnz), offs.ctypes.data)
+    check(st, "rvsp_cuda_spgemm_batched_f32")
+    return (prp.value, pci.value, pv.value), nnz.value, offs
+
+
+def free_device(*ptrs):
+    for p in ptrs:
+        if p:
+            lib().rvsp_cuda_free(p)

@@ -356,3 +356,28 @@ def test_descriptor_reuse_all_bins(gpu_lib, device):
         assert np.array_equal(got_ci, wci)
         assert np.array_equal(bits(got_v), bits(want)), rep
     d.close()
+
+
+@pytest.mark.parametrize("algo", [rv.RVSP_CUDA_ALGO_EXACT, rv.RVSP_CUDA_ALGO_LEARNED])
+def test_batched_products_match_oracle(gpu_lib, algo):
+    """Uneven products in one batched call: each row range of the packed C is
+    that product's C, bit for bit, with its own column indices."""
+    if algo == rv.RVSP_CUDA_ALGO_LEARNED and not rv.lib().rvsp_cuda_learned_available():
+        pytest.skip("no row-size model")
+    pairs = gen.batched_uneven(count=24, lo=8, hi=4000, seed=13)
+    pairs.append((gen.uniform_fixed(50, 3, 2, seed=1), gen.uniform_fixed(3, 9000, 3, seed=2)))
+    dev_pairs = [(DevCSR(A), DevCSR(B)) for A, B in pairs]
+    (prp, pci, pv), nnz, offs = rv.spgemm_batched(dev_pairs, algo)
+    try:
+        crp = d2h(prp, int(offs[-1]) + 1, np.int32)
+        cci = d2h(pci, nnz, np.int32)
+        cv = d2h(pv, nnz, np.float32)
+    finally:
+        rv.free_device(prp, pci, pv)
+    assert offs[-1] == sum(A.rows for A, _ in pairs)
+    for i, (A, B) in enumerate(pairs):
+        r0, r1 = int(offs[i]), int(offs[i + 1])
+        wrp, wci, wv = oracle.spgemm_f32(A, B)
+        assert np.array_equal(crp[r0:r1 + 1] - crp[r0], wrp), i
+        assert np.array_equal(cci[crp[r0]:crp[r1]], wci), i
+        assert np.array_equal(bits(cv[crp[r0]:crp[r1]]), bits(wv)), i
