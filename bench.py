@@ -486,8 +486,19 @@ def run_compare(args):
                                        "p99": float(np.quantile(e, 0.99)), "rows_sampled": 400}
     elif args.workload == "batched":
         pairs = gen.batched_uneven(count=args.batch_count)
-        P = sum(gen.products(A, B) for A, B in pairs)
+        prods = [gen.products(A, B) for A, B in pairs]
+        P = sum(prods)
         dev_pairs = [(DevMat(A, torch), DevMat(B, torch)) for A, B in pairs]
+        # one batched call per group whose products (an upper bound on nnz)
+        # fit the int32 row pointer of a packed C
+        groups, cur, acc = [], [], 0
+        for i, p in enumerate(prods):
+            if cur and acc + p > (1 << 31) - 1:
+                groups.append(cur)
+                cur, acc = [], 0
+            cur.append(i)
+            acc += p
+        groups.append(cur)
         def seq():
             for dA, dB in dev_pairs:
                 ptrs, n = _oneshot_dev(rv, dA, dB, rv.RVSP_CUDA_ALGO_EXACT)
@@ -496,10 +507,14 @@ def run_compare(args):
         for name, algo in (("batched_exact", rv.RVSP_CUDA_ALGO_EXACT),
                            ("batched_learned", rv.RVSP_CUDA_ALGO_LEARNED)):
             def fn(algo=algo):
-                ptrs, n, offs = rv.spgemm_batched(dev_pairs, algo)
-                rv.free_device(*ptrs)
+                for g in groups:
+                    ptrs, n, offs = rv.spgemm_batched([dev_pairs[i] for i in g], algo)
+                    rv.free_device(*ptrs)
             times[name] = _time(fn, args.steps, args.warmup, torch)
-        ptrs, n, offs = rv.spgemm_batched(dev_pairs, rv.RVSP_CUDA_ALGO_LEARNED)
+        # correctness: the group holding product 0 (and its spot checks)
+        g0 = groups[0]
+        pairs = [pairs[i] for i in g0]
+        ptrs, n, offs = rv.spgemm_batched([dev_pairs[i] for i in g0], rv.RVSP_CUDA_ALGO_LEARNED)
         crp = _d2h(ptrs[0], int(offs[-1]) + 1, np.int32, torch)
         cci = _d2h(ptrs[1], n, np.int32, torch)
         cv = _d2h(ptrs[2], n, np.float32, torch)
@@ -514,8 +529,8 @@ def run_compare(args):
             lrp = crp[r0:r1 + 1] - crp[r0]
             ok &= np.array_equal(lrp, wrp) and np.array_equal(cci[crp[r0]:crp[r1]], wci) and \
                 np.array_equal(cv[crp[r0]:crp[r1]].view(np.uint32), wv.view(np.uint32))
-        res["config"] = {"workload": f"batched_{len(pairs)}_uneven", "products": P,
-                         "rows": int(offs[-1]), "nnz_c": n}
+        res["config"] = {"workload": f"batched_{len(dev_pairs)}_uneven", "products": P,
+                         "groups": len(groups), "group0_rows": int(offs[-1]), "group0_nnz_c": n}
         res["gflops"] = {k: 2 * P / t / 1e9 for k, t in times.items()}
         res["ms"] = {k: t * 1e3 for k, t in times.items()}
         res["batched_learned_over_sequential"] = times["sequential_exact"] / times["batched_learned"]

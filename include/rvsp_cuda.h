@@ -216,10 +216,12 @@ RVSP_CUDA_API int rvsp_cuda_plan_collect_features(rvsp_cuda_plan_t plan, int on)
 RVSP_CUDA_API int rvsp_cuda_plan_row_stats(rvsp_cuda_plan_t plan, float *feat_out,
                                            int32_t *cnt_out, int32_t *ub_out, int32_t n);
 
-/* Learned-path statistics of the last analysis: [0] rows sized by the
- * prediction, [1] of those, rows that outgrew it, [2] rows too large for a
- * table (exact path), [3] sum of the counts and [4] sum of the capacities of
- * predicted rows that fit, [5] rows finished by the exact path. */
+/* Learned-path statistics of the last analysis (n >= 7): [0] rows sized by
+ * the prediction (where it gives a smaller table than the upper bound),
+ * [1] of those, rows that outgrew it, [2] rows too large for a table (exact
+ * path), [3] sum of the counts, [4] sum of the predicted capacities and
+ * [6] sum of the upper bounds of predicted rows that fit, [5] rows finished
+ * by the exact path. */
 RVSP_CUDA_API int rvsp_cuda_plan_learned_stats(rvsp_cuda_plan_t plan, int64_t *out, int32_t n);
 
 /*

@@ -45,6 +45,7 @@ constexpr int LBIN_EXACT = BIN_HEAVY;  // predicted bin of rows left to the exac
 struct LearnedBinsOut {
     uint8_t* lbin;
     int32_t* lcap;
+    uint8_t* predicted;  // 1 where the row is sized by the prediction
     int32_t* tile_hist;  // [NUM_BINS][tiles]
     int32_t* hist;       // [NUM_BINS]
     int64_t* slot_total;
@@ -52,7 +53,8 @@ struct LearnedBinsOut {
 
 __global__ void __launch_bounds__(AN_TILE)
     k_learned_bins(int32_t rows, const uint8_t* __restrict__ bin, const int64_t* __restrict__ ops,
-                   const int32_t* __restrict__ cap_pred, LearnedBinsOut out) {
+                   const int32_t* __restrict__ ub, const int32_t* __restrict__ cap_pred,
+                   LearnedBinsOut out) {
     __shared__ int32_t s_hist[NUM_BINS];
     __shared__ unsigned long long s_slots;
     const int t = threadIdx.x;
@@ -62,7 +64,7 @@ __global__ void __launch_bounds__(AN_TILE)
     const int row = blockIdx.x * AN_TILE + t;
     if (row < rows) {
         const int b = bin[row];
-        int lb, cap;
+        int lb, cap, predicted = 0;
         if (b == BIN_EMPTY) {
             lb = BIN_EMPTY;
             cap = 0;
@@ -70,18 +72,26 @@ __global__ void __launch_bounds__(AN_TILE)
             lb = BIN_TINY;
             cap = (int)ops[row];
         } else {
+            // the prediction is used only where it buys a smaller table than
+            // the upper bound would; otherwise the row gets the bound's table
+            // and a slot of ub entries, which cannot overflow
             const int c = max(cap_pred[row], 1);
-            const int64_t need = (int64_t)c + (c >> 2);
-            int tcap = WARP_CAP_MIN;
-            lb = BIN_WARP0;
-            while (tcap < need && lb < BIN_HEAVY) {
-                tcap <<= 1;
-                ++lb;
+            const int pb = bin_of(64, c);  // table class of the prediction (ops > tiny)
+            if (pb < b) {
+                lb = pb;
+                cap = c;
+                predicted = 1;
+            } else if (b < BIN_HEAVY) {
+                lb = b;
+                cap = ub[row];
+            } else {
+                lb = LBIN_EXACT;
+                cap = 0;
             }
-            cap = lb == BIN_HEAVY ? 0 : c;  // BIN_HEAVY here means LBIN_EXACT
         }
         out.lbin[row] = (uint8_t)lb;
         out.lcap[row] = cap;
+        out.predicted[row] = (uint8_t)predicted;
         atomicAdd(&s_hist[lb], 1);
         if (cap) atomicAdd(&s_slots, (unsigned long long)cap);
     }
@@ -93,42 +103,49 @@ __global__ void __launch_bounds__(AN_TILE)
     if (t == 0 && s_slots) atomicAdd((unsigned long long*)out.slot_total, s_slots);
 }
 
-// Rows the fused sweep could not finish: predicted too large for a table, or
-// overflowed. Their counts are reset for the exact count kernels.
-// stats: [0] predicted rows that overflowed, [1] rows exact by size,
-//        [2] sum of counts of predicted rows that fit, [3] their capacity
+// Rows the sweep could not finish: too large for a table, or sized by the
+// prediction and outgrown it. Their counts are reset for the exact kernels.
+// stats: [0] rows sized by the prediction, [1] of those, rows that outgrew
+//        it, [2] rows too large for a table, [3] sum of counts, [4] sum of
+//        capacities and [6] sum of upper bounds of predicted rows that fit
 __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
-                       const int32_t* __restrict__ lcap, int32_t* __restrict__ cnt,
-                       uint8_t* __restrict__ need, int32_t* __restrict__ n_need,
-                       int64_t* __restrict__ stats) {
+                       const uint8_t* __restrict__ predicted, const int32_t* __restrict__ lcap,
+                       const int32_t* __restrict__ ub, int32_t* __restrict__ cnt,
+                       uint8_t* __restrict__ need,
+                       int32_t* __restrict__ n_need, int64_t* __restrict__ stats) {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    bool nd = false, ovf = false, big = false;
-    int64_t fitc = 0, fitcap = 0;
+    bool nd = false, ovf = false, big = false, pr = false;
+    int64_t fitc = 0, fitcap = 0, fitub = 0;
     if (row < rows) {
         const int lb = lbin[row];
+        pr = predicted[row] != 0;
         big = lb == LBIN_EXACT;
         ovf = lb >= BIN_WARP0 && lb < LBIN_EXACT && cnt[row] < 0;
         nd = big || ovf;
-        if (lb >= BIN_WARP0 && lb < LBIN_EXACT && !ovf) {
+        if (pr && !ovf) {
             fitc = cnt[row];
             fitcap = lcap[row];
+            fitub = ub[row];
         }
         need[row] = nd ? 1 : 0;
         if (nd) cnt[row] = 0;
     }
-    const unsigned mn = __ballot_sync(FULL, nd), mo = __ballot_sync(FULL, ovf),
-                   mb = __ballot_sync(FULL, big);
+    const unsigned mn = __ballot_sync(FULL, nd), mo = __ballot_sync(FULL, ovf && pr),
+                   mb = __ballot_sync(FULL, big), mp = __ballot_sync(FULL, pr);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         fitc += __shfl_xor_sync(FULL, fitc, o);
         fitcap += __shfl_xor_sync(FULL, fitcap, o);
+        fitub += __shfl_xor_sync(FULL, fitub, o);
     }
     if ((threadIdx.x & 31) == 0) {
         if (mn) atomicAdd(n_need, __popc(mn));
-        if (mo) atomicAdd((unsigned long long*)&stats[0], (unsigned long long)__popc(mo));
-        if (mb) atomicAdd((unsigned long long*)&stats[1], (unsigned long long)__popc(mb));
-        if (fitc) atomicAdd((unsigned long long*)&stats[2], (unsigned long long)fitc);
-        if (fitcap) atomicAdd((unsigned long long*)&stats[3], (unsigned long long)fitcap);
+        if (mp) atomicAdd((unsigned long long*)&stats[0], (unsigned long long)__popc(mp));
+        if (mo) atomicAdd((unsigned long long*)&stats[1], (unsigned long long)__popc(mo));
+        if (mb) atomicAdd((unsigned long long*)&stats[2], (unsigned long long)__popc(mb));
+        if (fitc) atomicAdd((unsigned long long*)&stats[3], (unsigned long long)fitc);
+        if (fitcap) atomicAdd((unsigned long long*)&stats[4], (unsigned long long)fitcap);
+        if (fitub) atomicAdd((unsigned long long*)&stats[6], (unsigned long long)fitub);
     }
 }
 
@@ -175,16 +192,18 @@ static int learned_pre_sync(rvsp_cuda_plan* plan) {
     ENS(plan->lbin_rows, M * 4);
     ENS(plan->need, M);
     ENS(plan->row_flag, M);
+    ENS(plan->pflag, M);
 #undef ENS
     Misc* misc = plan->misc.as<Misc>();
     launch_mlp_infer(model, plan->feat.as<float4>(), plan->ub.as<int32_t>(), plan->bin.as<uint8_t>(),
                      (int32_t)M, plan->pred_cap.as<int32_t>(), plan->stream);
     note_launch(plan, 1);
     LearnedBinsOut lo{plan->lbin.as<uint8_t>(), plan->lcap.as<int32_t>(),
-                      plan->ltile_hist.as<int32_t>(), misc->lhist, &misc->slot_total};
+                      plan->pflag.as<uint8_t>(), plan->ltile_hist.as<int32_t>(), misc->lhist,
+                      &misc->slot_total};
     k_learned_bins<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(
-        (int32_t)M, plan->bin.as<uint8_t>(), plan->ops.as<int64_t>(), plan->pred_cap.as<int32_t>(),
-        lo);
+        (int32_t)M, plan->bin.as<uint8_t>(), plan->ops.as<int64_t>(), plan->ub.as<int32_t>(),
+        plan->pred_cap.as<int32_t>(), lo);
     note_launch(plan, 1);
     return scan_counts(plan, plan->ltile_hist.as<int32_t>(), NUM_BINS * tiles, nullptr,
                        plan->ltile_off.as<int32_t>(), &misc->ltile_total);
@@ -243,8 +262,10 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
     fo.learned_bins = true;
     run_rows(plan, fused ? FILL : COUNT, A, B, fo);
     k_need<<<(unsigned)((M + 255) / 256), 256, 0, plan->stream>>>(
-        (int32_t)M, plan->lbin.as<uint8_t>(), plan->lcap.as<int32_t>(), plan->cnt.as<int32_t>(),
-        plan->need.as<uint8_t>(), &misc->n_need, misc->lstats);
+        (int32_t)M, plan->lbin.as<uint8_t>(), plan->pflag.as<uint8_t>(),
+        plan->lcap.as<int32_t>(), plan->ub.as<int32_t>(), plan->cnt.as<int32_t>(),
+        plan->need.as<uint8_t>(),
+        &misc->n_need, misc->lstats);
     note_launch(plan, 1);
     // exact counts of the rows the sweep could not finish (tiny rows never overflow)
     RowOut co{plan->cnt.as<int32_t>(), nullptr, nullptr, nullptr, &misc->err, false};
@@ -276,13 +297,7 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
     plan->c_nnz = plan->host_misc.scan_total;
     // heavy rows sized by the prediction were never counted by column chunk
     plan->items_counted = plan->n_items == 0 || fused;
-    int64_t predicted = 0;
-    for (int b = BIN_WARP0; b < LBIN_EXACT; ++b) predicted += plan->lcount[b];
-    plan->lstats[0] = predicted;
-    plan->lstats[1] = plan->host_misc.lstats[0];
-    plan->lstats[2] = plan->host_misc.lstats[1];
-    plan->lstats[3] = plan->host_misc.lstats[2];
-    plan->lstats[4] = plan->host_misc.lstats[3];
+    for (int i = 0; i < 7; ++i) plan->lstats[i] = plan->host_misc.lstats[i];
     plan->lstats[5] = plan->host_misc.n_need;
     return RVSP_SUCCESS;
 }
@@ -409,7 +424,7 @@ extern "C" {
 
 int rvsp_cuda_plan_learned_stats(rvsp_cuda_plan_t plan, int64_t* out, int32_t n) {
     if (!plan || !out) return RVSP_ERROR_NULL_POINTER;
-    if (n < 6) return RVSP_ERROR_INVALID_ARGUMENT;
+    if (n < 7) return RVSP_ERROR_INVALID_ARGUMENT;
     if (plan->algo != RVSP_CUDA_ALGO_LEARNED || !plan->analysed) return RVSP_ERROR_INVALID_ARGUMENT;
     memcpy(out, plan->lstats, sizeof(plan->lstats));
     return RVSP_SUCCESS;

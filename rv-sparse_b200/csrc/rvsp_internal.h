@@ -44,7 +44,7 @@ struct Misc {
     int32_t n_need;            // learned path: rows sent to the exact path
     int32_t pad3;
     int64_t slot_total;        // learned path: sum of predicted capacities
-    int64_t lstats[6];         // learned path statistics (see rvsp_cuda_plan_learned_stats)
+    int64_t lstats[7];         // learned path statistics (see rvsp_cuda_plan_learned_stats)
     int64_t ltile_total;
 };
 
@@ -111,11 +111,11 @@ struct rvsp_cuda_plan {
     // learned path: predicted capacities, their bins (stable partition like
     // the exact bins), slot offsets of the over-allocated output, the mask of
     // rows sent back to the exact path
-    rvsp::DevBuf lbin, lcap, ltile_hist, ltile_off, lbin_rows, need;
+    rvsp::DevBuf lbin, lcap, ltile_hist, ltile_off, lbin_rows, need, pflag;
     int32_t lcount[rvsp::NUM_BINS] = {};
     rvsp::BinOffsets loffs = {};
     int64_t slot_total = 0;
-    int64_t lstats[6] = {};   // predicted rows, overflowed, exact by size, sum nnz / sum cap of predicted, exact rows
+    int64_t lstats[7] = {};   // see rvsp_cuda_plan_learned_stats
     rvsp::DevBuf pred_cap, slot_off, tmp_ci, tmp_v, row_flag;
 
     // numeric-only CUDA graph

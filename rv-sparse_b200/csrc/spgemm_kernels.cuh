@@ -504,7 +504,8 @@ __global__ void __launch_bounds__(TRM_WARPS * 32)
 // ---------------------------------------------------------------------------
 template <int CAP, int MODE>
 __host__ __device__ constexpr int warp_smem_bytes() {
-    return (MODE == COUNT ? 4 : 8) * CAP;
+    // COUNT: keys; REUSE: keys + values; FILL: keys + values + radix histogram
+    return (MODE == COUNT ? 4 : 8) * CAP + (MODE == FILL ? 4 * 256 : 0);
 }
 
 // Lane's product p of the current 32-entry A chunk: its B position and the
@@ -529,6 +530,117 @@ __device__ __forceinline__ ProductRef locate_product(int p, int incl, int bl, in
     return ProductRef{e_bs + (p - (e_incl - e_bl)), e_av};
 }
 
+// Walks row [a0, a1) of A times B in the reference's product order, 32
+// products per warp step: f(k, pv, col, bv, av) runs on every lane for the
+// product with row-local index k (pv false on idle lanes), and returns a
+// warp-uniform "stop". VALUES loads B's and A's values too.
+template <bool VALUES, class F>
+__device__ __forceinline__ void walk_products(const CsrView& A, const CsrView& B, int a0, int a1,
+                                              int32_t* err, F&& f) {
+    const int lane = lane_id();
+    int before = 0;
+    for (int base = a0; base < a1; base += 32) {
+        const int j = base + lane;
+        int bs = 0, bl = 0;
+        float av = 0.0f;
+        if (j < a1) {
+            int be;
+            row_range(B, A.ci[j], &bs, &be, err);
+            bl = be - bs;
+            if (VALUES) av = A.v[j];
+        }
+        const int incl = warp_incl_scan(bl);
+        const int total = __shfl_sync(FULL, incl, 31);
+        for (int f0 = 0; f0 < total; f0 += 32) {
+            const int p = f0 + lane;
+            const bool pv = p < total;
+            const ProductRef pr = locate_product(p, incl, bl, bs, av);
+            int col = -1;
+            float bv = 0.0f;
+            if (pv) {
+                col = B.ci[pr.q];
+                if (VALUES) bv = B.v[pr.q];
+            }
+            const bool stop = f(before + p, pv, col, bv, pr.a);
+            __syncwarp();
+            if (stop) return;
+        }
+        before += total;
+    }
+}
+
+// Stable LSD radix sort of keys[0, n) ascending (8-bit digits of key - min,
+// as many passes as the key range needs), tmp[0, n) as the ping-pong buffer,
+// hist 256 ints. Ranks within a digit follow lane order chunk by chunk, so
+// each pass is stable. Result in keys.
+__device__ void warp_radix_sort(int32_t* keys, int32_t* tmp, int n, int32_t* hist) {
+    const int lane = lane_id();
+    if (n <= 1) return;
+    int mn = INT_MAX, mx = INT_MIN;
+    for (int i = lane; i < n; i += 32) {
+        mn = min(mn, keys[i]);
+        mx = max(mx, keys[i]);
+    }
+    mn = __reduce_min_sync(FULL, mn);
+    mx = __reduce_max_sync(FULL, mx);
+    const uint32_t range = (uint32_t)mx - (uint32_t)mn;
+    const int passes = range < (1u << 8) ? 1 : range < (1u << 16) ? 2 : range < (1u << 24) ? 3 : 4;
+    int32_t* src = keys;
+    int32_t* dst = tmp;
+    for (int pass = 0; pass < passes; ++pass) {
+        const int shift = 8 * pass;
+        for (int i = lane; i < 256; i += 32) hist[i] = 0;
+        __syncwarp();
+        for (int i = lane; i < n; i += 32)
+            atomicAdd(&hist[(((uint32_t)src[i] - (uint32_t)mn) >> shift) & 255], 1);
+        __syncwarp();
+        int v[8], s = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            v[j] = hist[lane * 8 + j];
+            s += v[j];
+        }
+        int run = warp_incl_scan(s) - s;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            hist[lane * 8 + j] = run;
+            run += v[j];
+        }
+        __syncwarp();
+        for (int base = 0; base < n; base += 32) {
+            const int i = base + lane;
+            const bool ok = i < n;
+            const int32_t k = ok ? src[i] : 0;
+            const int d = ok ? (int)((((uint32_t)k - (uint32_t)mn) >> shift) & 255) : 256 + lane;
+            const unsigned peers = __match_any_sync(FULL, d);
+            const int leader = __ffs(peers) - 1;
+            int start = 0;
+            if (ok && lane == leader) {
+                start = hist[d];
+                hist[d] = start + __popc(peers);
+            }
+            start = __shfl_sync(FULL, start, leader);
+            if (ok) dst[start + __popc(peers & ((1u << lane) - 1))] = k;
+            __syncwarp();
+        }
+        int32_t* t = src;
+        src = dst;
+        dst = t;
+    }
+    if (src != keys) {
+        for (int i = lane; i < n; i += 32) keys[i] = src[i];
+        __syncwarp();
+    }
+}
+
+// Medium rows: one warp per row, a CAP-slot shared-memory table per warp.
+//   COUNT  hash-insert the row's columns, count the new ones
+//   FILL   COUNT's insert, compaction, radix sort -> sorted columns written;
+//          then the values: every product finds its column's position by
+//          binary search and is added in order (ordered_add); the positions
+//          are recorded in pm when requested (uint16, rows starting at
+//          list_off[w] - list_off[0])
+//   REUSE  the value pass alone, on the stored sorted columns
 template <int CAP, int WARPS, int MODE>
 __global__ void __launch_bounds__(WARPS * 32)
     k_warp(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
@@ -539,172 +651,100 @@ __global__ void __launch_bounds__(WARPS * 32)
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int LOG2CAP = __builtin_ctz(CAP);
     const int warp = threadIdx.x >> 5, lane = lane_id();
-    int32_t* keys = reinterpret_cast<int32_t*>(smem + warp * warp_smem_bytes<CAP, MODE>());
+    unsigned char* mine = smem + warp * warp_smem_bytes<CAP, MODE>();
+    int32_t* keys = reinterpret_cast<int32_t*>(mine);
     float* vals = reinterpret_cast<float*>(keys + CAP);
+    int32_t* hist = reinterpret_cast<int32_t*>(mine + 8 * CAP);
     volatile int32_t* vkeys = keys;
-
-    // learned FILL: a table that fills up means the row outgrew its predicted
+    // learned: a table that fills up means the row outgrew its predicted
     // capacity; the row is flagged for the exact path instead of an error
     const bool learned = MODE != REUSE && ctl.learned;
+
     for (int w = blockIdx.x * WARPS + warp; w < nrows; w += gridDim.x * WARPS) {
         const int row = rows[w];
         if (ctl.only && !ctl.only[row]) continue;
-        int L = 0, c0 = 0;
-        bool ovf = false;
-        if (MODE == REUSE) {
-            c0 = c_rp[row];
-            L = min(c_rp[row + 1] - c0, CAP);
-            for (int x = lane; x < L; x += 32) {
-                keys[x] = c_ci[c0 + x];
-                vals[x] = 0.0f;
-            }
-        } else {
-            for (int x = lane; x < CAP; x += 32) {
-                keys[x] = -1;
-                if (MODE == FILL) vals[x] = 0.0f;
-            }
-        }
-        __syncwarp();
-        int count = 0;
         int a0, a1;
         row_range(A, row, &a0, &a1, err);
-        for (int base = a0; base < a1 && !ovf; base += 32) {
-            const int j = base + lane;
-            int bs = 0, bl = 0;
-            float av = 0.0f;
-            if (j < a1) {
-                int be;
-                row_range(B, A.ci[j], &bs, &be, err);
-                bl = be - bs;
-                if (MODE != COUNT) av = A.v[j];
-            }
-            const int incl = warp_incl_scan(bl);
-            const int total = __shfl_sync(FULL, incl, 31);
-            for (int f = 0; f < total && !ovf; f += 32) {
-                const int p = f + lane;
-                const bool pv = p < total;
-                const ProductRef pr = locate_product(p, incl, bl, bs, av);
-                int col = -1;
-                float bv = 0.0f;
+        int n = 0;          // distinct columns (COUNT/FILL) or stored row length (REUSE)
+        int64_t o = 0;      // where the row's C entries go
+        if (MODE == REUSE) {
+            o = c_rp[row];
+            n = min(c_rp[row + 1] - (int)o, CAP);
+            for (int x = lane; x < n; x += 32) keys[x] = c_ci[o + x];
+        } else {
+            for (int x = lane; x < CAP; x += 32) keys[x] = -1;
+            __syncwarp();
+            bool ovf = false;
+            walk_products<false>(A, B, a0, a1, err, [&](int, bool pv, int col, float, float) {
+                bool inserted = false, ok = true;
                 if (pv) {
-                    col = B.ci[pr.q];
-                    if (MODE != COUNT) bv = B.v[pr.q];
-                }
-                int slot = -1;
-                bool ok = pv;
-                if (MODE == REUSE) {
-                    if (pv) {
-                        slot = smem_lower_bound(keys, L, col);
-                        ok = slot < L;
-                    }
-                } else {
-                    bool inserted = false;
-                    if (pv) {
-                        // at most CAP probes: a table can only fill up when an
-                        // operand breaks the column-range contract
-                        uint32_t h = hash_slot(col, LOG2CAP);
-                        ok = false;
-                        for (int probe = 0; probe < CAP; ++probe) {
-                            const int cur = vkeys[h];
-                            if (cur == col) {
+                    // at most CAP probes: a table can only fill up when an
+                    // operand breaks the column-range contract (or, learned,
+                    // when the prediction was too small)
+                    uint32_t h = hash_slot(col, LOG2CAP);
+                    ok = false;
+                    for (int probe = 0; probe < CAP; ++probe) {
+                        const int cur = vkeys[h];
+                        if (cur == col) {
+                            ok = true;
+                            break;
+                        }
+                        if (cur == -1) {
+                            const int old = atomicCAS(&keys[h], -1, col);
+                            if (old == -1 || old == col) {
+                                inserted = old == -1;
                                 ok = true;
                                 break;
                             }
-                            if (cur == -1) {
-                                const int old = atomicCAS(&keys[h], -1, col);
-                                if (old == -1 || old == col) {
-                                    inserted = old == -1;
-                                    ok = true;
-                                    break;
-                                }
-                            }
-                            h = (h + 1) & (CAP - 1);
                         }
-                        if (!ok && !learned) atomicOr(err, ERR_STRUCTURE);
-                        slot = (int)h;
+                        h = (h + 1) & (CAP - 1);
                     }
-                    count += __popc(__ballot_sync(FULL, inserted));
-                    if (learned) ovf = __any_sync(FULL, pv && !ok);
+                    if (!ok && !learned) atomicOr(err, ERR_STRUCTURE);
                 }
-                if (MODE != COUNT) ordered_add(vals, slot, ok, __fmul_rn(pr.a, bv));
-                __syncwarp();
+                n += __popc(__ballot_sync(FULL, inserted));
+                if (learned) ovf = __any_sync(FULL, !ok);
+                return ovf;
+            });
+            __syncwarp();
+            if (learned && (ovf || (MODE == FILL && n > ctl.slot_off[row + 1] - ctl.slot_off[row]))) {
+                if (lane == 0) cnt[row] = -1;
+                continue;
             }
-        }
-        __syncwarp();
-        if (learned && (ovf || (MODE == FILL && count > ctl.slot_off[row + 1] - ctl.slot_off[row]))) {
-            if (lane == 0) cnt[row] = -1;
-        } else if (MODE == COUNT) {
-            if (lane == 0) cnt[row] = count;
-        } else if (MODE == REUSE) {
-            for (int x = lane; x < L; x += 32) c_v[c0 + x] = vals[x];
-        } else {
-            // compact occupied slots to the front (left moves only)
+            if (MODE == COUNT) {
+                if (lane == 0) cnt[row] = n;
+                continue;
+            }
+            // FILL: compact occupied slots to the front (left moves only)
             int out = 0;
             for (int b0 = 0; b0 < CAP; b0 += 32) {
                 const int key = keys[b0 + lane];
-                const float val = vals[b0 + lane];
-                const bool ok = key != -1;
-                const unsigned m = __ballot_sync(FULL, ok);
+                const bool occ = key != -1;
+                const unsigned m = __ballot_sync(FULL, occ);
                 __syncwarp();
-                if (ok) {
-                    const int pos = out + __popc(m & ((1u << lane) - 1));
-                    keys[pos] = key;
-                    vals[pos] = val;
-                }
+                if (occ) keys[out + __popc(m & ((1u << lane) - 1))] = key;
                 out += __popc(m);
                 __syncwarp();
             }
-            const int n = out;
-            int P = 1;
-            while (P < n) P <<= 1;
-            for (int x = n + lane; x < P; x += 32) keys[x] = INT_MAX;
-            __syncwarp();
-            for (int k = 2; k <= P; k <<= 1) {  // bitonic sort of (key, val)
-                for (int jj = k >> 1; jj > 0; jj >>= 1) {
-                    for (int i = lane; i < P; i += 32) {
-                        const int ixj = i ^ jj;
-                        if (ixj > i) {
-                            const int ki = keys[i], kj = keys[ixj];
-                            const bool up = (i & k) == 0;
-                            if ((ki > kj) == up) {
-                                keys[i] = kj;
-                                keys[ixj] = ki;
-                                const float t0 = vals[i];
-                                vals[i] = vals[ixj];
-                                vals[ixj] = t0;
-                            }
-                        }
-                    }
-                    __syncwarp();
-                }
-            }
-            const int64_t o = learned ? ctl.slot_off[row] : (int64_t)c_rp[row];
-            for (int x = lane; x < n; x += 32) {
-                c_ci[o + x] = keys[x];
-                c_v[o + x] = vals[x];
-            }
+            warp_radix_sort(keys, reinterpret_cast<int32_t*>(vals), n, hist);
+            o = learned ? ctl.slot_off[row] : (int64_t)c_rp[row];
+            for (int x = lane; x < n; x += 32) c_ci[o + x] = keys[x];
             if (learned && lane == 0) cnt[row] = n;
-            if (pm) {  // second walk: position of every product in the sorted row
-                uint16_t* pp = pm + (list_off[w] - list_off[0]);
-                for (int base = a0; base < a1; base += 32) {
-                    const int j = base + lane;
-                    int bs = 0, bl = 0;
-                    if (j < a1) {
-                        int be;
-                        row_range(B, A.ci[j], &bs, &be, err);
-                        bl = be - bs;
-                    }
-                    const int incl = warp_incl_scan(bl);
-                    const int total = __shfl_sync(FULL, incl, 31);
-                    for (int f = 0; f < total; f += 32) {
-                        const int p = f + lane;
-                        const ProductRef pr = locate_product(p, incl, bl, bs, 0.0f);
-                        if (p < total) pp[p] = (uint16_t)smem_lower_bound(keys, n, B.ci[pr.q]);
-                    }
-                    pp += total;
-                }
-            }
         }
+        // values: every product to its column's position, in order
+        for (int x = lane; x < n; x += 32) vals[x] = 0.0f;
+        __syncwarp();
+        uint16_t* pp = (MODE == FILL && pm) ? pm + (list_off[w] - list_off[0]) : nullptr;
+        walk_products<true>(A, B, a0, a1, err, [&](int k, bool pv, int col, float bv, float av) {
+            int pos = -1;
+            if (pv) {
+                pos = smem_lower_bound(keys, n, col);
+                if (pp) pp[k] = (uint16_t)pos;
+            }
+            ordered_add(vals, pos, pv && pos < n, __fmul_rn(av, bv));
+            return false;
+        });
+        __syncwarp();
+        for (int x = lane; x < n; x += 32) c_v[o + x] = vals[x];
         __syncwarp();
     }
 }

@@ -309,10 +309,10 @@ class Plan:
         return feat[:n], cnt[:n], ub[:n]
 
     def learned_stats(self):
-        out = np.zeros(6, np.int64)
-        check(self.L.rvsp_cuda_plan_learned_stats(self.h, out.ctypes.data, 6), "learned_stats")
+        out = np.zeros(7, np.int64)
+        check(self.L.rvsp_cuda_plan_learned_stats(self.h, out.ctypes.data, 7), "learned_stats")
         keys = ["predicted_rows", "overflowed_rows", "exact_by_size_rows", "fit_nnz",
-                "fit_capacity", "exact_rows"]
+                "fit_capacity", "exact_rows", "fit_upper_bound"]
         return dict(zip(keys, out.tolist()))
 
 
