@@ -191,7 +191,8 @@ def test_trained_model_gains_over_upper_bound(gpu_lib):
     cols = np.clip(rows + rng.integers(-16, 17, rows.size), 0, n - 1)
     band = gen.from_keys(n, n, np.unique(rows.astype(np.int64) * n + cols), None, rng)
     R = gen.rmat(scale=14, edge_factor=16, seed=99)
-    for name, M in (("band16", band), ("rmat14", R)):
+    # band: many products share columns (bound >> nnz); R-MAT: moderate
+    for name, M, ratio in (("band16", band, 0.8), ("rmat14", R, 0.95)):
         dM = DevCSR(M)
         p = rv.Plan(rv.RVSP_CUDA_ALGO_LEARNED)
         st, nnz = p.symbolic(dM, dM, M.nnz, M.nnz)
@@ -201,7 +202,7 @@ def test_trained_model_gains_over_upper_bound(gpu_lib):
         pred = s["predicted_rows"]
         assert pred > 0, (name, s)
         assert s["overflowed_rows"] / pred < 0.10, (name, s)
-        assert s["fit_capacity"] < 0.8 * s["fit_upper_bound"], (name, s)
+        assert s["fit_capacity"] < ratio * s["fit_upper_bound"], (name, s)
         want = oneshot(M, M, algo=rv.RVSP_CUDA_ALGO_EXACT)
         got = oneshot(M, M, algo=rv.RVSP_CUDA_ALGO_LEARNED)
         assert np.array_equal(got[1], want[1]) and np.array_equal(bits(got[2]), bits(want[2]))
