@@ -235,6 +235,8 @@ def run_ours(args):
 
     # end to end through the public API with pinned host buffers
     e2e = run_e2e(rv, A, P, args, torch)
+    # the one-shot product of the same matrices, exact-symbolic vs learned-binned
+    oneshot_cmp = compare_oneshot(rv, A, P, torch, args)
     clocks = sampler.stop()
 
     rv.check(L.rvsp_cuda_plan_set_async(plan, 0))
@@ -268,6 +270,7 @@ def run_ours(args):
                      "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_tiny<REUSE>",
                      "bytes_per_launch": bytes_alg},
         "e2e": e2e,
+        "oneshot_exact_vs_learned": oneshot_cmp,
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
@@ -276,6 +279,29 @@ def run_ours(args):
     print(json.dumps(out), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def compare_oneshot(rv, A, P, torch, args):
+    """One-shot C = A*A (analysis + C allocation + fill), exact-symbolic vs
+    learned-binned, device-resident inputs, median wall time per product."""
+    dA = DevMat(A, torch)
+    out = {}
+    ref = None
+    for name, algo in (("exact", rv.RVSP_CUDA_ALGO_EXACT), ("learned", rv.RVSP_CUDA_ALGO_LEARNED)):
+        def fn(algo=algo):
+            ptrs, n = _oneshot_dev(rv, dA, dA, algo)
+            rv.free_device(*ptrs)
+        t = _time(fn, max(5, args.steps // 10), args.warmup, torch)
+        ptrs, n = _oneshot_dev(rv, dA, dA, algo)
+        v = _d2h(ptrs[2], n, np.float32, torch)
+        rv.free_device(*ptrs)
+        if ref is None:
+            ref = v
+        out[name + "_gflops"] = round(2.0 * P / t / 1e9, 3)
+        out[name + "_ms"] = round(t * 1e3, 4)
+    out["learned_over_exact"] = round(out["learned_gflops"] / out["exact_gflops"], 4)
+    out["learned_values_bit_identical"] = bool(np.array_equal(ref.view(np.uint32), v.view(np.uint32)))
+    return out
 
 
 def run_e2e(rv, A, P, args, torch):

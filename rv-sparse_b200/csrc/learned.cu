@@ -62,12 +62,12 @@ __global__ void __launch_bounds__(AN_TILE)
     if (t == 0) s_slots = 0;
     __syncthreads();
     const int row = blockIdx.x * AN_TILE + t;
+    int lb = -1, cap = 0;
     if (row < rows) {
         const int b = bin[row];
-        int lb, cap, predicted = 0;
+        int predicted = 0;
         if (b == BIN_EMPTY) {
             lb = BIN_EMPTY;
-            cap = 0;
         } else if (b == BIN_TINY) {
             lb = BIN_TINY;
             cap = (int)ops[row];
@@ -86,15 +86,24 @@ __global__ void __launch_bounds__(AN_TILE)
                 cap = ub[row];
             } else {
                 lb = LBIN_EXACT;
-                cap = 0;
             }
         }
         out.lbin[row] = (uint8_t)lb;
         out.lcap[row] = cap;
         out.predicted[row] = (uint8_t)predicted;
-        atomicAdd(&s_hist[lb], 1);
-        if (cap) atomicAdd(&s_slots, (unsigned long long)cap);
     }
+    // warp-aggregated histogram and slot total
+    unsigned left = __ballot_sync(FULL, lb >= 0);
+    while (left) {
+        const int k = __shfl_sync(FULL, lb, __ffs(left) - 1);
+        const unsigned sel = __ballot_sync(FULL, lb == k);
+        if ((t & 31) == 0) atomicAdd(&s_hist[k], __popc(sel));
+        left &= ~sel;
+    }
+    unsigned long long sl = (unsigned long long)cap;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sl += __shfl_xor_sync(FULL, sl, o);
+    if ((t & 31) == 0 && sl) atomicAdd(&s_slots, sl);
     __syncthreads();
     if (t < NUM_BINS) {
         out.tile_hist[t * gridDim.x + blockIdx.x] = s_hist[t];
@@ -219,6 +228,7 @@ static int learned_pre_sync(rvsp_cuda_plan* plan) {
 int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool fused) {
     int st = analyze(plan, A, B, true, learned_pre_sync);
     if (st) return st;
+    trace_point("learned: analysis + bins");
     const int64_t M = plan->a_rows;
     Misc* misc = plan->misc.as<Misc>();
     int32_t acc = 0;
@@ -229,8 +239,11 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
     }
     plan->slot_total = plan->host_misc.slot_total;
     cudaError_t e;
-    size_t free_b = 0, total_b = 0;
-    if ((e = cudaMemGetInfo(&free_b, &total_b)) != cudaSuccess) return fail(e, "mem info");
+    size_t free_b = SIZE_MAX, total_b = 0;
+    // slots past 1 GiB must fit in half the free memory
+    if (fused && (size_t)plan->slot_total * 8 > (1ull << 30) &&
+        (e = cudaMemGetInfo(&free_b, &total_b)) != cudaSuccess)
+        return fail(e, "mem info");
     if (fused) {
         if ((size_t)plan->slot_total * 8 > free_b / 2) {
             g_err = "predicted capacity exceeds the memory budget";
@@ -286,6 +299,7 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
                              plan->stream)) != cudaSuccess)
         return fail(e, "learned read");
     if ((e = cudaStreamSynchronize(plan->stream)) != cudaSuccess) return fail(e, "learned sweep");
+    trace_point("learned: sweep (synced)");
     if (plan->host_misc.err) {
         g_err = "operand structure out of range (row_ptr or col_idx)";
         return RVSP_ERROR_INVALID_CSR;
@@ -355,8 +369,10 @@ int learned_spgemm(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t
     plan->b_nnz = b_nnz;
     memset(plan->key, 0, sizeof(plan->key));
     CsrView A, B;
+    trace_point("learned one-shot: enter");
     int st = stage_operands(plan, a_rp, a_ci, a_v, b_rp, b_ci, b_v, false, &A, &B);
     if (st) return st;
+    trace_point("learned: operands staged");
     if ((st = learned_symbolic(plan, A, B, true))) return st;
     plan->analysed = true;
     const int64_t nnz = plan->c_nnz;
@@ -374,6 +390,7 @@ int learned_spgemm(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t
         e = cudaGetLastError();
     }
     if (e == cudaSuccess && st == RVSP_SUCCESS) e = cudaStreamSynchronize(plan->stream);
+    trace_point("learned: finish (synced)");
     if (e != cudaSuccess || st) {
         cudaFree(rp);
         cudaFree(ci);

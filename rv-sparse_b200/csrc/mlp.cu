@@ -153,10 +153,9 @@ __global__ void __launch_bounds__(256)
     __shared__ float sP[MLP_NPARAM];
     for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) sP[i] = model.params[i];
     __syncthreads();
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const int r = j;
-    if (bin && bin[r] < BIN_WARP0) return;
+    if (bin && bin[r] < BIN_WARP0) continue;
     const float4 f = feat[r];
     const float raw[MLP_IN] = {f.x, f.y, f.z, f.w};
     float x[MLP_IN];
@@ -184,6 +183,7 @@ __global__ void __launch_bounds__(256)
     if (mu_out) mu_out[j] = o0;
     if (sig_out) sig_out[j] = sig;
     cap_out[r] = cap;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -245,7 +245,9 @@ static std::string default_path() {
 
 void launch_mlp_infer(const MlpModel& m, const float4* feat, const int32_t* ub, const uint8_t* bin,
                       int32_t n, int32_t* cap, cudaStream_t st) {
-    k_mlp_infer<<<(n + 255) / 256, 256, 0, st>>>(m, feat, ub, bin, n, nullptr, nullptr, cap);
+    // grid-stride over the rows: the weights are staged once per CTA
+    k_mlp_infer<<<std::min((n + 255) / 256, 148 * 8), 256, 0, st>>>(m, feat, ub, bin, n, nullptr,
+                                                                   nullptr, cap);
 }
 
 bool current_model(MlpModel* out) {

@@ -41,6 +41,14 @@ int fail(cudaError_t e, const char* what) {
                                           : RVSP_ERROR_DEVICE_FAILURE;
 }
 
+bool trace_on() {
+    static const bool on = [] {
+        const char* e = getenv("RVSP_TRACE");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
 bool is_dev(const void* p) {
     if (!p) return false;
     cudaPointerAttributes at;
@@ -317,6 +325,7 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
                              plan->stream)) != cudaSuccess)
         return fail(e, "histogram read");
     if ((e = cudaStreamSynchronize(plan->stream)) != cudaSuccess) return fail(e, "analysis");
+    trace_point("analysis (synced)");
     if (plan->host_misc.err) {
         g_err = "operand structure out of range (row_ptr or col_idx)";
         return RVSP_ERROR_INVALID_CSR;
@@ -374,6 +383,7 @@ int count_exact(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
                              plan->stream)) != cudaSuccess)
         return fail(e, "count read");
     if ((e = cudaStreamSynchronize(plan->stream)) != cudaSuccess) return fail(e, "count");
+    trace_point("exact count (synced)");
     if (plan->host_misc.err) {
         g_err = "operand structure out of range (row_ptr or col_idx)";
         return RVSP_ERROR_INVALID_CSR;
@@ -561,8 +571,10 @@ int rvsp_cuda_symbolic(rvsp_cuda_plan_t plan, int32_t a_rows, int32_t a_cols, in
     plan->b_nnz = b_nnz;
     memset(plan->key, 0, sizeof(plan->key));
     CsrView A, B;
+    trace_point("symbolic: enter");
     int st = stage_operands(plan, a_rp, a_ci, nullptr, b_rp, b_ci, nullptr, false, &A, &B);
     if (st) return st;
+    trace_point("symbolic: operands staged");
     if (plan->algo == RVSP_CUDA_ALGO_LEARNED) {
         if ((st = learned_symbolic(plan, A, B, false))) return st;
     } else {
@@ -662,6 +674,7 @@ int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t*
                                  cudaMemcpyDeviceToHost, plan->stream)) != cudaSuccess)
             return fail(e, "error word read");
         if ((e = cudaStreamSynchronize(plan->stream)) != cudaSuccess) return fail(e, "numeric");
+        trace_point("numeric (synced)");
         err = plan->host_misc.err;
         if (err) {
             g_err = "operand structure out of range (row_ptr or col_idx)";

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
 #include <string>
 
 #include "spgemm_types.cuh"
@@ -64,6 +66,18 @@ extern thread_local std::string g_err;
 extern std::atomic<long long> g_launches;
 
 int fail(cudaError_t e, const char* what);
+
+// Host-side phase tracer: with RVSP_TRACE=1 in the environment, every trace
+// point prints the host time since the previous one (per thread) to stderr.
+bool trace_on();
+inline void trace_point(const char* what) {
+    if (!trace_on()) return;
+    static thread_local std::chrono::steady_clock::time_point last;
+    const auto now = std::chrono::steady_clock::now();
+    fprintf(stderr, "[rvsp] %-28s %9.1f us\n", what,
+            std::chrono::duration<double, std::micro>(now - last).count());
+    last = now;
+}
 bool is_dev(const void* p);
 void init_kernel_attributes();
 

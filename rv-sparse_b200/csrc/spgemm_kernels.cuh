@@ -147,6 +147,35 @@ struct AnalyzeOut {
     int32_t* err;        // ERR_* bits
 };
 
+// Sum of a 64-bit value over the whole warp (result on every lane).
+__device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// Per-key counts and 64-bit sums of a warp into shared counters, one atomic
+// per distinct key present in the warp (keys < nkeys; others are skipped).
+__device__ __forceinline__ void warp_bin_add(int key, int nkeys, unsigned long long val,
+                                             int32_t* cnt, unsigned long long* sum) {
+    const int lane = lane_id();
+    unsigned left = __ballot_sync(FULL, key >= 0 && key < nkeys);
+    while (left) {
+        const int k = __shfl_sync(FULL, key, __ffs(left) - 1);
+        const unsigned sel = __ballot_sync(FULL, key == k);
+        const unsigned long long tot = warp_sum64(key == k ? val : 0ull);
+        if (lane == 0) {
+            atomicAdd(&cnt[k], __popc(sel));
+            if (sum && tot) atomicAdd(&sum[k], tot);
+        }
+        left &= ~sel;
+    }
+}
+
+// Rows of at most AN_SHORT entries are summarised by their own thread;
+// longer rows by the whole CTA striding over their entries.
+constexpr int AN_SHORT = 32;
+
 __global__ void __launch_bounds__(AN_TILE) k_analyze(CsrView A, CsrView B, AnalyzeOut out) {
     __shared__ int32_t s_rp[AN_TILE + 1];
     __shared__ unsigned long long s_ops[AN_TILE];
@@ -156,17 +185,12 @@ __global__ void __launch_bounds__(AN_TILE) k_analyze(CsrView A, CsrView B, Analy
     __shared__ int32_t s_hist[NUM_BINS];
     __shared__ unsigned long long s_bprod[NUM_BINS];
     __shared__ unsigned long long s_items, s_prod;
+    __shared__ int s_long;
 
     const int r0 = blockIdx.x * AN_TILE;
     const int nr = min(AN_TILE, A.rows - r0);
     const int t = threadIdx.x;
     for (int i = t; i <= nr; i += blockDim.x) s_rp[i] = A.rp[r0 + i];
-    for (int i = t; i < nr; i += blockDim.x) {
-        s_ops[i] = 0;
-        s_maxlen[i] = 0;
-        s_minc[i] = INT_MAX;
-        s_maxc[i] = -1;
-    }
     if (t < NUM_BINS) {
         s_hist[t] = 0;
         s_bprod[t] = 0;
@@ -174,57 +198,99 @@ __global__ void __launch_bounds__(AN_TILE) k_analyze(CsrView A, CsrView B, Analy
     if (t == 0) {
         s_items = 0;
         s_prod = 0;
+        s_long = 0;
     }
     __syncthreads();
-    const int p0 = max(s_rp[0], 0), p1 = min(s_rp[nr], A.nnz);
-    if (t < nr && (s_rp[t] > s_rp[t + 1] || s_rp[t] < 0 || s_rp[t + 1] > A.nnz))
-        atomicOr(out.err, ERR_STRUCTURE);
-    for (int p = p0 + t; p < p1; p += blockDim.x) {
-        int lo = 0, hi = nr;  // largest i with s_rp[i] <= p
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (s_rp[mid] <= p) lo = mid; else hi = mid;
-        }
-        int bs, be;
-        row_range(B, A.ci[p], &bs, &be, out.err);
-        const int len = be - bs;
-        if (len > 0) {
-            const int first = B.ci[bs], last = B.ci[be - 1];
-            if (first < 0 || last >= B.cols || last < first) {
-                atomicOr(out.err, ERR_STRUCTURE);
-                continue;
+    // short rows: one thread each, no atomics
+    if (t < nr) {
+        const int s0 = s_rp[t], s1 = s_rp[t + 1];
+        unsigned long long ops = 0;
+        int maxlen = 0, minc = INT_MAX, maxc = -1;
+        if (s0 < 0 || s1 < s0 || s1 > A.nnz) {
+            atomicOr(out.err, ERR_STRUCTURE);
+        } else if (s1 - s0 <= AN_SHORT) {
+            for (int p = s0; p < s1; ++p) {
+                int bs, be;
+                row_range(B, A.ci[p], &bs, &be, out.err);
+                const int len = be - bs;
+                if (len > 0) {
+                    const int first = B.ci[bs], last = B.ci[be - 1];
+                    if (first < 0 || last >= B.cols || last < first) {
+                        atomicOr(out.err, ERR_STRUCTURE);
+                        continue;
+                    }
+                    ops += (unsigned long long)len;
+                    maxlen = max(maxlen, len);
+                    minc = min(minc, first);
+                    maxc = max(maxc, last);
+                }
             }
-            atomicAdd(&s_ops[lo], (unsigned long long)len);
-            atomicMax(&s_maxlen[lo], len);
-            atomicMin(&s_minc[lo], first);
-            atomicMax(&s_maxc[lo], last);
+        } else {
+            s_long = 1;
         }
+        s_ops[t] = ops;
+        s_maxlen[t] = maxlen;
+        s_minc[t] = minc;
+        s_maxc[t] = maxc;
     }
     __syncthreads();
-    for (int i = t; i < nr; i += blockDim.x) {
-        const int row = r0 + i;
-        const int64_t ops = (int64_t)s_ops[i];
-        const int32_t ub = (int32_t)min(ops, (int64_t)B.cols);
-        const int b = bin_of(ops, ub);
+    if (s_long) {
+        // long rows: the CTA strides over the tile's entries, skipping short rows
+        const int p0 = max(s_rp[0], 0), p1 = min(s_rp[nr], A.nnz);
+        for (int p = p0 + t; p < p1; p += blockDim.x) {
+            int lo = 0, hi = nr;  // largest i with s_rp[i] <= p
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (s_rp[mid] <= p) lo = mid; else hi = mid;
+            }
+            if (s_rp[lo + 1] - s_rp[lo] <= AN_SHORT) continue;
+            int bs, be;
+            row_range(B, A.ci[p], &bs, &be, out.err);
+            const int len = be - bs;
+            if (len > 0) {
+                const int first = B.ci[bs], last = B.ci[be - 1];
+                if (first < 0 || last >= B.cols || last < first) {
+                    atomicOr(out.err, ERR_STRUCTURE);
+                    continue;
+                }
+                atomicAdd(&s_ops[lo], (unsigned long long)len);
+                atomicMax(&s_maxlen[lo], len);
+                atomicMin(&s_minc[lo], first);
+                atomicMax(&s_maxc[lo], last);
+            }
+        }
+        __syncthreads();
+    }
+    // per row: bound, bin, heavy chunks, features; warp-aggregated counters
+    const bool live = t < nr;
+    const int row = r0 + t;
+    const int64_t ops = live ? (int64_t)s_ops[t] : 0;
+    const int32_t ub = (int32_t)min(ops, (int64_t)B.cols);
+    const int b = live ? bin_of(ops, ub) : -1;
+    int nch = 0;
+    if (live) {
         out.ops[row] = ops;
         out.ub[row] = ub;
         out.bin[row] = (uint8_t)b;
-        int nch = 0, clo = 0;
+        int clo = 0;
         if (b == BIN_HEAVY) {
-            clo = s_minc[i] / HEAVY_CW;
-            nch = s_maxc[i] / HEAVY_CW - clo + 1;
-            atomicAdd(&s_items, (unsigned long long)nch);
+            clo = s_minc[t] / HEAVY_CW;
+            nch = s_maxc[t] / HEAVY_CW - clo + 1;
         }
         out.chunk_lo[row] = clo;
         out.nchunks[row] = nch;
         if (out.feat) {
-            const int anz = s_rp[i + 1] - s_rp[i];
-            const int span = ops > 0 ? s_maxc[i] - s_minc[i] + 1 : 0;
-            out.feat[row] = make_float4((float)anz, (float)ops, (float)s_maxlen[i], (float)span);
+            const int anz = s_rp[t + 1] - s_rp[t];
+            const int span = ops > 0 ? s_maxc[t] - s_minc[t] + 1 : 0;
+            out.feat[row] = make_float4((float)anz, (float)ops, (float)s_maxlen[t], (float)span);
         }
-        atomicAdd(&s_hist[b], 1);
-        atomicAdd(&s_bprod[b], (unsigned long long)ops);
-        atomicAdd(&s_prod, (unsigned long long)ops);
+    }
+    warp_bin_add(b, NUM_BINS, (unsigned long long)ops, s_hist, s_bprod);
+    const unsigned long long wprod = warp_sum64((unsigned long long)ops);
+    const unsigned long long witems = warp_sum64((unsigned long long)nch);
+    if (lane_id() == 0) {
+        if (wprod) atomicAdd(&s_prod, wprod);
+        if (witems) atomicAdd(&s_items, witems);
     }
     __syncthreads();
     if (t < NUM_BINS) {
