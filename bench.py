@@ -267,7 +267,7 @@ def run_ours(args):
         "parity_first_pass_vs_reference": parity,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "traffic": traffic,
-                     "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_tiny<REUSE>",
+                     "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_tiny_reuse_map",
                      "bytes_per_launch": bytes_alg},
         "e2e": e2e,
         "oneshot_exact_vs_learned": oneshot_cmp,

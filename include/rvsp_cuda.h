@@ -71,6 +71,62 @@ RVSP_CUDA_API int rvsp_cuda_plan_set_async(rvsp_cuda_plan_t plan, int async);
 RVSP_CUDA_API void *rvsp_cuda_plan_stream(rvsp_cuda_plan_t plan);
 
 /*
+ * Runtime bin parameters. The reference fixes its kernel tunables at compile
+ * time (RVSP_CONTIG_MIN, rv-sparse src/kernels/spgemm/accum_contig_f32.c:18-19;
+ * RVSP_GATHER_MIN, accum_adaptive_f32.c:28-29; RVSP_SORT_INSERTION_LIMIT,
+ * rvsp_sort.h:17-18). Here the equivalent choices are per plan, as
+ * RVSP_CUDA_BIN_PARAMS int32 values:
+ *   [0] tiny_ops      rows with at most this many products run one thread
+ *                     per row (0..32); the others get a warp
+ *   [1] slack_shift   a warp row's hash table holds at least
+ *                     ub + (ub >> slack_shift) slots, ub = min(products, cols(B))
+ *                     (1..4: load factor at most 2/3, 4/5, 8/9, 16/17)
+ *   [2] warp_cap_max  largest warp hash table, a power of two in 64..4096;
+ *                     rows needing more are split into column chunks, a warp each
+ *   [3] heavy_cw_log2 log2 of the columns of one chunk (9..13)
+ * Defaults: 32, 2, 4096, 13. Results do not depend on the parameters (the
+ * pattern and the values are bit-identical under every valid setting); only
+ * the time does.
+ *
+ * set_params takes effect at the plan's next symbolic call and discards the
+ * current analysis (numeric fails until symbolic runs again). The default
+ * applies to plans created afterwards and to the one-shot and batched entry
+ * points; NULL restores the built-in default. Out-of-range values return
+ * RVSP_ERROR_INVALID_ARGUMENT.
+ */
+#define RVSP_CUDA_BIN_PARAMS 4
+RVSP_CUDA_API int rvsp_cuda_plan_set_params(rvsp_cuda_plan_t plan, const int32_t *params, int32_t n);
+RVSP_CUDA_API int rvsp_cuda_plan_get_params(rvsp_cuda_plan_t plan, int32_t *params, int32_t n);
+RVSP_CUDA_API int rvsp_cuda_set_default_params(const int32_t *params, int32_t n);
+RVSP_CUDA_API int rvsp_cuda_get_default_params(int32_t *params, int32_t n);
+
+/*
+ * Autotuner: symbolic analysis that first picks the plan's bin parameters
+ * for this product. Coordinate descent over the candidates of each parameter
+ * (warp_cap_max 1024/2048/4096, heavy_cw_log2 11/12/13 when the product has
+ * chunked rows, slack_shift 1/2/3, tiny_ops 16/32), each trial timing
+ * symbolic + a structure-filling numeric of the plan's own algorithm into
+ * scratch memory, best of `reps` runs (>= 1). The best parameters stay in
+ * the plan, which is left analysed with them exactly as after
+ * rvsp_cuda_symbolic (same outputs). Operand values are needed for the
+ * numeric trials. No reference counterpart (the reference has no runtime
+ * tuning; its choice of strategy is rvsp_spgemm_descr_set_algo,
+ * src/core/spgemm_descr.c:102-125).
+ *   params_out      RVSP_CUDA_BIN_PARAMS values of the choice (may be NULL)
+ *   trial_params    max_trials x RVSP_CUDA_BIN_PARAMS values tried (may be NULL)
+ *   trial_ms        milliseconds of each trial (may be NULL)
+ *   n_trials_out    trials run (may be NULL); at most max_trials are recorded
+ */
+RVSP_CUDA_API int rvsp_cuda_plan_autotune(rvsp_cuda_plan_t plan,
+                       int32_t a_rows, int32_t a_cols, int32_t a_nnz,
+                       const int32_t *a_row_ptr, const int32_t *a_col_idx, const float *a_values,
+                       int32_t b_rows, int32_t b_cols, int32_t b_nnz,
+                       const int32_t *b_row_ptr, const int32_t *b_col_idx, const float *b_values,
+                       int32_t reps, int32_t *params_out, int32_t *trial_params,
+                       float *trial_ms, int32_t max_trials, int32_t *n_trials_out,
+                       int64_t *c_nnz_out, size_t *ws_bytes_out);
+
+/*
  * Structure analysis. Replaces rvsp_symbolic_count
  * (rv-sparse src/kernels/spgemm/rvsp_symbolic.c:13-87) as called by
  * rvsp_spgemm_work_estimation (spgemm_descr.c:162-255): per-row op counts,

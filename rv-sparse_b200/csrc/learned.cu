@@ -54,7 +54,7 @@ struct LearnedBinsOut {
 __global__ void __launch_bounds__(AN_TILE)
     k_learned_bins(int32_t rows, const uint8_t* __restrict__ bin, const int64_t* __restrict__ ops,
                    const int32_t* __restrict__ ub, const int32_t* __restrict__ cap_pred,
-                   LearnedBinsOut out) {
+                   LearnedBinsOut out, BinParams P) {
     __shared__ int32_t s_hist[NUM_BINS];
     __shared__ unsigned long long s_slots;
     const int t = threadIdx.x;
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(AN_TILE)
             // the upper bound would; otherwise the row gets the bound's table
             // and a slot of ub entries, which cannot overflow
             const int c = max(cap_pred[row], 1);
-            const int pb = bin_of(64, c);  // table class of the prediction (ops > tiny)
+            const int pb = table_bin(c, P);  // table class of the prediction
             if (pb < b) {
                 lb = pb;
                 cap = c;
@@ -212,7 +212,7 @@ static int learned_pre_sync(rvsp_cuda_plan* plan) {
                       &misc->slot_total};
     k_learned_bins<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(
         (int32_t)M, plan->bin.as<uint8_t>(), plan->ops.as<int64_t>(), plan->ub.as<int32_t>(),
-        plan->pred_cap.as<int32_t>(), lo);
+        plan->pred_cap.as<int32_t>(), lo, plan->params);
     note_launch(plan, 1);
     return scan_counts(plan, plan->ltile_hist.as<int32_t>(), NUM_BINS * tiles, nullptr,
                        plan->ltile_off.as<int32_t>(), &misc->ltile_total);

@@ -153,36 +153,35 @@ __global__ void __launch_bounds__(256)
     __shared__ float sP[MLP_NPARAM];
     for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) sP[i] = model.params[i];
     __syncthreads();
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    const int r = j;
-    if (bin && bin[r] < BIN_WARP0) continue;
-    const float4 f = feat[r];
-    const float raw[MLP_IN] = {f.x, f.y, f.z, f.w};
-    float x[MLP_IN];
-    for (int i = 0; i < MLP_IN; ++i)
-        x[i] = (log2f(1.0f + raw[i]) - model.mean[i]) * model.inv_std[i];
-    float h1[MLP_H];
-    for (int h = 0; h < MLP_H; ++h) {
-        float z = sP[MLP_B1 + h];
-        for (int i = 0; i < MLP_IN; ++i) z += sP[MLP_W1 + h * MLP_IN + i] * x[i];
-        h1[h] = fmaxf(z, 0.0f);
-    }
-    float o0 = sP[MLP_B3], o1 = sP[MLP_B3 + 1];
-    for (int h = 0; h < MLP_H; ++h) {
-        float z = sP[MLP_B2 + h];
-        for (int k = 0; k < MLP_H; ++k) z += sP[MLP_W2 + h * MLP_H + k] * h1[k];
-        z = fmaxf(z, 0.0f);
-        o0 += sP[MLP_W3 + h] * z;
-        o1 += sP[MLP_W3 + MLP_H + h] * z;
-    }
-    const float sig = mlp_softplus(o1) + 1e-3f;
-    const int32_t u = ub[r];
-    const float e = fminf(o0 + model.z * sig, 30.0f);
-    int32_t cap = (int32_t)ceilf(exp2f(e) - 1.0f);
-    cap = u <= 0 ? 0 : min(max(cap, 1), u);
-    if (mu_out) mu_out[j] = o0;
-    if (sig_out) sig_out[j] = sig;
-    cap_out[r] = cap;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        if (bin && bin[r] < BIN_WARP0) continue;
+        const float4 f = feat[r];
+        const float raw[MLP_IN] = {f.x, f.y, f.z, f.w};
+        float x[MLP_IN];
+        for (int i = 0; i < MLP_IN; ++i)
+            x[i] = (log2f(1.0f + raw[i]) - model.mean[i]) * model.inv_std[i];
+        float h1[MLP_H];
+        for (int h = 0; h < MLP_H; ++h) {
+            float z = sP[MLP_B1 + h];
+            for (int i = 0; i < MLP_IN; ++i) z += sP[MLP_W1 + h * MLP_IN + i] * x[i];
+            h1[h] = fmaxf(z, 0.0f);
+        }
+        float o0 = sP[MLP_B3], o1 = sP[MLP_B3 + 1];
+        for (int h = 0; h < MLP_H; ++h) {
+            float z = sP[MLP_B2 + h];
+            for (int k = 0; k < MLP_H; ++k) z += sP[MLP_W2 + h * MLP_H + k] * h1[k];
+            z = fmaxf(z, 0.0f);
+            o0 += sP[MLP_W3 + h] * z;
+            o1 += sP[MLP_W3 + MLP_H + h] * z;
+        }
+        const float sig = mlp_softplus(o1) + 1e-3f;
+        const int32_t u = ub[r];
+        const float e = fminf(o0 + model.z * sig, 30.0f);
+        int32_t cap = (int32_t)ceilf(exp2f(e) - 1.0f);
+        cap = u <= 0 ? 0 : min(max(cap, 1), u);
+        if (mu_out) mu_out[r] = o0;
+        if (sig_out) sig_out[r] = sig;
+        cap_out[r] = cap;
     }
 }
 

@@ -320,7 +320,17 @@ rvsp_status_t rvsp_spgemm_work_estimation(rvsp_spgemm_descr_t descr, const rvsp_
     }
     int64_t nnz = 0;
     size_t ws = 0;
-    int cst = rvsp_cuda_symbolic(descr->plan, A->rows, A->cols, A->nnz, A->row_ptr, A->col_idx,
+    int cst;
+    /* RVSP_AUTOTUNE=1: pick the plan's bin parameters for this product first
+     * (the descriptor keeps them for its computes) */
+    const char *tune = getenv("RVSP_AUTOTUNE");
+    if (tune != NULL && tune[0] == '1' && A->values != NULL && B->values != NULL)
+        cst = rvsp_cuda_plan_autotune(descr->plan, A->rows, A->cols, A->nnz, A->row_ptr,
+                                      A->col_idx, (const float *)A->values, B->rows, B->cols,
+                                      B->nnz, B->row_ptr, B->col_idx, (const float *)B->values,
+                                      2, NULL, NULL, NULL, 0, NULL, &nnz, &ws);
+    else
+        cst = rvsp_cuda_symbolic(descr->plan, A->rows, A->cols, A->nnz, A->row_ptr, A->col_idx,
                                  B->rows, B->cols, B->nnz, B->row_ptr, B->col_idx, &nnz, &ws);
     if (cst != RVSP_SUCCESS)
         return (rvsp_status_t)cst;

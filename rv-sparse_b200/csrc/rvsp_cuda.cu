@@ -86,9 +86,11 @@ constexpr int warps_for() {
     return w > 8 ? 8 : (w < 1 ? 1 : w);
 }
 
-template <int MODE>
-constexpr int heavy_warps() {
-    return MODE == COUNT ? 8 : 2;
+// warps per CTA of the heavy kernel: as many per-warp accumulators as fit
+// in 64 KB, at most 8
+static int heavy_warps(int mode, int cw_log2) {
+    const int w = 65536 / heavy_smem_bytes(mode, 1 << cw_log2);
+    return w > 8 ? 8 : (w < 1 ? 1 : w);
 }
 
 // warps per CTA of the map-replay reuse kernel (a float per slot)
@@ -119,9 +121,7 @@ static void set_mode_attrs() {
     set_warp_attr<1024, MODE>();
     set_warp_attr<2048, MODE>();
     set_warp_attr<4096, MODE>();
-    constexpr int W = heavy_warps<MODE>();
-    cudaFuncSetAttribute(k_heavy<W, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         W * heavy_smem_bytes<MODE>());
+    cudaFuncSetAttribute(k_heavy<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
 }
 
 static std::once_flag g_attr_once;
@@ -132,6 +132,28 @@ void init_kernel_attributes() {
         set_mode_attrs<REUSE>();
         cudaGetLastError();
     });
+}
+
+static std::mutex g_params_mu;
+static BinParams g_default_params = DEFAULT_BIN_PARAMS;
+
+// RVSP_CUDA_BIN_PARAMS="tiny_ops,slack_shift,warp_cap_max,heavy_cw_log2" in
+// the environment replaces the built-in default at the first use (ignored
+// unless all four values parse and are in range).
+static std::once_flag g_params_env_once;
+
+BinParams default_params() {
+    std::call_once(g_params_env_once, [] {
+        const char* e = getenv("RVSP_CUDA_BIN_PARAMS");
+        BinParams p;
+        if (e && sscanf(e, "%d,%d,%d,%d", &p.tiny_ops, &p.slack_shift, &p.warp_cap_max,
+                        &p.heavy_cw_log2) == 4 && bin_params_valid(p)) {
+            std::lock_guard<std::mutex> lk(g_params_mu);
+            g_default_params = p;
+        }
+    });
+    std::lock_guard<std::mutex> lk(g_params_mu);
+    return g_default_params;
 }
 
 void note_launch(rvsp_cuda_plan* plan, int n) {
@@ -195,11 +217,12 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
                 default: launch_warp<4096, MODE>(plan, A, B, b, o); break;
             }
         } else if (plan->n_items > 0) {
-            constexpr int W = heavy_warps<MODE>();
+            const int cl = plan->params.heavy_cw_log2;
+            const int W = heavy_warps(MODE, cl);
             const int grid = (plan->n_items + W - 1) / W;
-            k_heavy<W, MODE><<<grid, W * 32, W * heavy_smem_bytes<MODE>(), plan->stream>>>(
+            k_heavy<MODE><<<grid, W * 32, W * heavy_smem_bytes(MODE, 1 << cl), plan->stream>>>(
                 A, B, plan->items.as<HeavyItem>(), plan->n_items, plan->item_cnt.as<int32_t>(),
-                o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, o.ctl);
+                o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, o.ctl, cl);
             note_launch(plan, 1);
         }
     }
@@ -315,7 +338,7 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
                    plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
                    features ? plan->feat.as<float4>() : nullptr, misc->hist,
                    plan->tile_hist.as<int32_t>(), misc->totals, misc->bin_prod, &misc->err};
-    k_analyze<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(A, B, out);
+    k_analyze<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(A, B, out, plan->params);
     note_launch(plan, 1);
     int st = scan_counts(plan, plan->tile_hist.as<int32_t>(), NUM_BINS * tiles, nullptr,
                          plan->tile_off.as<int32_t>(), &misc->tile_total);
@@ -512,6 +535,7 @@ int rvsp_cuda_plan_create(rvsp_cuda_plan_t* out, int algo) {
     rvsp_cuda_plan* p = new (std::nothrow) rvsp_cuda_plan();
     if (!p) return RVSP_ERROR_ALLOCATION_FAILED;
     p->algo = algo;
+    p->params = default_params();
     // A blocking stream: work the caller queued on the legacy default stream
     // (e.g. filling device-resident operands) is ordered before the plan's
     // kernels, and the caller's later default-stream work after them.
@@ -548,6 +572,65 @@ int rvsp_cuda_plan_set_async(rvsp_cuda_plan_t p, int async) {
 }
 
 void* rvsp_cuda_plan_stream(rvsp_cuda_plan_t p) { return p ? (void*)p->stream : nullptr; }
+
+static int params_from(const int32_t* v, int32_t n, BinParams* out) {
+    if (!v) return RVSP_ERROR_NULL_POINTER;
+    if (n < BIN_PARAMS_N) return RVSP_ERROR_INVALID_ARGUMENT;
+    const BinParams p{v[0], v[1], v[2], v[3]};
+    if (!bin_params_valid(p)) {
+        g_err = "bin parameters out of range";
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    }
+    *out = p;
+    return RVSP_SUCCESS;
+}
+
+static int params_to(const BinParams& p, int32_t* v, int32_t n) {
+    if (!v) return RVSP_ERROR_NULL_POINTER;
+    if (n < BIN_PARAMS_N) return RVSP_ERROR_INVALID_ARGUMENT;
+    v[0] = p.tiny_ops;
+    v[1] = p.slack_shift;
+    v[2] = p.warp_cap_max;
+    v[3] = p.heavy_cw_log2;
+    return RVSP_SUCCESS;
+}
+
+int rvsp_cuda_plan_set_params(rvsp_cuda_plan_t p, const int32_t* params, int32_t n) {
+    if (!p) return RVSP_ERROR_NULL_POINTER;
+    BinParams bp;
+    int st = params_from(params, n, &bp);
+    if (st) return st;
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    p->params = bp;
+    // the analysed bins and heavy items belong to the old parameters
+    p->analysed = false;
+    p->maps_ready = false;
+    p->filled = nullptr;
+    p->filled_host = nullptr;
+    reset_graph(p);
+    return RVSP_SUCCESS;
+}
+
+int rvsp_cuda_plan_get_params(rvsp_cuda_plan_t p, int32_t* params, int32_t n) {
+    if (!p) return RVSP_ERROR_NULL_POINTER;
+    return params_to(p->params, params, n);
+}
+
+int rvsp_cuda_set_default_params(const int32_t* params, int32_t n) {
+    (void)default_params();  // the environment's value is read first, then replaced
+    BinParams bp = DEFAULT_BIN_PARAMS;
+    if (params) {
+        int st = params_from(params, n, &bp);
+        if (st) return st;
+    }
+    std::lock_guard<std::mutex> lk(g_params_mu);
+    g_default_params = bp;
+    return RVSP_SUCCESS;
+}
+
+int rvsp_cuda_get_default_params(int32_t* params, int32_t n) {
+    return params_to(default_params(), params, n);
+}
 
 int rvsp_cuda_symbolic(rvsp_cuda_plan_t plan, int32_t a_rows, int32_t a_cols, int32_t a_nnz,
                        const int32_t* a_rp, const int32_t* a_ci, int32_t b_rows, int32_t b_cols,

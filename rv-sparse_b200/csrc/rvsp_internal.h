@@ -80,6 +80,7 @@ inline void trace_point(const char* what) {
 }
 bool is_dev(const void* p);
 void init_kernel_attributes();
+BinParams default_params();  // the process-wide default of new and internal plans
 
 }  // namespace rvsp
 
@@ -90,6 +91,9 @@ struct rvsp_cuda_plan {
     bool analysed = false;
     bool capturing = false;
     int32_t a_rows = 0, a_cols = 0, a_nnz = 0, b_rows = 0, b_cols = 0, b_nnz = 0;
+    // bin parameters of the next analysis (the plan's own once set, else the
+    // process default at plan creation)
+    rvsp::BinParams params = rvsp::DEFAULT_BIN_PARAMS;
 
     // staging copies of host-resident operands; key[] holds the host
     // pointers of the staged index arrays (a_rp, a_ci, b_rp, b_ci)

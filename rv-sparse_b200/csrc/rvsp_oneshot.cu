@@ -88,6 +88,7 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
         if ((st = rvsp_cuda_plan_create(&plan, algo))) return st;
         plan->map_policy = 0;  // a one-shot product is never reused
     }
+    plan->params = default_params();
     const bool dev = is_dev(a_rp);
     keep_pool_memory();
 

@@ -176,7 +176,8 @@ __device__ __forceinline__ void warp_bin_add(int key, int nkeys, unsigned long l
 // longer rows by the whole CTA striding over their entries.
 constexpr int AN_SHORT = 32;
 
-__global__ void __launch_bounds__(AN_TILE) k_analyze(CsrView A, CsrView B, AnalyzeOut out) {
+__global__ void __launch_bounds__(AN_TILE)
+    k_analyze(CsrView A, CsrView B, AnalyzeOut out, BinParams P) {
     __shared__ int32_t s_rp[AN_TILE + 1];
     __shared__ unsigned long long s_ops[AN_TILE];
     __shared__ int32_t s_maxlen[AN_TILE];
@@ -266,7 +267,7 @@ __global__ void __launch_bounds__(AN_TILE) k_analyze(CsrView A, CsrView B, Analy
     const int row = r0 + t;
     const int64_t ops = live ? (int64_t)s_ops[t] : 0;
     const int32_t ub = (int32_t)min(ops, (int64_t)B.cols);
-    const int b = live ? bin_of(ops, ub) : -1;
+    const int b = live ? bin_of(ops, ub, P) : -1;
     int nch = 0;
     if (live) {
         out.ops[row] = ops;
@@ -274,8 +275,8 @@ __global__ void __launch_bounds__(AN_TILE) k_analyze(CsrView A, CsrView B, Analy
         out.bin[row] = (uint8_t)b;
         int clo = 0;
         if (b == BIN_HEAVY) {
-            clo = s_minc[t] / HEAVY_CW;
-            nch = s_maxc[t] / HEAVY_CW - clo + 1;
+            clo = s_minc[t] >> P.heavy_cw_log2;
+            nch = (s_maxc[t] >> P.heavy_cw_log2) - clo + 1;
         }
         out.chunk_lo[row] = clo;
         out.nchunks[row] = nch;
@@ -870,78 +871,100 @@ __global__ void __launch_bounds__(WARPS * 32)
 }
 
 // ---------------------------------------------------------------------------
-// Heavy rows: one warp per (row, chunk of HEAVY_CW columns). The warp walks
-// the row's A entries in order; for each B row that reaches the chunk it
-// locates the chunk's sub-range and adds the products into a dense
-// accumulator (distinct columns within one B row, so no two lanes collide).
+// Heavy rows: one warp per (row, chunk of cw = 2^cw_log2 columns). The warp
+// walks the row's A entries 32 at a time; each lane finds the part of its B
+// row that falls in the chunk (a binary search only when the B row straddles
+// a chunk edge), and the warp then walks the flattened in-chunk products 32
+// at a time, in A-row order, into a dense accumulator of cw floats and a
+// presence bitmap. Same-column products of one step combine in lane order
+// (ordered_add), so each column's sum keeps the reference's order. The A row
+// is re-read once per chunk; the products are read once in all.
 // ---------------------------------------------------------------------------
-template <int MODE>
-__host__ __device__ constexpr int heavy_smem_bytes() {
-    return (MODE == COUNT ? 0 : 4 * HEAVY_CW) + (MODE == REUSE ? 0 : HEAVY_CW / 8);
+__host__ __device__ constexpr int heavy_smem_bytes(int mode, int cw) {
+    return (mode == COUNT ? 0 : 4 * cw) + (mode == REUSE ? 0 : cw / 8);
 }
 
-template <int WARPS, int MODE>
-__global__ void __launch_bounds__(WARPS * 32)
+// First index in [lo, hi) with a[idx] >= target (hi if none); one thread.
+__device__ __forceinline__ int seq_lower_bound(const int32_t* __restrict__ a, int lo, int hi,
+                                               int target) {
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (__ldg(a + mid) < target) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256)
     k_heavy(CsrView A, CsrView B, const HeavyItem* __restrict__ items, int nitems,
             int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
             const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
             int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err,
-            RowCtl ctl) {
+            RowCtl ctl, int cw_log2) {
     extern __shared__ __align__(16) unsigned char smem[];
-    constexpr int NW = HEAVY_CW / 32;
+    const int cw = 1 << cw_log2;
+    const int nw = cw >> 5;  // bitmap words
+    const int warps = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = lane_id();
-    unsigned char* mine = smem + warp * heavy_smem_bytes<MODE>();
+    unsigned char* mine = smem + warp * heavy_smem_bytes(MODE, cw);
     float* acc = reinterpret_cast<float*>(mine);
-    unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * HEAVY_CW));
+    unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * cw));
 
-    for (int w = blockIdx.x * WARPS + warp; w < nitems; w += gridDim.x * WARPS) {
+    for (int w = blockIdx.x * warps + warp; w < nitems; w += gridDim.x * warps) {
         const HeavyItem it = items[w];
         const int row = it.row;
         if (ctl.only && !ctl.only[row]) continue;
-        const int lo = it.chunk * HEAVY_CW;
-        const int hi = min(lo + HEAVY_CW, B.cols);
-        if (MODE != COUNT)
-            for (int x = lane; x < HEAVY_CW; x += 32) acc[x] = 0.0f;
+        const int lo = it.chunk << cw_log2;
+        const int hi = (int)min((int64_t)lo + cw, (int64_t)B.cols);
+        if (MODE != COUNT) {
+            float4* a4 = reinterpret_cast<float4*>(acc);
+            for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
         if (MODE != REUSE)
-            for (int x = lane; x < NW; x += 32) bits[x] = 0u;
+            for (int x = lane; x < nw; x += 32) bits[x] = 0u;
         __syncwarp();
         int a0, a1;
         row_range(A, row, &a0, &a1, err);
         for (int base = a0; base < a1; base += 32) {
             const int j = base + lane;
-            int bs = 0, be = 0;
+            int s = 0, len = 0;
             float av = 0.0f;
-            bool hit = false;
             if (j < a1) {
+                int bs, be;
                 row_range(B, A.ci[j], &bs, &be, err);
-                if (MODE != COUNT) av = A.v[j];
-                hit = be > bs && B.ci[be - 1] >= lo && B.ci[bs] < hi;
-            }
-            unsigned hm = __ballot_sync(FULL, hit);
-            while (hm) {
-                const int e = __ffs(hm) - 1;
-                hm &= hm - 1;
-                const int ebs = __shfl_sync(FULL, bs, e);
-                const int ebe = __shfl_sync(FULL, be, e);
-                const float eav = __shfl_sync(FULL, av, e);
-                const int s = warp_lower_bound(B.ci, ebs, ebe, lo);
-                const int t = warp_lower_bound(B.ci, s, ebe, hi);
-                for (int q = s + lane; q < t; q += 32) {
-                    const int col = B.ci[q] - lo;
-                    if ((unsigned)col >= (unsigned)HEAVY_CW) {
-                        atomicOr(err, ERR_STRUCTURE);
-                        continue;
+                if (be > bs) {
+                    const int first = __ldg(B.ci + bs), last = __ldg(B.ci + be - 1);
+                    if (last >= lo && first < hi) {
+                        s = first >= lo ? bs : seq_lower_bound(B.ci, bs, be, lo);
+                        const int t = last < hi ? be : seq_lower_bound(B.ci, s, be, hi);
+                        len = t - s;
+                        if (MODE != COUNT) av = A.v[j];
                     }
-                    if (MODE != REUSE) atomicOr(&bits[col >> 5], 1u << (col & 31));
-                    if (MODE != COUNT) acc[col] = __fadd_rn(acc[col], __fmul_rn(eav, B.v[q]));
                 }
+            }
+            const int incl = warp_incl_scan(len);
+            const int total = __shfl_sync(FULL, incl, 31);
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                const int p = f0 + lane;
+                const ProductRef pr = locate_product(p, incl, len, s, av);
+                int col = 0;
+                bool ok = false;
+                float prod = 0.0f;
+                if (p < total) {
+                    col = __ldg(B.ci + pr.q) - lo;
+                    ok = (unsigned)col < (unsigned)cw;
+                    if (!ok) atomicOr(err, ERR_STRUCTURE);  // B row not sorted
+                    else if (MODE != COUNT) prod = __fmul_rn(pr.a, __ldg(B.v + pr.q));
+                }
+                if (MODE != REUSE && ok) atomicOr(&bits[col >> 5], 1u << (col & 31));
+                if (MODE != COUNT) ordered_add(acc, ok ? col : 0, ok, prod);
                 __syncwarp();
             }
         }
         __syncwarp();
         if (MODE == COUNT) {
             int c = 0;
-            for (int x = lane; x < NW; x += 32) c += __popc(bits[x]);
+            for (int x = lane; x < nw; x += 32) c += __popc(bits[x]);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
             if (lane == 0) {
@@ -950,8 +973,8 @@ __global__ void __launch_bounds__(WARPS * 32)
             }
         } else if (MODE == FILL) {
             int64_t out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
-            for (int x0 = 0; x0 < NW; x0 += 32) {
-                unsigned word = bits[x0 + lane];
+            for (int x0 = 0; x0 < nw; x0 += 32) {
+                unsigned word = x0 + lane < nw ? bits[x0 + lane] : 0u;
                 const int pc = __popc(word);
                 const int incl = warp_incl_scan(pc);
                 int64_t pos = out + (incl - pc);
@@ -971,7 +994,7 @@ __global__ void __launch_bounds__(WARPS * 32)
             const int t = warp_lower_bound(c_ci, s, r1, hi);
             for (int q = s + lane; q < t; q += 32) {
                 const int col = c_ci[q] - lo;
-                c_v[q] = (unsigned)col < (unsigned)HEAVY_CW ? acc[col] : 0.0f;
+                c_v[q] = (unsigned)col < (unsigned)cw ? acc[col] : 0.0f;
             }
         }
         __syncwarp();

@@ -28,8 +28,12 @@ constexpr int ERR_STRUCTURE = 1;  // an operand's row pointer or column index is
 
 // ---------------------------------------------------------------------------
 // Bins. A row's upper bound ub = min(ops, b_cols) bounds its distinct columns.
+// Which rows go to which bin, how many threads a row gets and how large its
+// table is are runtime parameters of a plan (BinParams, chosen by the
+// autotuner or left at their defaults); the constants below are the
+// compiled limits those parameters range over.
 // ---------------------------------------------------------------------------
-constexpr int TINY_CAP = 32;      // thread-per-row: rows with ops <= 32
+constexpr int TINY_CAP = 32;      // thread-per-row rows hold at most 32 products
 constexpr int WARP_CAP_MIN = 64;  // warp-per-row hash tables: 64 .. 4096 slots
 constexpr int NUM_WARP_BINS = 7;
 constexpr int WARP_CAP_MAX = WARP_CAP_MIN << (NUM_WARP_BINS - 1);
@@ -38,8 +42,33 @@ constexpr int BIN_TINY = 1;
 constexpr int BIN_WARP0 = 2;
 constexpr int BIN_HEAVY = BIN_WARP0 + NUM_WARP_BINS;
 constexpr int NUM_BINS = BIN_HEAVY + 1;
-constexpr int HEAVY_CW = 8192;  // columns per heavy work item
+constexpr int HEAVY_CW_LOG2_MIN = 9;    // heavy column chunks: 512 ..
+constexpr int HEAVY_CW_LOG2_MAX = 13;   // .. 8192 columns per work item
 constexpr int AN_TILE = 256;    // rows per analysis / binning tile
+
+// Runtime bin parameters of a plan.
+//   tiny_ops       rows with at most tiny_ops products run one thread per row
+//                  (0 .. TINY_CAP); the others get a warp
+//   slack_shift    a warp row's hash table holds at least ub + (ub >> slack_shift)
+//                  slots (1 .. 4: load factor at most 2/3, 4/5, 8/9, 16/17)
+//   warp_cap_max   largest warp table (64 .. 4096, a power of two); rows that
+//                  need more are heavy: a warp per column chunk
+//   heavy_cw_log2  log2 of the columns per heavy work item (9 .. 13)
+struct BinParams {
+    int32_t tiny_ops;
+    int32_t slack_shift;
+    int32_t warp_cap_max;
+    int32_t heavy_cw_log2;
+};
+constexpr int BIN_PARAMS_N = 4;
+constexpr BinParams DEFAULT_BIN_PARAMS = {TINY_CAP, 2, WARP_CAP_MAX, HEAVY_CW_LOG2_MAX};
+
+__host__ __device__ inline bool bin_params_valid(const BinParams& p) {
+    const bool pow2 = p.warp_cap_max > 0 && (p.warp_cap_max & (p.warp_cap_max - 1)) == 0;
+    return p.tiny_ops >= 0 && p.tiny_ops <= TINY_CAP && p.slack_shift >= 1 && p.slack_shift <= 4 &&
+           pow2 && p.warp_cap_max >= WARP_CAP_MIN && p.warp_cap_max <= WARP_CAP_MAX &&
+           p.heavy_cw_log2 >= HEAVY_CW_LOG2_MIN && p.heavy_cw_log2 <= HEAVY_CW_LOG2_MAX;
+}
 
 struct HeavyItem {
     int32_t row;
@@ -66,16 +95,22 @@ struct RowCtl {
     int learned;
 };
 
-__host__ __device__ inline int bin_of(int64_t ops, int32_t ub) {
-    if (ub <= 0) return BIN_EMPTY;
-    if (ops <= TINY_CAP) return BIN_TINY;
-    int64_t need = (int64_t)ub + (ub >> 2);  // load factor <= 0.8
+// Table bin of a warp row holding up to ub distinct columns: the smallest
+// warp table with ub + (ub >> slack_shift) slots, BIN_HEAVY past warp_cap_max.
+__host__ __device__ inline int table_bin(int32_t ub, const BinParams& p) {
+    const int64_t need = (int64_t)ub + (ub >> p.slack_shift);
     int cap = WARP_CAP_MIN, b = BIN_WARP0;
-    while (cap < need && b < BIN_HEAVY) {
+    while (cap < need && cap < p.warp_cap_max) {
         cap <<= 1;
         ++b;
     }
-    return b;  // BIN_HEAVY when need > WARP_CAP_MAX
+    return cap < need ? BIN_HEAVY : b;
+}
+
+__host__ __device__ inline int bin_of(int64_t ops, int32_t ub, const BinParams& p) {
+    if (ub <= 0) return BIN_EMPTY;
+    if (ops <= p.tiny_ops) return BIN_TINY;
+    return table_bin(ub, p);
 }
 
 }  // namespace rvsp

@@ -118,12 +118,23 @@ _PROTOS = {
     "rvsp_cuda_plan_row_stats": (C.c_int, [_VP, _VP, _VP, _VP, _I32]),
     "rvsp_cuda_plan_learned_stats": (C.c_int, [_VP, _VP, _I32]),
     "rvsp_cuda_row_ptr_noalloc": (C.c_int, [_VP, _I32, _VP, C.POINTER(_I64), _VP]),
+    "rvsp_cuda_plan_set_params": (C.c_int, [_VP, _VP, _I32]),
+    "rvsp_cuda_plan_get_params": (C.c_int, [_VP, _VP, _I32]),
+    "rvsp_cuda_set_default_params": (C.c_int, [_VP, _I32]),
+    "rvsp_cuda_get_default_params": (C.c_int, [_VP, _I32]),
+    "rvsp_cuda_plan_autotune": (C.c_int, [_VP, _I32, _I32, _I32, _VP, _VP, _VP, _I32, _I32, _I32,
+                                          _VP, _VP, _VP, _I32, _VP, _VP, _VP, _I32,
+                                          C.POINTER(_I32), C.POINTER(_I64),
+                                          C.POINTER(C.c_size_t)]),
     "rvsp_cuda_spgemm_batched_f32": (C.c_int, [C.c_int, _I32, _VP, _VP, _VP, _VP, _VP,
                                                _VP, _VP, _VP, _VP, _VP, _VP,
                                                C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
                                                C.POINTER(_I64), _VP]),
 }
 
+BIN_PARAMS = 4  # tiny_ops, slack_shift, warp_cap_max, heavy_cw_log2
+BIN_PARAM_NAMES = ("tiny_ops", "slack_shift", "warp_cap_max", "heavy_cw_log2")
+DEFAULT_BIN_PARAMS = (32, 2, 4096, 13)
 MLP_PARAMS = 1282
 MLP_FLOATS = 1291  # [mean(4), inv_std(4), z, params(1282)]
 
@@ -299,6 +310,36 @@ class Plan:
                                         ptr(B.row_ptr), ptr(B.col_idx), ptr(B.values), ptr(c_rp),
                                         ptr(c_ci), ptr(c_v), 1 if fill else 0, None)
 
+    def set_params(self, params):
+        """Bin parameters (BIN_PARAM_NAMES order) for the next symbolic call."""
+        v = np.asarray(params, np.int32)
+        return self.L.rvsp_cuda_plan_set_params(self.h, v.ctypes.data, v.size)
+
+    def get_params(self):
+        v = np.zeros(BIN_PARAMS, np.int32)
+        check(self.L.rvsp_cuda_plan_get_params(self.h, v.ctypes.data, BIN_PARAMS), "get_params")
+        return tuple(int(x) for x in v)
+
+    def autotune(self, A, B, reps=2, max_trials=16):
+        """Symbolic analysis after choosing the bin parameters for A * B.
+
+        Returns (status, nnz(C), chosen parameters, [(parameters, ms), ...])."""
+        best = np.zeros(BIN_PARAMS, np.int32)
+        tp = np.zeros((max_trials, BIN_PARAMS), np.int32)
+        tms = np.zeros(max_trials, np.float32)
+        ntr = C.c_int32()
+        nnz = C.c_int64()
+        ws = C.c_size_t()
+        st = self.L.rvsp_cuda_plan_autotune(
+            self.h, A.rows, A.cols, int(A.row_ptr[-1]), ptr(A.row_ptr), ptr(A.col_idx),
+            ptr(A.values), B.rows, B.cols, int(B.row_ptr[-1]), ptr(B.row_ptr), ptr(B.col_idx),
+            ptr(B.values), reps, best.ctypes.data, tp.ctypes.data, tms.ctypes.data, max_trials,
+            C.byref(ntr), C.byref(nnz), C.byref(ws))
+        self.rows = A.rows
+        n = min(ntr.value, max_trials)
+        trials = [(tuple(int(x) for x in tp[i]), float(tms[i])) for i in range(n)]
+        return st, nnz.value, tuple(int(x) for x in best), trials
+
     def row_stats(self):
         n = self.rows
         feat = np.zeros((max(n, 1), 4), np.float32)
@@ -314,6 +355,21 @@ class Plan:
         keys = ["predicted_rows", "overflowed_rows", "exact_by_size_rows", "fit_nnz",
                 "fit_capacity", "exact_rows", "fit_upper_bound"]
         return dict(zip(keys, out.tolist()))
+
+
+def set_default_params(params=None):
+    """Process-wide bin parameters of new plans and of the one-shot and batched
+    entry points; None restores the built-in default."""
+    if params is None:
+        return lib().rvsp_cuda_set_default_params(None, 0)
+    v = np.asarray(params, np.int32)
+    return lib().rvsp_cuda_set_default_params(v.ctypes.data, v.size)
+
+
+def get_default_params():
+    v = np.zeros(BIN_PARAMS, np.int32)
+    check(lib().rvsp_cuda_get_default_params(v.ctypes.data, BIN_PARAMS), "get_default_params")
+    return tuple(int(x) for x in v)
 
 
 def model_to_vector(mean, inv_std, z, params):
