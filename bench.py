@@ -2,7 +2,7 @@
 """FP32 CSR SpGEMM benchmark on B200 (one process per GPU).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload poisson_reuse|plain|batched|tall_skinny]
+                    [--workload poisson_reuse|plain|batched|tall_skinny|rmat]
 
 Default workload (the descriptor-reuse case): C = A * A for the 5-point
 Laplacian on a 1024 x 1024 grid (N = 1,048,576, nnz(A) = 5,238,784,
@@ -23,6 +23,13 @@ Printed as one JSON line by rank 0:
           from the reference sources) on 1 host core, bounded sample
 With --impl reference the reference's CPU implementation is timed instead,
 on all host cores (row panels), with the same workload, metric and unit.
+
+The other workloads (--workload) print one JSON line of one-shot comparisons:
+exact-symbolic vs learned-binned, default vs autotuned bin parameters, and
+batched vs sequential products, with the FP32-vs-FP64 error of sampled rows.
+rmat is C = A * A for an R-MAT graph of 2^scale vertices (default 20, 16
+edges per vertex); its intermediate products exceed the int32 range of one
+CSR, so it runs as row panels of at most 2^31 - 1 products each.
 
 N > 1 (torchrun): every rank runs its own full-size product on its own GPU
 (independent products, no data-path collective; weak scaling); a gloo
@@ -452,6 +459,114 @@ def _d2h(ptr_, n, dtype, torch):
     return out
 
 
+class PanelView:
+    """Rows [r0, r1) of a device CSR: the row pointer is a view into the full
+    one, so its offsets index the full column and value arrays directly."""
+
+    def __init__(self, M, r0, r1):
+        self.rows, self.cols = r1 - r0, M.cols
+        self.row_ptr = M.row_ptr[r0:r1 + 1]
+        self.col_idx, self.values = M.col_idx, M.values
+
+
+def row_panels(ops, limit=(1 << 31) - 1):
+    """Contiguous row ranges whose products stay within limit (so nnz does)."""
+    cum = np.cumsum(ops)
+    out, r0, base = [], 0, 0
+    n = len(ops)
+    while r0 < n:
+        r1 = int(np.searchsorted(cum, base + limit, side="right"))
+        r1 = max(r1, r0 + 1)
+        out.append((r0, r1))
+        base = int(cum[r1 - 1])
+        r0 = r1
+    return out
+
+
+def run_rmat(args, rv, gen, torch):
+    """Power-law C = A * A by row panels: exact vs learned, default vs tuned."""
+    import oracle
+    t0 = time.time()
+    A = gen.rmat(scale=args.rmat_scale, edge_factor=16, seed=0)
+    ops = gen.row_products(A, A)
+    P = int(ops.sum())
+    panels = row_panels(ops)
+    log(f"rmat scale {args.rmat_scale}: {A.rows} rows, nnz {A.nnz}, {P} products, "
+        f"{len(panels)} panels, generated in {time.time() - t0:.1f} s")
+    dA = DevMat(A, torch)
+    views = [PanelView(dA, r0, r1) for r0, r1 in panels]
+    heavy = int(np.argmax([ops[r0:r1].sum() for r0, r1 in panels]))
+
+    def run_all(algo):
+        nnz = 0
+        for v in views:
+            ptrs, n = _oneshot_dev(rv, v, dA, algo)
+            rv.free_device(*ptrs)
+            nnz += n
+        return nnz
+
+    steps = max(1, min(args.steps, 3))
+    times = {}
+    nnz_c = run_all(rv.RVSP_CUDA_ALGO_EXACT)
+    for name, algo in (("exact", rv.RVSP_CUDA_ALGO_EXACT), ("learned", rv.RVSP_CUDA_ALGO_LEARNED)):
+        times[name] = _time(lambda algo=algo: run_all(algo), steps, 1, torch)
+    # autotune on the panel with the most products, then every panel under the choice
+    plan = rv.Plan()
+    st, _, best, trials = plan.autotune(views[heavy], dA, reps=1)
+    rv.check(st, "autotune")
+    plan.close()
+    rv.check(rv.set_default_params(best))
+    try:
+        for name, algo in (("tuned_exact", rv.RVSP_CUDA_ALGO_EXACT),
+                           ("tuned_learned", rv.RVSP_CUDA_ALGO_LEARNED)):
+            times[name] = _time(lambda algo=algo: run_all(algo), steps, 1, torch)
+        # misprediction rate of the learned sizing, judged by the exact recount
+        lp = rv.Plan(rv.RVSP_CUDA_ALGO_LEARNED)
+        st, lnnz = lp.symbolic(views[heavy], dA)
+        rv.check(st, "learned symbolic")
+        ls = lp.learned_stats()
+        lp.close()
+        # parity: sampled rows of the first and the heaviest panel, bit-exact
+        rng = np.random.default_rng(1)
+        ok, errs = True, []
+        for pi in sorted({0, heavy}):
+            r0, r1 = panels[pi]
+            for algo in (rv.RVSP_CUDA_ALGO_EXACT, rv.RVSP_CUDA_ALGO_LEARNED):
+                ptrs, n = _oneshot_dev(rv, views[pi], dA, algo)
+                rp = _d2h(ptrs[0], r1 - r0 + 1, np.int32, torch)
+                ci = _d2h(ptrs[1], n, np.int32, torch)
+                v = _d2h(ptrs[2], n, np.float32, torch)
+                rv.free_device(*ptrs)
+                for r in np.sort(rng.choice(np.arange(r0, r1), min(100, r1 - r0), replace=False)):
+                    srp, sci, sv = oracle.spgemm_f32(A, A, int(r), int(r) + 1)
+                    lo, hi = rp[r - r0], rp[r - r0 + 1]
+                    ok &= np.array_equal(sci, ci[lo:hi]) and \
+                        np.array_equal(sv.view(np.uint32), v[lo:hi].view(np.uint32))
+                    if algo == rv.RVSP_CUDA_ALGO_EXACT and sci.size:
+                        d = oracle.numeric_f64(A, A, srp, sci, int(r), int(r) + 1)
+                        errs.append(np.abs(v[lo:hi] - d) / np.maximum(np.abs(d), 1e-30))
+    finally:
+        rv.check(rv.set_default_params(None))
+    e = np.concatenate(errs) if errs else np.zeros(1)
+    g = {k: 2 * P / t / 1e9 for k, t in times.items()}
+    return {
+        "config": {"workload": f"rmat_scale{args.rmat_scale}_ef16_a0.57_b0.19_c0.19", "rows": A.rows,
+                   "nnz_a": A.nnz, "products": P, "nnz_c": nnz_c, "panels": len(panels),
+                   "max_row_products": int(ops.max())},
+        "gflops": g, "ms": {k: t * 1e3 for k, t in times.items()},
+        "learned_over_exact": times["exact"] / times["learned"],
+        "tuned_learned_over_exact": times["exact"] / times["tuned_learned"],
+        "tuned_params": list(best),
+        "autotune_trials": [[list(p), round(ms, 3)] for p, ms in trials],
+        "mispredict": {"panel": heavy, **ls,
+                       "rate": ls["underpredicted_rows"] / max(ls["predicted_rows"], 1),
+                       "rerun_rate": ls["overflowed_rows"] / max(ls["predicted_rows"], 1)},
+        "sampled_rows_bit_exact_vs_oracle": bool(ok),
+        "fp32_vs_fp64_rel_err": {"max": float(e.max()), "median": float(np.median(e)),
+                                 "p99": float(np.quantile(e, 0.99))},
+    }
+
+
 def run_compare(args):
     """One-shot exact vs learned (and batched vs sequential) on a BASELINE config."""
     import torch
@@ -510,6 +625,8 @@ def run_compare(args):
         e = np.concatenate(errs) if errs else np.zeros(1)
         res["fp32_vs_fp64_rel_err"] = {"max": float(e.max()), "median": float(np.median(e)),
                                        "p99": float(np.quantile(e, 0.99)), "rows_sampled": 400}
+    elif args.workload == "rmat":
+        res = run_rmat(args, rv, gen, torch)
     elif args.workload == "batched":
         pairs = gen.batched_uneven(count=args.batch_count)
         prods = [gen.products(A, B) for A, B in pairs]
@@ -572,7 +689,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson_reuse",
-                    choices=["poisson_reuse", "plain", "batched", "tall_skinny"])
+                    choices=["poisson_reuse", "plain", "batched", "tall_skinny", "rmat"])
+    ap.add_argument("--rmat-scale", type=int, default=20)
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--ts-rows", type=int, default=2_000_000)
     args = ap.parse_args()

@@ -14,6 +14,10 @@
  *     reference (rv-sparse include/rv_sparse_types.h:53-67).
  *   - Inputs are canonical CSR, unchecked (rv-sparse
  *     src/kernels/spgemm/rvsp_spgemm.h:12-17), except in rvsp_cuda_csr_check.
+ *   - A device-resident A may be a row panel of a larger CSR: row_ptr points
+ *     at the panel's first row and need not start at 0; its offsets index
+ *     col_idx and values directly (nnz arguments are then the end offset
+ *     row_ptr[rows]). This is how products too large for one int32 C run.
  *   - A plan is not thread-safe; different plans are independent.
  */
 
@@ -84,7 +88,7 @@ RVSP_CUDA_API void *rvsp_cuda_plan_stream(rvsp_cuda_plan_t plan);
  *   [2] warp_cap_max  largest warp hash table, a power of two in 64..4096;
  *                     rows needing more are split into column chunks, a warp each
  *   [3] heavy_cw_log2 log2 of the columns of one chunk (9..13)
- * Defaults: 32, 2, 4096, 13. Results do not depend on the parameters (the
+ * Defaults: 32, 2, 4096, 11. Results do not depend on the parameters (the
  * pattern and the values are bit-identical under every valid setting); only
  * the time does.
  *
@@ -103,7 +107,7 @@ RVSP_CUDA_API int rvsp_cuda_get_default_params(int32_t *params, int32_t n);
 /*
  * Autotuner: symbolic analysis that first picks the plan's bin parameters
  * for this product. Coordinate descent over the candidates of each parameter
- * (warp_cap_max 1024/2048/4096, heavy_cw_log2 11/12/13 when the product has
+ * (warp_cap_max 1024/2048/4096, heavy_cw_log2 10..13 when the product has
  * chunked rows, slack_shift 1/2/3, tiny_ops 16/32), each trial timing
  * symbolic + a structure-filling numeric of the plan's own algorithm into
  * scratch memory, best of `reps` runs (>= 1). The best parameters stay in
@@ -277,7 +281,10 @@ RVSP_CUDA_API int rvsp_cuda_plan_row_stats(rvsp_cuda_plan_t plan, float *feat_ou
  * [1] of those, rows that outgrew it, [2] rows too large for a table (exact
  * path), [3] sum of the counts, [4] sum of the predicted capacities and
  * [6] sum of the upper bounds of predicted rows that fit, [5] rows finished
- * by the exact path. */
+ * by the exact path, and (n >= 8) [7] rows sized by the prediction whose
+ * exact count exceeds the predicted capacity: the misprediction count. In a
+ * structure-filling numeric every such row is re-run ([7] == [1]); in the
+ * descriptor's count a row whose hash table still held it needs no re-run. */
 RVSP_CUDA_API int rvsp_cuda_plan_learned_stats(rvsp_cuda_plan_t plan, int64_t *out, int32_t n);
 
 /*

@@ -26,16 +26,16 @@ namespace {
 
 struct Knob {
     int32_t BinParams::*field;
-    int32_t cand[3];
+    int32_t cand[4];
     int n;
     bool heavy_only;  // matters only when the product has chunked rows
 };
 
 const Knob kKnobs[] = {
-    {&BinParams::warp_cap_max, {1024, 2048, 4096}, 3, false},
-    {&BinParams::heavy_cw_log2, {11, 12, 13}, 3, true},
-    {&BinParams::slack_shift, {1, 2, 3}, 3, false},
-    {&BinParams::tiny_ops, {16, 32, 0}, 2, false},
+    {&BinParams::warp_cap_max, {1024, 2048, 4096, 0}, 3, false},
+    {&BinParams::heavy_cw_log2, {10, 11, 12, 13}, 4, true},
+    {&BinParams::slack_shift, {1, 2, 3, 0}, 3, false},
+    {&BinParams::tiny_ops, {16, 32, 0, 0}, 2, false},
 };
 
 struct Scratch {

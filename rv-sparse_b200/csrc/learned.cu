@@ -123,7 +123,7 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
                        uint8_t* __restrict__ need,
                        int32_t* __restrict__ n_need, int64_t* __restrict__ stats) {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    bool nd = false, ovf = false, big = false, pr = false;
+    bool nd = false, ovf = false, big = false, pr = false, under = false;
     int64_t fitc = 0, fitcap = 0, fitub = 0;
     if (row < rows) {
         const int lb = lbin[row];
@@ -131,6 +131,7 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
         big = lb == LBIN_EXACT;
         ovf = lb >= BIN_WARP0 && lb < LBIN_EXACT && cnt[row] < 0;
         nd = big || ovf;
+        under = pr && (ovf || cnt[row] > lcap[row]);
         if (pr && !ovf) {
             fitc = cnt[row];
             fitcap = lcap[row];
@@ -140,7 +141,8 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
         if (nd) cnt[row] = 0;
     }
     const unsigned mn = __ballot_sync(FULL, nd), mo = __ballot_sync(FULL, ovf && pr),
-                   mb = __ballot_sync(FULL, big), mp = __ballot_sync(FULL, pr);
+                   mb = __ballot_sync(FULL, big), mp = __ballot_sync(FULL, pr),
+                   mu = __ballot_sync(FULL, under);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         fitc += __shfl_xor_sync(FULL, fitc, o);
@@ -155,6 +157,7 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
         if (fitc) atomicAdd((unsigned long long*)&stats[3], (unsigned long long)fitc);
         if (fitcap) atomicAdd((unsigned long long*)&stats[4], (unsigned long long)fitcap);
         if (fitub) atomicAdd((unsigned long long*)&stats[6], (unsigned long long)fitub);
+        if (mu) atomicAdd((unsigned long long*)&stats[7], (unsigned long long)__popc(mu));
     }
 }
 
@@ -311,7 +314,7 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
     plan->c_nnz = plan->host_misc.scan_total;
     // heavy rows sized by the prediction were never counted by column chunk
     plan->items_counted = plan->n_items == 0 || fused;
-    for (int i = 0; i < 7; ++i) plan->lstats[i] = plan->host_misc.lstats[i];
+    for (int i = 0; i < 8; ++i) plan->lstats[i] = plan->host_misc.lstats[i];
     plan->lstats[5] = plan->host_misc.n_need;
     return RVSP_SUCCESS;
 }
@@ -443,7 +446,7 @@ int rvsp_cuda_plan_learned_stats(rvsp_cuda_plan_t plan, int64_t* out, int32_t n)
     if (!plan || !out) return RVSP_ERROR_NULL_POINTER;
     if (n < 7) return RVSP_ERROR_INVALID_ARGUMENT;
     if (plan->algo != RVSP_CUDA_ALGO_LEARNED || !plan->analysed) return RVSP_ERROR_INVALID_ARGUMENT;
-    memcpy(out, plan->lstats, sizeof(plan->lstats));
+    memcpy(out, plan->lstats, sizeof(int64_t) * (n < 8 ? n : 8));
     return RVSP_SUCCESS;
 }
 

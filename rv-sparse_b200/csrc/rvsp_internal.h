@@ -46,7 +46,7 @@ struct Misc {
     int32_t n_need;            // learned path: rows sent to the exact path
     int32_t pad3;
     int64_t slot_total;        // learned path: sum of predicted capacities
-    int64_t lstats[7];         // learned path statistics (see rvsp_cuda_plan_learned_stats)
+    int64_t lstats[8];         // learned path statistics (see rvsp_cuda_plan_learned_stats)
     int64_t ltile_total;
 };
 
@@ -133,7 +133,7 @@ struct rvsp_cuda_plan {
     int32_t lcount[rvsp::NUM_BINS] = {};
     rvsp::BinOffsets loffs = {};
     int64_t slot_total = 0;
-    int64_t lstats[7] = {};   // see rvsp_cuda_plan_learned_stats
+    int64_t lstats[8] = {};   // see rvsp_cuda_plan_learned_stats
     rvsp::DevBuf pred_cap, slot_off, tmp_ci, tmp_v, row_flag;
 
     // numeric-only CUDA graph

@@ -106,6 +106,26 @@ __device__ __forceinline__ int smem_lower_bound(const int32_t* keys, int n, int3
 // vals[slot] += prod for every active lane, in lane order when several lanes
 // share a slot. Lanes hold consecutive products of the row's flattened
 // (A entry, B entry) sequence, so lane order is the reference's order.
+// Bits of an accumulator slot that no product has reached yet (a NaN that
+// the arithmetic below never stores: see acc_store).
+constexpr uint32_t ACC_EMPTY = 0xFFFFFFFFu;
+
+template <bool SENT>
+__device__ __forceinline__ float acc_load(const float* vals, int slot) {
+    const float v = vals[slot];
+    return (SENT && __float_as_uint(v) == ACC_EMPTY) ? 0.0f : v;
+}
+
+template <bool SENT>
+__device__ __forceinline__ void acc_store(float* vals, int slot, float v) {
+    // a NaN result with the sentinel's bits would read as "empty": store the
+    // canonical NaN instead
+    if (SENT && __float_as_uint(v) == ACC_EMPTY) v = __uint_as_float(0x7FFFFFFFu);
+    vals[slot] = v;
+}
+
+// With SENT, slots holding ACC_EMPTY count as +0.0f (the reference's start).
+template <bool SENT = false>
 __device__ __forceinline__ void ordered_add(float* vals, int slot, bool active, float prod) {
     const int lane = lane_id();
     const int key = active ? slot : (0x40000000 | lane);
@@ -113,12 +133,12 @@ __device__ __forceinline__ void ordered_add(float* vals, int slot, bool active, 
     const int n = __popc(peers);
     const int maxn = __reduce_max_sync(FULL, (unsigned)n);
     if (maxn == 1) {
-        if (active) vals[slot] = __fadd_rn(vals[slot], prod);
+        if (active) acc_store<SENT>(vals, slot, __fadd_rn(acc_load<SENT>(vals, slot), prod));
         return;
     }
     const int leader = __ffs(peers) - 1;
     const bool lead = active && lane == leader;
-    float acc = lead ? vals[slot] : 0.0f;
+    float acc = lead ? acc_load<SENT>(vals, slot) : 0.0f;
     unsigned m = peers;
     for (int r = 0; r < maxn; ++r) {
         const int src = m ? (__ffs(m) - 1) : lane;
@@ -126,7 +146,7 @@ __device__ __forceinline__ void ordered_add(float* vals, int slot, bool active, 
         if (lead && m) acc = __fadd_rn(acc, v);
         m &= m - 1;
     }
-    if (lead) vals[slot] = acc;
+    if (lead) acc_store<SENT>(vals, slot, acc);
 }
 // ---------------------------------------------------------------------------
 // Analysis: one CTA per tile of AN_TILE rows; threads stride over the tile's
@@ -387,6 +407,48 @@ __global__ void __launch_bounds__(TINY_TPB)
             c0 = c_rp[row];
             n = min((int)(c_rp[row + 1] - c0), TINY_CAP);
             for (int x = 0; x < n; ++x) COL(x) = c_ci[c0 + x];
+        } else if (MODE == FILL && !pm) {
+            // one walk: (column, product) pairs in A-row order, a stable
+            // insertion sort by column, then each run of equal columns summed
+            // left to right from +0.0f -- the reference's order per column
+            for (int p = a0; p < a1; ++p) {
+                const float a = A.v[p];
+                int q0, q1;
+                row_range(B, A.ci[p], &q0, &q1, err);
+                for (int q = q0; q < q1 && n < TINY_CAP; ++q) {
+                    COL(n) = B.ci[q];
+                    VAL(n) = __fmul_rn(a, B.v[q]);
+                    ++n;
+                }
+            }
+            for (int x = 1; x < n; ++x) {
+                const int key = COL(x);
+                const float v = VAL(x);
+                int y = x - 1;
+                while (y >= 0 && COL(y) > key) {
+                    COL(y + 1) = COL(y);
+                    VAL(y + 1) = VAL(y);
+                    --y;
+                }
+                COL(y + 1) = key;
+                VAL(y + 1) = v;
+            }
+            int m = 0;
+            for (int x = 0; x < n;) {
+                const int c = COL(x);
+                float acc = 0.0f;
+                for (; x < n && COL(x) == c; ++x) acc = __fadd_rn(acc, VAL(x));
+                COL(m) = c;
+                VAL(m) = acc;
+                ++m;
+            }
+            n = m;
+            if (ctl.slot_off) {
+                c0 = ctl.slot_off[row];
+                cnt[row] = n;
+            } else {
+                c0 = c_rp[row];
+            }
         } else {
             for (int p = a0; p < a1; ++p) {
                 int q0, q1;
@@ -417,7 +479,7 @@ __global__ void __launch_bounds__(TINY_TPB)
                 c0 = c_rp[row];
             }
         }
-        if (MODE != COUNT) {
+        if (MODE == REUSE || (MODE == FILL && pm)) {
             uint8_t* pp = pm ? pm + (list_off[i] - list_off[0]) : nullptr;
             for (int x = 0; x < n; ++x) VAL(x) = 0.0f;
             for (int p = a0; p < a1; ++p) {
@@ -571,8 +633,9 @@ __global__ void __launch_bounds__(TRM_WARPS * 32)
 // ---------------------------------------------------------------------------
 template <int CAP, int MODE>
 __host__ __device__ constexpr int warp_smem_bytes() {
-    // COUNT: keys; REUSE: keys + values; FILL: keys + values + radix histogram
-    return (MODE == COUNT ? 4 : 8) * CAP + (MODE == FILL ? 4 * 256 : 0);
+    // COUNT: keys; REUSE: keys + values; FILL: keys + values + radix
+    // histogram + the radix sort's ping-pong buffer
+    return (MODE == COUNT ? 4 : MODE == REUSE ? 8 : 12) * CAP + (MODE == FILL ? 4 * 256 : 0);
 }
 
 // Lane's product p of the current 32-entry A chunk: its B position and the
@@ -636,30 +699,21 @@ __device__ __forceinline__ void walk_products(const CsrView& A, const CsrView& B
     }
 }
 
-// Stable LSD radix sort of keys[0, n) ascending (8-bit digits of key - min,
-// as many passes as the key range needs), tmp[0, n) as the ping-pong buffer,
-// hist 256 ints. Ranks within a digit follow lane order chunk by chunk, so
-// each pass is stable. Result in keys.
-__device__ void warp_radix_sort(int32_t* keys, int32_t* tmp, int n, int32_t* hist) {
+// One warp's stable LSD radix sort of the 32-bit words keys[0, n) by the
+// 8-bit digits of (word - sub) >> base_shift, `passes` of them, with tmp[0, n)
+// as the ping-pong buffer and hist 256 ints. Ranks within a digit follow lane
+// order chunk by chunk, so each pass is stable. Result in keys.
+__device__ void warp_radix_sort_core(int32_t* keys, int32_t* tmp, int n, uint32_t sub,
+                                     int base_shift, int passes, int32_t* hist) {
     const int lane = lane_id();
-    if (n <= 1) return;
-    int mn = INT_MAX, mx = INT_MIN;
-    for (int i = lane; i < n; i += 32) {
-        mn = min(mn, keys[i]);
-        mx = max(mx, keys[i]);
-    }
-    mn = __reduce_min_sync(FULL, mn);
-    mx = __reduce_max_sync(FULL, mx);
-    const uint32_t range = (uint32_t)mx - (uint32_t)mn;
-    const int passes = range < (1u << 8) ? 1 : range < (1u << 16) ? 2 : range < (1u << 24) ? 3 : 4;
     int32_t* src = keys;
     int32_t* dst = tmp;
     for (int pass = 0; pass < passes; ++pass) {
-        const int shift = 8 * pass;
+        const int shift = base_shift + 8 * pass;
         for (int i = lane; i < 256; i += 32) hist[i] = 0;
         __syncwarp();
         for (int i = lane; i < n; i += 32)
-            atomicAdd(&hist[(((uint32_t)src[i] - (uint32_t)mn) >> shift) & 255], 1);
+            atomicAdd(&hist[(((uint32_t)src[i] - sub) >> shift) & 255], 1);
         __syncwarp();
         int v[8], s = 0;
 #pragma unroll
@@ -678,7 +732,7 @@ __device__ void warp_radix_sort(int32_t* keys, int32_t* tmp, int n, int32_t* his
             const int i = base + lane;
             const bool ok = i < n;
             const int32_t k = ok ? src[i] : 0;
-            const int d = ok ? (int)((((uint32_t)k - (uint32_t)mn) >> shift) & 255) : 256 + lane;
+            const int d = ok ? (int)((((uint32_t)k - sub) >> shift) & 255) : 256 + lane;
             const unsigned peers = __match_any_sync(FULL, d);
             const int leader = __ffs(peers) - 1;
             int start = 0;
@@ -698,6 +752,23 @@ __device__ void warp_radix_sort(int32_t* keys, int32_t* tmp, int n, int32_t* his
         for (int i = lane; i < n; i += 32) keys[i] = src[i];
         __syncwarp();
     }
+}
+
+// Keys[0, n) ascending: digits of key - min, as many passes as the key range
+// needs.
+__device__ void warp_radix_sort(int32_t* keys, int32_t* tmp, int n, int32_t* hist) {
+    const int lane = lane_id();
+    if (n <= 1) return;
+    int mn = INT_MAX, mx = INT_MIN;
+    for (int i = lane; i < n; i += 32) {
+        mn = min(mn, keys[i]);
+        mx = max(mx, keys[i]);
+    }
+    mn = __reduce_min_sync(FULL, mn);
+    mx = __reduce_max_sync(FULL, mx);
+    const uint32_t range = (uint32_t)mx - (uint32_t)mn;
+    const int passes = range < (1u << 8) ? 1 : range < (1u << 16) ? 2 : range < (1u << 24) ? 3 : 4;
+    warp_radix_sort_core(keys, tmp, n, (uint32_t)mn, 0, passes, hist);
 }
 
 // Medium rows: one warp per row, a CAP-slot shared-memory table per warp.
@@ -722,6 +793,7 @@ __global__ void __launch_bounds__(WARPS * 32)
     int32_t* keys = reinterpret_cast<int32_t*>(mine);
     float* vals = reinterpret_cast<float*>(keys + CAP);
     int32_t* hist = reinterpret_cast<int32_t*>(mine + 8 * CAP);
+    int32_t* sorttmp = reinterpret_cast<int32_t*>(mine + 8 * CAP + 4 * 256);  // FILL only
     volatile int32_t* vkeys = keys;
     // learned: a table that fills up means the row outgrew its predicted
     // capacity; the row is flagged for the exact path instead of an error
@@ -739,6 +811,94 @@ __global__ void __launch_bounds__(WARPS * 32)
             n = min(c_rp[row + 1] - (int)o, CAP);
             for (int x = lane; x < n; x += 32) keys[x] = c_ci[o + x];
         } else {
+            if (MODE == FILL && !pm) {
+                // One walk: each product finds or inserts its column's slot
+                // and is added to the slot's accumulator in A-row order; then
+                // the occupied slots are compacted and sorted by column as
+                // packed words (column - min) << 12 | compacted index, and the
+                // values are gathered through the index at write-out. Rows
+                // whose columns span 2^20 or more take the two-walk path below.
+                for (int x = lane; x < CAP; x += 32) {
+                    keys[x] = -1;
+                    vals[x] = 0.0f;
+                }
+                __syncwarp();
+                bool ovf = false;
+                walk_products<true>(A, B, a0, a1, err, [&](int, bool pv, int col, float bv, float av) {
+                    int slot = -1;
+                    bool inserted = false, ok = true;
+                    if (pv) {
+                        uint32_t h = hash_slot(col, LOG2CAP);
+                        ok = false;
+                        for (int probe = 0; probe < CAP; ++probe) {
+                            const int cur = vkeys[h];
+                            if (cur == col) {
+                                ok = true;
+                                break;
+                            }
+                            if (cur == -1) {
+                                const int old = atomicCAS(&keys[h], -1, col);
+                                if (old == -1 || old == col) {
+                                    inserted = old == -1;
+                                    ok = true;
+                                    break;
+                                }
+                            }
+                            h = (h + 1) & (CAP - 1);
+                        }
+                        if (ok) slot = (int)h;
+                        else if (!learned) atomicOr(err, ERR_STRUCTURE);
+                    }
+                    n += __popc(__ballot_sync(FULL, inserted));
+                    ordered_add(vals, slot, slot >= 0, __fmul_rn(av, bv));
+                    if (learned) ovf = __any_sync(FULL, !ok);
+                    return ovf;
+                });
+                __syncwarp();
+                if (learned && (ovf || n > ctl.slot_off[row + 1] - ctl.slot_off[row])) {
+                    if (lane == 0) cnt[row] = -1;
+                    continue;
+                }
+                int out = 0;
+                int mn = INT_MAX, mx = INT_MIN;
+                for (int b0 = 0; b0 < CAP; b0 += 32) {
+                    const int key = keys[b0 + lane];
+                    const float v = vals[b0 + lane];
+                    const bool occ = key != -1;
+                    const unsigned m = __ballot_sync(FULL, occ);
+                    __syncwarp();
+                    if (occ) {
+                        const int d = out + __popc(m & ((1u << lane) - 1));
+                        keys[d] = key;
+                        vals[d] = v;
+                        mn = min(mn, key);
+                        mx = max(mx, key);
+                    }
+                    out += __popc(m);
+                    __syncwarp();
+                }
+                mn = __reduce_min_sync(FULL, mn);
+                mx = __reduce_max_sync(FULL, mx);
+                const uint32_t range = n > 0 ? (uint32_t)mx - (uint32_t)mn : 0u;
+                if (range < (1u << 20) && n < 4096) {
+                    for (int x = lane; x < n; x += 32)
+                        keys[x] = (int32_t)((((uint32_t)keys[x] - (uint32_t)mn) << 12) | (uint32_t)x);
+                    __syncwarp();
+                    const int passes = range < (1u << 8) ? 1 : range < (1u << 16) ? 2 : 3;
+                    if (n > 1)
+                        warp_radix_sort_core(keys, sorttmp, n, 0u, 12, passes, hist);
+                    o = learned ? ctl.slot_off[row] : (int64_t)c_rp[row];
+                    for (int x = lane; x < n; x += 32) {
+                        const uint32_t w = (uint32_t)keys[x];
+                        c_ci[o + x] = (int32_t)((w >> 12) + (uint32_t)mn);
+                        c_v[o + x] = vals[w & 4095u];
+                    }
+                    if (learned && lane == 0) cnt[row] = n;
+                    __syncwarp();
+                    continue;
+                }
+                n = 0;  // wide row: start over on the two-walk path
+            }
             for (int x = lane; x < CAP; x += 32) keys[x] = -1;
             __syncwarp();
             bool ovf = false;
@@ -874,14 +1034,16 @@ __global__ void __launch_bounds__(WARPS * 32)
 // Heavy rows: one warp per (row, chunk of cw = 2^cw_log2 columns). The warp
 // walks the row's A entries 32 at a time; each lane finds the part of its B
 // row that falls in the chunk (a binary search only when the B row straddles
-// a chunk edge), and the warp then walks the flattened in-chunk products 32
-// at a time, in A-row order, into a dense accumulator of cw floats and a
-// presence bitmap. Same-column products of one step combine in lane order
-// (ordered_add), so each column's sum keeps the reference's order. The A row
-// is re-read once per chunk; the products are read once in all.
+// a chunk edge), and the warp then walks the flattened in-chunk products in
+// A-row order, two steps of 32 in flight. COUNT sets bits of a presence
+// bitmap; FILL and REUSE add into a dense accumulator of cw floats whose
+// untouched slots hold ACC_EMPTY (so FILL needs no bitmap: a slot is present
+// once a product reached it). Same-column products of one step combine in
+// lane order (ordered_add), so each column's sum keeps the reference's
+// order. The A row is re-read once per chunk; the products once in all.
 // ---------------------------------------------------------------------------
 __host__ __device__ constexpr int heavy_smem_bytes(int mode, int cw) {
-    return (mode == COUNT ? 0 : 4 * cw) + (mode == REUSE ? 0 : cw / 8);
+    return mode == COUNT ? cw / 8 : 4 * cw;
 }
 
 // First index in [lo, hi) with a[idx] >= target (hi if none); one thread.
@@ -903,12 +1065,12 @@ __global__ void __launch_bounds__(256)
             RowCtl ctl, int cw_log2) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int cw = 1 << cw_log2;
-    const int nw = cw >> 5;  // bitmap words
+    const int nw = cw >> 5;  // bitmap words (COUNT)
     const int warps = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = lane_id();
     unsigned char* mine = smem + warp * heavy_smem_bytes(MODE, cw);
     float* acc = reinterpret_cast<float*>(mine);
-    unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * cw));
+    unsigned* bits = reinterpret_cast<unsigned*>(mine);
 
     for (int w = blockIdx.x * warps + warp; w < nitems; w += gridDim.x * warps) {
         const HeavyItem it = items[w];
@@ -916,12 +1078,13 @@ __global__ void __launch_bounds__(256)
         if (ctl.only && !ctl.only[row]) continue;
         const int lo = it.chunk << cw_log2;
         const int hi = (int)min((int64_t)lo + cw, (int64_t)B.cols);
-        if (MODE != COUNT) {
-            float4* a4 = reinterpret_cast<float4*>(acc);
-            for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        if (MODE != REUSE)
+        if (MODE == COUNT) {
             for (int x = lane; x < nw; x += 32) bits[x] = 0u;
+        } else {
+            uint4* a4 = reinterpret_cast<uint4*>(acc);
+            for (int x = lane; x < (cw >> 2); x += 32)
+                a4[x] = make_uint4(ACC_EMPTY, ACC_EMPTY, ACC_EMPTY, ACC_EMPTY);
+        }
         __syncwarp();
         int a0, a1;
         row_range(A, row, &a0, &a1, err);
@@ -944,20 +1107,34 @@ __global__ void __launch_bounds__(256)
             }
             const int incl = warp_incl_scan(len);
             const int total = __shfl_sync(FULL, incl, 31);
-            for (int f0 = 0; f0 < total; f0 += 32) {
-                const int p = f0 + lane;
-                const ProductRef pr = locate_product(p, incl, len, s, av);
-                int col = 0;
-                bool ok = false;
-                float prod = 0.0f;
-                if (p < total) {
-                    col = __ldg(B.ci + pr.q) - lo;
-                    ok = (unsigned)col < (unsigned)cw;
-                    if (!ok) atomicOr(err, ERR_STRUCTURE);  // B row not sorted
-                    else if (MODE != COUNT) prod = __fmul_rn(pr.a, __ldg(B.v + pr.q));
+            for (int f0 = 0; f0 < total; f0 += 64) {
+                // two steps located and loaded before either is accumulated
+                const int p0 = f0 + lane, p1 = f0 + 32 + lane;
+                const ProductRef r0 = locate_product(p0, incl, len, s, av);
+                const ProductRef r1 = locate_product(p1, incl, len, s, av);
+                int c0 = 0, c1 = 0;
+                float b0 = 0.0f, b1 = 0.0f;
+                if (p0 < total) {
+                    c0 = __ldg(B.ci + r0.q) - lo;
+                    if (MODE != COUNT) b0 = __ldg(B.v + r0.q);
                 }
-                if (MODE != REUSE && ok) atomicOr(&bits[col >> 5], 1u << (col & 31));
-                if (MODE != COUNT) ordered_add(acc, ok ? col : 0, ok, prod);
+                if (p1 < total) {
+                    c1 = __ldg(B.ci + r1.q) - lo;
+                    if (MODE != COUNT) b1 = __ldg(B.v + r1.q);
+                }
+                const bool ok0 = p0 < total && (unsigned)c0 < (unsigned)cw;
+                const bool ok1 = p1 < total && (unsigned)c1 < (unsigned)cw;
+                if ((p0 < total && !ok0) || (p1 < total && !ok1))
+                    atomicOr(err, ERR_STRUCTURE);  // B row not sorted
+                if (MODE == COUNT) {
+                    if (ok0) atomicOr(&bits[c0 >> 5], 1u << (c0 & 31));
+                    if (ok1) atomicOr(&bits[c1 >> 5], 1u << (c1 & 31));
+                } else {
+                    ordered_add<true>(acc, ok0 ? c0 : 0, ok0, __fmul_rn(r0.a, b0));
+                    __syncwarp();
+                    if (f0 + 32 < total)
+                        ordered_add<true>(acc, ok1 ? c1 : 0, ok1, __fmul_rn(r1.a, b1));
+                }
                 __syncwarp();
             }
         }
@@ -973,20 +1150,16 @@ __global__ void __launch_bounds__(256)
             }
         } else if (MODE == FILL) {
             int64_t out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
-            for (int x0 = 0; x0 < nw; x0 += 32) {
-                unsigned word = x0 + lane < nw ? bits[x0 + lane] : 0u;
-                const int pc = __popc(word);
-                const int incl = warp_incl_scan(pc);
-                int64_t pos = out + (incl - pc);
-                while (word) {
-                    const int b = __ffs(word) - 1;
-                    word &= word - 1;
-                    const int col = (x0 + lane) * 32 + b;
-                    c_ci[pos] = lo + col;
-                    c_v[pos] = acc[col];
-                    ++pos;
+            for (int x0 = 0; x0 < cw; x0 += 32) {
+                const float v = acc[x0 + lane];
+                const bool present = __float_as_uint(v) != ACC_EMPTY;
+                const unsigned m = __ballot_sync(FULL, present);
+                if (present) {
+                    const int64_t pos = out + __popc(m & ((1u << lane) - 1));
+                    c_ci[pos] = lo + x0 + lane;
+                    c_v[pos] = v;
                 }
-                out += __shfl_sync(FULL, incl, 31);
+                out += __popc(m);
             }
         } else {
             const int r0 = c_rp[row], r1 = c_rp[row + 1];
@@ -994,7 +1167,7 @@ __global__ void __launch_bounds__(256)
             const int t = warp_lower_bound(c_ci, s, r1, hi);
             for (int q = s + lane; q < t; q += 32) {
                 const int col = c_ci[q] - lo;
-                c_v[q] = (unsigned)col < (unsigned)cw ? acc[col] : 0.0f;
+                c_v[q] = (unsigned)col < (unsigned)cw ? acc_load<true>(acc, col) : 0.0f;
             }
         }
         __syncwarp();

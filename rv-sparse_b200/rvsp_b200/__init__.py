@@ -134,7 +134,7 @@ _PROTOS = {
 
 BIN_PARAMS = 4  # tiny_ops, slack_shift, warp_cap_max, heavy_cw_log2
 BIN_PARAM_NAMES = ("tiny_ops", "slack_shift", "warp_cap_max", "heavy_cw_log2")
-DEFAULT_BIN_PARAMS = (32, 2, 4096, 13)
+DEFAULT_BIN_PARAMS = (32, 2, 4096, 11)
 MLP_PARAMS = 1282
 MLP_FLOATS = 1291  # [mean(4), inv_std(4), z, params(1282)]
 
@@ -350,10 +350,10 @@ class Plan:
         return feat[:n], cnt[:n], ub[:n]
 
     def learned_stats(self):
-        out = np.zeros(7, np.int64)
-        check(self.L.rvsp_cuda_plan_learned_stats(self.h, out.ctypes.data, 7), "learned_stats")
+        out = np.zeros(8, np.int64)
+        check(self.L.rvsp_cuda_plan_learned_stats(self.h, out.ctypes.data, 8), "learned_stats")
         keys = ["predicted_rows", "overflowed_rows", "exact_by_size_rows", "fit_nnz",
-                "fit_capacity", "exact_rows", "fit_upper_bound"]
+                "fit_capacity", "exact_rows", "fit_upper_bound", "underpredicted_rows"]
         return dict(zip(keys, out.tolist()))
 
 

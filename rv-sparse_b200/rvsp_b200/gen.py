@@ -188,11 +188,10 @@ def products(A: CSR, B: CSR) -> int:
 def row_products(A: CSR, B: CSR) -> np.ndarray:
     blen = np.diff(B.row_ptr.astype(np.int64))
     per = blen[A.col_idx] if A.nnz else np.zeros(0, np.int64)
-    out = np.zeros(A.rows, np.int64)
-    if A.nnz:
-        rows = np.repeat(np.arange(A.rows), np.diff(A.row_ptr.astype(np.int64)))
-        np.add.at(out, rows, per)
-    return out
+    if not A.nnz:
+        return np.zeros(A.rows, np.int64)
+    rows = np.repeat(np.arange(A.rows), np.diff(A.row_ptr.astype(np.int64)))
+    return np.bincount(rows, weights=per, minlength=A.rows).astype(np.int64)
 
 
 def scale_values(M: CSR, rng: np.random.Generator, lo: float = 0.5, hi: float = 1.5) -> CSR:
