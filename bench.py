@@ -157,12 +157,8 @@ def run_ours(args):
 
     import rvsp_b200 as rv
 
-    dist = None
-    if WORLD > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    from rvsp_b200 import ranks
+    dist = ranks.init("gloo", timeout_s=300)
     torch.cuda.set_device(0)
     torch.zeros(1, device="cuda")  # context current on this thread for both runtimes
     L = rv.lib()
@@ -219,8 +215,7 @@ def run_ours(args):
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    ranks.barrier(dist)
     torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
@@ -229,15 +224,10 @@ def run_ours(args):
         step(args.warmup + i, *evs[i])
     torch.cuda.synchronize()
     launches = rv.launch_count() - l0
-    if dist:
-        dist.barrier()
+    ranks.barrier(dist)
     times = [a.elapsed_time(b) for a, b in evs]  # ms
     ms = sum(times) / len(times)
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t[0])
+    ms_max = ranks.max_over_ranks(dist, ms)
     value = 2.0 * P * WORLD / (ms_max * 1e-3) / 1e9
 
     # end to end through the public API with pinned host buffers
@@ -248,8 +238,7 @@ def run_ours(args):
 
     rv.check(L.rvsp_cuda_plan_set_async(plan, 0))
     L.rvsp_cuda_plan_destroy(plan)
-    if dist:
-        dist.barrier()
+    ranks.barrier(dist)
     if RANK != 0:
         if dist:
             dist.destroy_process_group()
@@ -469,28 +458,17 @@ class PanelView:
         self.col_idx, self.values = M.col_idx, M.values
 
 
-def row_panels(ops, limit=(1 << 31) - 1):
-    """Contiguous row ranges whose products stay within limit (so nnz does)."""
-    cum = np.cumsum(ops)
-    out, r0, base = [], 0, 0
-    n = len(ops)
-    while r0 < n:
-        r1 = int(np.searchsorted(cum, base + limit, side="right"))
-        r1 = max(r1, r0 + 1)
-        out.append((r0, r1))
-        base = int(cum[r1 - 1])
-        r0 = r1
-    return out
-
-
 def run_rmat(args, rv, gen, torch):
     """Power-law C = A * A by row panels: exact vs learned, default vs tuned."""
     import oracle
+    from rvsp_b200 import ranks
+    dist = ranks.init("gloo", timeout_s=900)
     t0 = time.time()
     A = gen.rmat(scale=args.rmat_scale, edge_factor=16, seed=0)
     ops = gen.row_products(A, A)
     P = int(ops.sum())
-    panels = row_panels(ops)
+    # every rank computes its contiguous group of row panels (strong scaling)
+    panels = ranks.shard_panels(ranks.row_panels(ops), ops, RANK, WORLD)
     log(f"rmat scale {args.rmat_scale}: {A.rows} rows, nnz {A.nnz}, {P} products, "
         f"{len(panels)} panels, generated in {time.time() - t0:.1f} s")
     dA = DevMat(A, torch)
@@ -507,9 +485,14 @@ def run_rmat(args, rv, gen, torch):
 
     steps = max(1, min(args.steps, 3))
     times = {}
-    nnz_c = run_all(rv.RVSP_CUDA_ALGO_EXACT)
+    def timed(algo):
+        # all ranks start together; the job's time is the slowest rank's
+        ranks.barrier(dist)
+        return ranks.max_over_ranks(dist, _time(lambda: run_all(algo), steps, 1, torch))
+
+    nnz_c = ranks.sum_over_ranks(dist, run_all(rv.RVSP_CUDA_ALGO_EXACT))
     for name, algo in (("exact", rv.RVSP_CUDA_ALGO_EXACT), ("learned", rv.RVSP_CUDA_ALGO_LEARNED)):
-        times[name] = _time(lambda algo=algo: run_all(algo), steps, 1, torch)
+        times[name] = timed(algo)
     # autotune on the panel with the most products, then every panel under the choice
     plan = rv.Plan()
     st, _, best, trials = plan.autotune(views[heavy], dA, reps=1)
@@ -519,7 +502,7 @@ def run_rmat(args, rv, gen, torch):
     try:
         for name, algo in (("tuned_exact", rv.RVSP_CUDA_ALGO_EXACT),
                            ("tuned_learned", rv.RVSP_CUDA_ALGO_LEARNED)):
-            times[name] = _time(lambda algo=algo: run_all(algo), steps, 1, torch)
+            times[name] = timed(algo)
         # misprediction rate of the learned sizing, judged by the exact recount
         lp = rv.Plan(rv.RVSP_CUDA_ALGO_LEARNED)
         st, lnnz = lp.symbolic(views[heavy], dA)
@@ -551,8 +534,9 @@ def run_rmat(args, rv, gen, torch):
     g = {k: 2 * P / t / 1e9 for k, t in times.items()}
     return {
         "config": {"workload": f"rmat_scale{args.rmat_scale}_ef16_a0.57_b0.19_c0.19", "rows": A.rows,
-                   "nnz_a": A.nnz, "products": P, "nnz_c": nnz_c, "panels": len(panels),
+                   "nnz_a": A.nnz, "products": P, "nnz_c": nnz_c, "panels_this_rank": len(panels),
                    "max_row_products": int(ops.max())},
+        "n_gpus": WORLD, "scaling": "strong",
         "gflops": g, "ms": {k: t * 1e3 for k, t in times.items()},
         "learned_over_exact": times["exact"] / times["learned"],
         "tuned_learned_over_exact": times["exact"] / times["tuned_learned"],
@@ -679,7 +663,8 @@ def run_compare(args):
         res["batched_learned_over_sequential"] = times["sequential_exact"] / times["batched_learned"]
         res["batched_learned_over_batched_exact"] = times["batched_exact"] / times["batched_learned"]
         res["spot_check_bit_exact_vs_oracle"] = bool(ok)
-    print(json.dumps({"workload": args.workload, **res}), flush=True)
+    if RANK == 0:
+        print(json.dumps({"workload": args.workload, **res}), flush=True)
 
 
 def main():

@@ -660,10 +660,16 @@ __device__ __forceinline__ ProductRef locate_product(int p, int incl, int bl, in
     return ProductRef{e_bs + (p - (e_incl - e_bl)), e_av};
 }
 
-// Walks row [a0, a1) of A times B in the reference's product order, 32
-// products per warp step: f(k, pv, col, bv, av) runs on every lane for the
-// product with row-local index k (pv false on idle lanes), and returns a
-// warp-uniform "stop". VALUES loads B's and A's values too.
+// Walks row [a0, a1) of A times B in the reference's product order:
+// f(k, pv, col, bv, av, distinct) runs on every lane for the product with
+// row-local index k (pv false on idle lanes) and returns a warp-uniform
+// "stop". A's entries are taken 32 at a time; runs of short B rows are walked
+// flattened, 32 products per step spread over their entries (distinct false:
+// two lanes may hold the same column), and a B row of WALK_SEG or more
+// entries is walked on its own, 32 of its entries per step (distinct true:
+// the lanes' columns differ). VALUES loads B's and A's values too.
+constexpr int WALK_SEG = 12;
+
 template <bool VALUES, class F>
 __device__ __forceinline__ void walk_products(const CsrView& A, const CsrView& B, int a0, int a1,
                                               int32_t* err, F&& f) {
@@ -680,22 +686,52 @@ __device__ __forceinline__ void walk_products(const CsrView& A, const CsrView& B
             if (VALUES) av = A.v[j];
         }
         const int incl = warp_incl_scan(bl);
-        const int total = __shfl_sync(FULL, incl, 31);
-        for (int f0 = 0; f0 < total; f0 += 32) {
-            const int p = f0 + lane;
-            const bool pv = p < total;
-            const ProductRef pr = locate_product(p, incl, bl, bs, av);
-            int col = -1;
-            float bv = 0.0f;
-            if (pv) {
-                col = B.ci[pr.q];
-                if (VALUES) bv = B.v[pr.q];
+        const unsigned longm = __ballot_sync(FULL, bl >= WALK_SEG);
+        int e = 0;
+        while (e < 32) {
+            const unsigned rest = (longm >> e) << e;
+            const int nl = rest ? __ffs(rest) - 1 : 32;
+            if (nl > e) {
+                const int pstart = e > 0 ? __shfl_sync(FULL, incl, (e - 1) & 31) : 0;
+                const int pend = __shfl_sync(FULL, incl, nl - 1);
+                for (int f0 = pstart; f0 < pend; f0 += 32) {
+                    const int p = f0 + lane;
+                    const bool pv = p < pend;
+                    const ProductRef pr = locate_product(p, incl, bl, bs, av);
+                    int col = -1;
+                    float bv = 0.0f;
+                    if (pv) {
+                        col = B.ci[pr.q];
+                        if (VALUES) bv = B.v[pr.q];
+                    }
+                    const bool stop = f(before + p, pv, col, bv, pr.a, false);
+                    __syncwarp();
+                    if (stop) return;
+                }
+                e = nl;
             }
-            const bool stop = f(before + p, pv, col, bv, pr.a);
-            __syncwarp();
-            if (stop) return;
+            if (e < 32) {
+                const int se = __shfl_sync(FULL, bs, e);
+                const int le = __shfl_sync(FULL, bl, e);
+                const float ae = __shfl_sync(FULL, av, e);
+                const int kb = before + __shfl_sync(FULL, incl, e) - le;
+                for (int q0 = 0; q0 < le; q0 += 32) {
+                    const int q = q0 + lane;
+                    const bool pv = q < le;
+                    int col = -1;
+                    float bv = 0.0f;
+                    if (pv) {
+                        col = B.ci[se + q];
+                        if (VALUES) bv = B.v[se + q];
+                    }
+                    const bool stop = f(kb + q, pv, col, bv, ae, true);
+                    __syncwarp();
+                    if (stop) return;
+                }
+                ++e;
+            }
         }
-        before += total;
+        before += __shfl_sync(FULL, incl, 31);
     }
 }
 
@@ -824,7 +860,8 @@ __global__ void __launch_bounds__(WARPS * 32)
                 }
                 __syncwarp();
                 bool ovf = false;
-                walk_products<true>(A, B, a0, a1, err, [&](int, bool pv, int col, float bv, float av) {
+                walk_products<true>(A, B, a0, a1, err, [&](int, bool pv, int col, float bv, float av,
+                                                           bool distinct) {
                     int slot = -1;
                     bool inserted = false, ok = true;
                     if (pv) {
@@ -850,7 +887,11 @@ __global__ void __launch_bounds__(WARPS * 32)
                         else if (!learned) atomicOr(err, ERR_STRUCTURE);
                     }
                     n += __popc(__ballot_sync(FULL, inserted));
-                    ordered_add(vals, slot, slot >= 0, __fmul_rn(av, bv));
+                    if (distinct) {
+                        if (slot >= 0) vals[slot] = __fadd_rn(vals[slot], __fmul_rn(av, bv));
+                    } else {
+                        ordered_add(vals, slot, slot >= 0, __fmul_rn(av, bv));
+                    }
                     if (learned) ovf = __any_sync(FULL, !ok);
                     return ovf;
                 });
@@ -902,7 +943,7 @@ __global__ void __launch_bounds__(WARPS * 32)
             for (int x = lane; x < CAP; x += 32) keys[x] = -1;
             __syncwarp();
             bool ovf = false;
-            walk_products<false>(A, B, a0, a1, err, [&](int, bool pv, int col, float, float) {
+            walk_products<false>(A, B, a0, a1, err, [&](int, bool pv, int col, float, float, bool) {
                 bool inserted = false, ok = true;
                 if (pv) {
                     // at most CAP probes: a table can only fill up when an
@@ -961,13 +1002,18 @@ __global__ void __launch_bounds__(WARPS * 32)
         for (int x = lane; x < n; x += 32) vals[x] = 0.0f;
         __syncwarp();
         uint16_t* pp = (MODE == FILL && pm) ? pm + (list_off[w] - list_off[0]) : nullptr;
-        walk_products<true>(A, B, a0, a1, err, [&](int k, bool pv, int col, float bv, float av) {
+        walk_products<true>(A, B, a0, a1, err, [&](int k, bool pv, int col, float bv, float av,
+                                                   bool distinct) {
             int pos = -1;
             if (pv) {
                 pos = smem_lower_bound(keys, n, col);
                 if (pp) pp[k] = (uint16_t)pos;
             }
-            ordered_add(vals, pos, pv && pos < n, __fmul_rn(av, bv));
+            if (distinct) {
+                if (pv && pos < n) vals[pos] = __fadd_rn(vals[pos], __fmul_rn(av, bv));
+            } else {
+                ordered_add(vals, pos, pv && pos < n, __fmul_rn(av, bv));
+            }
             return false;
         });
         __syncwarp();
@@ -1042,6 +1088,8 @@ __global__ void __launch_bounds__(WARPS * 32)
 // lane order (ordered_add), so each column's sum keeps the reference's
 // order. The A row is re-read once per chunk; the products once in all.
 // ---------------------------------------------------------------------------
+constexpr int HEAVY_SEG = 12;  // in-chunk B segments this long are walked on their own
+
 __host__ __device__ constexpr int heavy_smem_bytes(int mode, int cw) {
     return mode == COUNT ? cw / 8 : 4 * cw;
 }
@@ -1106,36 +1154,86 @@ __global__ void __launch_bounds__(256)
                 }
             }
             const int incl = warp_incl_scan(len);
-            const int total = __shfl_sync(FULL, incl, 31);
-            for (int f0 = 0; f0 < total; f0 += 64) {
-                // two steps located and loaded before either is accumulated
-                const int p0 = f0 + lane, p1 = f0 + 32 + lane;
-                const ProductRef r0 = locate_product(p0, incl, len, s, av);
-                const ProductRef r1 = locate_product(p1, incl, len, s, av);
-                int c0 = 0, c1 = 0;
-                float b0 = 0.0f, b1 = 0.0f;
-                if (p0 < total) {
-                    c0 = __ldg(B.ci + r0.q) - lo;
-                    if (MODE != COUNT) b0 = __ldg(B.v + r0.q);
+            // Entries in order: a run of short in-chunk segments is walked
+            // flattened (products spread over the lanes, same-column products
+            // of a step combined in lane order); a segment of HEAVY_SEG or more
+            // products is walked with the lanes over its own columns, which
+            // are distinct, so it needs neither the product search nor the
+            // ordered combine.
+            const unsigned longm = __ballot_sync(FULL, len >= HEAVY_SEG);
+            int e = 0;
+            while (e < 32) {
+                const unsigned rest = (longm >> e) << e;
+                const int nl = rest ? __ffs(rest) - 1 : 32;
+                if (nl > e) {
+                    const int pstart = e > 0 ? __shfl_sync(FULL, incl, (e - 1) & 31) : 0;
+                    const int pend = __shfl_sync(FULL, incl, nl - 1);
+                    for (int f0 = pstart; f0 < pend; f0 += 64) {
+                        // two steps located and loaded before either is accumulated
+                        const int p0 = f0 + lane, p1 = f0 + 32 + lane;
+                        const ProductRef r0 = locate_product(p0, incl, len, s, av);
+                        const ProductRef r1 = locate_product(p1, incl, len, s, av);
+                        int c0 = 0, c1 = 0;
+                        float b0 = 0.0f, b1 = 0.0f;
+                        if (p0 < pend) {
+                            c0 = __ldg(B.ci + r0.q) - lo;
+                            if (MODE != COUNT) b0 = __ldg(B.v + r0.q);
+                        }
+                        if (p1 < pend) {
+                            c1 = __ldg(B.ci + r1.q) - lo;
+                            if (MODE != COUNT) b1 = __ldg(B.v + r1.q);
+                        }
+                        const bool ok0 = p0 < pend && (unsigned)c0 < (unsigned)cw;
+                        const bool ok1 = p1 < pend && (unsigned)c1 < (unsigned)cw;
+                        if ((p0 < pend && !ok0) || (p1 < pend && !ok1))
+                            atomicOr(err, ERR_STRUCTURE);  // B row not sorted
+                        if (MODE == COUNT) {
+                            if (ok0) atomicOr(&bits[c0 >> 5], 1u << (c0 & 31));
+                            if (ok1) atomicOr(&bits[c1 >> 5], 1u << (c1 & 31));
+                        } else {
+                            ordered_add<true>(acc, ok0 ? c0 : 0, ok0, __fmul_rn(r0.a, b0));
+                            __syncwarp();
+                            if (f0 + 32 < pend)
+                                ordered_add<true>(acc, ok1 ? c1 : 0, ok1, __fmul_rn(r1.a, b1));
+                        }
+                        __syncwarp();
+                    }
+                    e = nl;
                 }
-                if (p1 < total) {
-                    c1 = __ldg(B.ci + r1.q) - lo;
-                    if (MODE != COUNT) b1 = __ldg(B.v + r1.q);
-                }
-                const bool ok0 = p0 < total && (unsigned)c0 < (unsigned)cw;
-                const bool ok1 = p1 < total && (unsigned)c1 < (unsigned)cw;
-                if ((p0 < total && !ok0) || (p1 < total && !ok1))
-                    atomicOr(err, ERR_STRUCTURE);  // B row not sorted
-                if (MODE == COUNT) {
-                    if (ok0) atomicOr(&bits[c0 >> 5], 1u << (c0 & 31));
-                    if (ok1) atomicOr(&bits[c1 >> 5], 1u << (c1 & 31));
-                } else {
-                    ordered_add<true>(acc, ok0 ? c0 : 0, ok0, __fmul_rn(r0.a, b0));
+                if (e < 32) {
+                    const int se = __shfl_sync(FULL, s, e);
+                    const int qe = se + __shfl_sync(FULL, len, e);
+                    const float ae = __shfl_sync(FULL, av, e);
+                    for (int q0 = se; q0 < qe; q0 += 64) {
+                        const int qa = q0 + lane, qb = q0 + 32 + lane;
+                        int ca = 0, cb = 0;
+                        float va = 0.0f, vb = 0.0f;
+                        if (qa < qe) {
+                            ca = __ldg(B.ci + qa) - lo;
+                            if (MODE != COUNT) va = __ldg(B.v + qa);
+                        }
+                        if (qb < qe) {
+                            cb = __ldg(B.ci + qb) - lo;
+                            if (MODE != COUNT) vb = __ldg(B.v + qb);
+                        }
+                        const bool oka = qa < qe && (unsigned)ca < (unsigned)cw;
+                        const bool okb = qb < qe && (unsigned)cb < (unsigned)cw;
+                        if ((qa < qe && !oka) || (qb < qe && !okb)) atomicOr(err, ERR_STRUCTURE);
+                        if (MODE == COUNT) {
+                            if (oka) atomicOr(&bits[ca >> 5], 1u << (ca & 31));
+                            if (okb) atomicOr(&bits[cb >> 5], 1u << (cb & 31));
+                        } else {
+                            if (oka)
+                                acc_store<true>(acc, ca, __fadd_rn(acc_load<true>(acc, ca),
+                                                                   __fmul_rn(ae, va)));
+                            if (okb)
+                                acc_store<true>(acc, cb, __fadd_rn(acc_load<true>(acc, cb),
+                                                                   __fmul_rn(ae, vb)));
+                        }
+                    }
                     __syncwarp();
-                    if (f0 + 32 < total)
-                        ordered_add<true>(acc, ok1 ? c1 : 0, ok1, __fmul_rn(r1.a, b1));
+                    ++e;
                 }
-                __syncwarp();
             }
         }
         __syncwarp();
