@@ -106,26 +106,6 @@ __device__ __forceinline__ int smem_lower_bound(const int32_t* keys, int n, int3
 // vals[slot] += prod for every active lane, in lane order when several lanes
 // share a slot. Lanes hold consecutive products of the row's flattened
 // (A entry, B entry) sequence, so lane order is the reference's order.
-// Bits of an accumulator slot that no product has reached yet (a NaN that
-// the arithmetic below never stores: see acc_store).
-constexpr uint32_t ACC_EMPTY = 0xFFFFFFFFu;
-
-template <bool SENT>
-__device__ __forceinline__ float acc_load(const float* vals, int slot) {
-    const float v = vals[slot];
-    return (SENT && __float_as_uint(v) == ACC_EMPTY) ? 0.0f : v;
-}
-
-template <bool SENT>
-__device__ __forceinline__ void acc_store(float* vals, int slot, float v) {
-    // a NaN result with the sentinel's bits would read as "empty": store the
-    // canonical NaN instead
-    if (SENT && __float_as_uint(v) == ACC_EMPTY) v = __uint_as_float(0x7FFFFFFFu);
-    vals[slot] = v;
-}
-
-// With SENT, slots holding ACC_EMPTY count as +0.0f (the reference's start).
-template <bool SENT = false>
 __device__ __forceinline__ void ordered_add(float* vals, int slot, bool active, float prod) {
     const int lane = lane_id();
     const int key = active ? slot : (0x40000000 | lane);
@@ -133,12 +113,12 @@ __device__ __forceinline__ void ordered_add(float* vals, int slot, bool active, 
     const int n = __popc(peers);
     const int maxn = __reduce_max_sync(FULL, (unsigned)n);
     if (maxn == 1) {
-        if (active) acc_store<SENT>(vals, slot, __fadd_rn(acc_load<SENT>(vals, slot), prod));
+        if (active) vals[slot] = __fadd_rn(vals[slot], prod);
         return;
     }
     const int leader = __ffs(peers) - 1;
     const bool lead = active && lane == leader;
-    float acc = lead ? acc_load<SENT>(vals, slot) : 0.0f;
+    float acc = lead ? vals[slot] : 0.0f;
     unsigned m = peers;
     for (int r = 0; r < maxn; ++r) {
         const int src = m ? (__ffs(m) - 1) : lane;
@@ -146,7 +126,7 @@ __device__ __forceinline__ void ordered_add(float* vals, int slot, bool active, 
         if (lead && m) acc = __fadd_rn(acc, v);
         m &= m - 1;
     }
-    if (lead) acc_store<SENT>(vals, slot, acc);
+    if (lead) vals[slot] = acc;
 }
 // ---------------------------------------------------------------------------
 // Analysis: one CTA per tile of AN_TILE rows; threads stride over the tile's
@@ -1080,18 +1060,21 @@ __global__ void __launch_bounds__(WARPS * 32)
 // Heavy rows: one warp per (row, chunk of cw = 2^cw_log2 columns). The warp
 // walks the row's A entries 32 at a time; each lane finds the part of its B
 // row that falls in the chunk (a binary search only when the B row straddles
-// a chunk edge), and the warp then walks the flattened in-chunk products in
-// A-row order, two steps of 32 in flight. COUNT sets bits of a presence
-// bitmap; FILL and REUSE add into a dense accumulator of cw floats whose
-// untouched slots hold ACC_EMPTY (so FILL needs no bitmap: a slot is present
-// once a product reached it). Same-column products of one step combine in
-// lane order (ordered_add), so each column's sum keeps the reference's
-// order. The A row is re-read once per chunk; the products once in all.
+// a chunk edge). In A-row order, a run of short in-chunk segments is walked
+// flattened (products spread over the lanes, two steps of 32 in flight,
+// same-column products of a step combined in lane order by ordered_add),
+// and a segment of HEAVY_SEG or more products is walked with the lanes over
+// its own columns, which are distinct, so it needs neither the product
+// search nor the ordered combine. COUNT and FILL set bits of a presence
+// bitmap; FILL and REUSE add into a dense accumulator of cw floats started
+// at +0.0f, the reference's start. FILL writes the chunk's entries in column
+// order straight from the bitmap. The A row is re-read once per chunk; the
+// products once in all.
 // ---------------------------------------------------------------------------
 constexpr int HEAVY_SEG = 12;  // in-chunk B segments this long are walked on their own
 
 __host__ __device__ constexpr int heavy_smem_bytes(int mode, int cw) {
-    return mode == COUNT ? cw / 8 : 4 * cw;
+    return (mode == COUNT ? 0 : 4 * cw) + (mode == REUSE ? 0 : cw / 8);
 }
 
 // First index in [lo, hi) with a[idx] >= target (hi if none); one thread.
@@ -1113,12 +1096,12 @@ __global__ void __launch_bounds__(256)
             RowCtl ctl, int cw_log2) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int cw = 1 << cw_log2;
-    const int nw = cw >> 5;  // bitmap words (COUNT)
+    const int nw = cw >> 5;  // bitmap words
     const int warps = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = lane_id();
     unsigned char* mine = smem + warp * heavy_smem_bytes(MODE, cw);
     float* acc = reinterpret_cast<float*>(mine);
-    unsigned* bits = reinterpret_cast<unsigned*>(mine);
+    unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * cw));
 
     for (int w = blockIdx.x * warps + warp; w < nitems; w += gridDim.x * warps) {
         const HeavyItem it = items[w];
@@ -1126,13 +1109,12 @@ __global__ void __launch_bounds__(256)
         if (ctl.only && !ctl.only[row]) continue;
         const int lo = it.chunk << cw_log2;
         const int hi = (int)min((int64_t)lo + cw, (int64_t)B.cols);
-        if (MODE == COUNT) {
-            for (int x = lane; x < nw; x += 32) bits[x] = 0u;
-        } else {
-            uint4* a4 = reinterpret_cast<uint4*>(acc);
-            for (int x = lane; x < (cw >> 2); x += 32)
-                a4[x] = make_uint4(ACC_EMPTY, ACC_EMPTY, ACC_EMPTY, ACC_EMPTY);
+        if (MODE != COUNT) {
+            float4* a4 = reinterpret_cast<float4*>(acc);
+            for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
+        if (MODE != REUSE)
+            for (int x = lane; x < nw; x += 32) bits[x] = 0u;
         __syncwarp();
         int a0, a1;
         row_range(A, row, &a0, &a1, err);
@@ -1154,12 +1136,6 @@ __global__ void __launch_bounds__(256)
                 }
             }
             const int incl = warp_incl_scan(len);
-            // Entries in order: a run of short in-chunk segments is walked
-            // flattened (products spread over the lanes, same-column products
-            // of a step combined in lane order); a segment of HEAVY_SEG or more
-            // products is walked with the lanes over its own columns, which
-            // are distinct, so it needs neither the product search nor the
-            // ordered combine.
             const unsigned longm = __ballot_sync(FULL, len >= HEAVY_SEG);
             int e = 0;
             while (e < 32) {
@@ -1187,14 +1163,15 @@ __global__ void __launch_bounds__(256)
                         const bool ok1 = p1 < pend && (unsigned)c1 < (unsigned)cw;
                         if ((p0 < pend && !ok0) || (p1 < pend && !ok1))
                             atomicOr(err, ERR_STRUCTURE);  // B row not sorted
-                        if (MODE == COUNT) {
+                        if (MODE != REUSE) {
                             if (ok0) atomicOr(&bits[c0 >> 5], 1u << (c0 & 31));
                             if (ok1) atomicOr(&bits[c1 >> 5], 1u << (c1 & 31));
-                        } else {
-                            ordered_add<true>(acc, ok0 ? c0 : 0, ok0, __fmul_rn(r0.a, b0));
+                        }
+                        if (MODE != COUNT) {
+                            ordered_add(acc, ok0 ? c0 : 0, ok0, __fmul_rn(r0.a, b0));
                             __syncwarp();
                             if (f0 + 32 < pend)
-                                ordered_add<true>(acc, ok1 ? c1 : 0, ok1, __fmul_rn(r1.a, b1));
+                                ordered_add(acc, ok1 ? c1 : 0, ok1, __fmul_rn(r1.a, b1));
                         }
                         __syncwarp();
                     }
@@ -1206,29 +1183,28 @@ __global__ void __launch_bounds__(256)
                     const float ae = __shfl_sync(FULL, av, e);
                     for (int q0 = se; q0 < qe; q0 += 64) {
                         const int qa = q0 + lane, qb = q0 + 32 + lane;
+                        const bool two = q0 + 32 < qe;  // warp-uniform
                         int ca = 0, cb = 0;
                         float va = 0.0f, vb = 0.0f;
                         if (qa < qe) {
                             ca = __ldg(B.ci + qa) - lo;
                             if (MODE != COUNT) va = __ldg(B.v + qa);
                         }
-                        if (qb < qe) {
+                        if (two && qb < qe) {
                             cb = __ldg(B.ci + qb) - lo;
                             if (MODE != COUNT) vb = __ldg(B.v + qb);
                         }
                         const bool oka = qa < qe && (unsigned)ca < (unsigned)cw;
-                        const bool okb = qb < qe && (unsigned)cb < (unsigned)cw;
-                        if ((qa < qe && !oka) || (qb < qe && !okb)) atomicOr(err, ERR_STRUCTURE);
-                        if (MODE == COUNT) {
+                        const bool okb = two && qb < qe && (unsigned)cb < (unsigned)cw;
+                        if ((qa < qe && !oka) || (two && qb < qe && !okb))
+                            atomicOr(err, ERR_STRUCTURE);
+                        if (MODE != REUSE) {
                             if (oka) atomicOr(&bits[ca >> 5], 1u << (ca & 31));
                             if (okb) atomicOr(&bits[cb >> 5], 1u << (cb & 31));
-                        } else {
-                            if (oka)
-                                acc_store<true>(acc, ca, __fadd_rn(acc_load<true>(acc, ca),
-                                                                   __fmul_rn(ae, va)));
-                            if (okb)
-                                acc_store<true>(acc, cb, __fadd_rn(acc_load<true>(acc, cb),
-                                                                   __fmul_rn(ae, vb)));
+                        }
+                        if (MODE != COUNT) {
+                            if (oka) acc[ca] = __fadd_rn(acc[ca], __fmul_rn(ae, va));
+                            if (okb) acc[cb] = __fadd_rn(acc[cb], __fmul_rn(ae, vb));
                         }
                     }
                     __syncwarp();
@@ -1247,17 +1223,23 @@ __global__ void __launch_bounds__(256)
                 if (c && row_cnt) atomicAdd(&row_cnt[row], c);
             }
         } else if (MODE == FILL) {
+            // lane l writes the present columns of bitmap word x0 + l; the
+            // words' popcounts give each lane its first output position
             int64_t out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
-            for (int x0 = 0; x0 < cw; x0 += 32) {
-                const float v = acc[x0 + lane];
-                const bool present = __float_as_uint(v) != ACC_EMPTY;
-                const unsigned m = __ballot_sync(FULL, present);
-                if (present) {
-                    const int64_t pos = out + __popc(m & ((1u << lane) - 1));
-                    c_ci[pos] = lo + x0 + lane;
-                    c_v[pos] = v;
+            for (int x0 = 0; x0 < nw; x0 += 32) {
+                unsigned word = x0 + lane < nw ? bits[x0 + lane] : 0u;
+                const int pc = __popc(word);
+                const int incl = warp_incl_scan(pc);
+                int64_t pos = out + (incl - pc);
+                while (word) {
+                    const int b = __ffs(word) - 1;
+                    word &= word - 1;
+                    const int col = (x0 + lane) * 32 + b;
+                    c_ci[pos] = lo + col;
+                    c_v[pos] = acc[col];
+                    ++pos;
                 }
-                out += __popc(m);
+                out += __shfl_sync(FULL, incl, 31);
             }
         } else {
             const int r0 = c_rp[row], r1 = c_rp[row + 1];
@@ -1265,7 +1247,7 @@ __global__ void __launch_bounds__(256)
             const int t = warp_lower_bound(c_ci, s, r1, hi);
             for (int q = s + lane; q < t; q += 32) {
                 const int col = c_ci[q] - lo;
-                c_v[q] = (unsigned)col < (unsigned)cw ? acc_load<true>(acc, col) : 0.0f;
+                c_v[q] = (unsigned)col < (unsigned)cw ? acc[col] : 0.0f;
             }
         }
         __syncwarp();
