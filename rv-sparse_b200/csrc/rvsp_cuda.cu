@@ -220,9 +220,12 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
             const int cl = plan->params.heavy_cw_log2;
             const int W = heavy_warps(MODE, cl);
             const int grid = (plan->n_items + W - 1) / W;
+            const HeavyAux aux{plan->bmeta.as<int4>(), plan->bdoff.as<int64_t>(),
+                               plan->dir_ok ? plan->bdir.as<int32_t>() : nullptr};
             k_heavy<MODE><<<grid, W * 32, W * heavy_smem_bytes(MODE, 1 << cl), plan->stream>>>(
                 A, B, plan->items.as<HeavyItem>(), plan->n_items, plan->item_cnt.as<int32_t>(),
-                o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, o.ctl, cl);
+                o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, o.ctl, cl,
+                aux);
             note_launch(plan, 1);
         }
     }
@@ -368,6 +371,45 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     launch_bin_scatter(plan, plan->bin.as<uint8_t>(), plan->tile_off.as<int32_t>(),
                        plan->bin_rows.as<int32_t>(), true);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "analysis launch");
+    if (plan->n_items > 0 && (st = build_heavy_aux(plan, B))) return st;
+    return RVSP_SUCCESS;
+}
+
+// Per-B-row lookups of the heavy kernel (HeavyAux): metadata of every B row,
+// and the chunk directory of long rows spanning several chunks, unless the
+// directory would pass 2^28 entries (the kernel then binary-searches). One
+// device->host read of the directory size.
+int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& B) {
+    const int64_t K = plan->b_rows;
+    const int cl = plan->params.heavy_cw_log2;
+    cudaError_t e;
+    if ((e = plan->bmeta.ensure(K * 16)) != cudaSuccess ||
+        (e = plan->bdcount.ensure(K * 4)) != cudaSuccess ||
+        (e = plan->bdscan.ensure((K + 1) * 8)) != cudaSuccess ||
+        (e = plan->bdoff.ensure(K * 8)) != cudaSuccess)
+        return fail(e, "heavy lookups");
+    Misc* misc = plan->misc.as<Misc>();
+    k_bmeta<<<(unsigned)((K + 255) / 256), 256, 0, plan->stream>>>(
+        B, cl, plan->bmeta.as<int4>(), plan->bdcount.as<int32_t>(), &misc->err);
+    note_launch(plan, 1);
+    int st = scan_counts(plan, plan->bdcount.as<int32_t>(), K, plan->bdscan.as<int64_t>(), nullptr,
+                         &misc->dir_total);
+    if (st) return st;
+    int64_t total = 0;
+    if ((e = cudaMemcpyAsync(&total, &misc->dir_total, 8, cudaMemcpyDeviceToHost,
+                             plan->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(plan->stream)) != cudaSuccess)
+        return fail(e, "directory size");
+    plan->dir_ok = total > 0 && total <= (int64_t(1) << 28) &&
+                   plan->bdir.ensure((size_t)total * 4) == cudaSuccess;
+    cudaGetLastError();  // a refused directory allocation only costs the searches
+    if (plan->dir_ok) {
+        k_bdir<<<(unsigned)((K * 32 + 255) / 256), 256, 0, plan->stream>>>(
+            B, cl, plan->bmeta.as<int4>(), plan->bdcount.as<int32_t>(),
+            plan->bdscan.as<int64_t>(), plan->bdoff.as<int64_t>(), plan->bdir.as<int32_t>());
+        note_launch(plan, 1);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "heavy lookups launch");
     return RVSP_SUCCESS;
 }
 
@@ -559,7 +601,8 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
                       &p->pred_cap, &p->slot_off, &p->tmp_ci, &p->tmp_v, &p->row_flag,
                       &p->tile_hist, &p->tile_off, &p->pm8, &p->pm16, &p->list_ops,
                       &p->list_off, &p->lbin, &p->lcap, &p->ltile_hist, &p->ltile_off,
-                      &p->lbin_rows, &p->need, &p->pflag};
+                      &p->lbin_rows, &p->need, &p->pflag, &p->bmeta, &p->bdcount,
+                      &p->bdscan, &p->bdoff, &p->bdir};
     for (DevBuf* b : bufs) b->release();
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;

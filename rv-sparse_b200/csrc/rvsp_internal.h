@@ -48,6 +48,7 @@ struct Misc {
     int64_t slot_total;        // learned path: sum of predicted capacities
     int64_t lstats[8];         // learned path statistics (see rvsp_cuda_plan_learned_stats)
     int64_t ltile_total;
+    int64_t dir_total;         // heavy-row B directory entries
 };
 
 // Output pointers of a row-kernel launch.
@@ -103,6 +104,10 @@ struct rvsp_cuda_plan {
     // analysed structure
     rvsp::DevBuf ops, ub, bin, chunk_lo, nchunks, feat, cnt, c_rp, bin_rows, tile_hist, tile_off;
     rvsp::DevBuf items, item_cnt, item_scan, scan_tmp, misc;
+    // per-B-row lookups of the heavy kernel (HeavyAux), built by the analysis
+    // when the product has chunked rows; dir_ok when the directory exists
+    rvsp::DevBuf bmeta, bdcount, bdscan, bdoff, bdir;
+    bool dir_ok = false;
     int32_t bin_count[rvsp::NUM_BINS] = {};
     rvsp::BinOffsets offs = {};
     int32_t n_items = 0;
@@ -155,6 +160,7 @@ int scan_counts(rvsp_cuda_plan* plan, const int32_t* in, int64_t n, int64_t* out
                 int32_t* out32, int64_t* total_dev);
 void note_launch(rvsp_cuda_plan* plan, int n);
 void reset_graph(rvsp_cuda_plan* plan);
+int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& B);
 void launch_bin_scatter(rvsp_cuda_plan* plan, const uint8_t* bin, const int32_t* tile_off,
                         int32_t* bin_rows, bool heavy_items);
 int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool fused);

@@ -1087,13 +1087,69 @@ __device__ __forceinline__ int seq_lower_bound(const int32_t* __restrict__ a, in
     return lo;
 }
 
+// Per-B-row metadata and directory sizes (HeavyAux). Rows whose structure is
+// out of range flag ERR_STRUCTURE and read as empty.
+__global__ void k_bmeta(CsrView B, int cw_log2, int4* __restrict__ meta,
+                        int32_t* __restrict__ dcount, int32_t* __restrict__ err) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= B.rows) return;
+    int bs, be;
+    row_range(B, k, &bs, &be, err);
+    int first = 0, last = -1, dc = 0;
+    if (be > bs) {
+        first = B.ci[bs];
+        last = B.ci[be - 1];
+        if (first < 0 || last >= B.cols || last < first) {
+            atomicOr(err, ERR_STRUCTURE);
+            be = bs;
+            first = 0;
+            last = -1;
+        } else {
+            const int fc = first >> cw_log2, lc = last >> cw_log2;
+            if (be - bs >= DIR_MIN_LEN && lc > fc) dc = lc - fc + 2;
+        }
+    }
+    meta[k] = make_int4(bs, be, first, last);
+    dcount[k] = dc;
+}
+
+// Directory fill: one warp per B row with a directory; the entry at q writes
+// itself as the start of every chunk from just after its predecessor's chunk
+// up to its own; the row end closes the list. doff[k] = -1 for the others.
+__global__ void k_bdir(CsrView B, int cw_log2, const int4* __restrict__ meta,
+                       const int32_t* __restrict__ dcount, const int64_t* __restrict__ dscan,
+                       int64_t* __restrict__ doff, int32_t* __restrict__ dir) {
+    const int k = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = lane_id();
+    if (k >= B.rows) return;
+    const int dc = dcount[k];
+    if (dc == 0) {
+        if (lane == 0) doff[k] = -1;
+        return;
+    }
+    const int64_t off = dscan[k];
+    const int4 m = meta[k];
+    const int fc = m.z >> cw_log2, lc = m.w >> cw_log2;
+    if (lane == 0) {
+        doff[k] = off;
+        dir[off + (lc - fc + 1)] = m.y;
+    }
+    for (int q = m.x + lane; q < m.y; q += 32) {
+        const int c = B.ci[q] >> cw_log2;
+        const int prev = q > m.x ? (B.ci[q - 1] >> cw_log2) : fc - 1;
+        // clamped to [fc, lc]: an unsorted row (a broken operand) cannot
+        // write outside its directory
+        for (int x = max(prev + 1, fc); x <= min(c, lc); ++x) dir[off + (x - fc)] = q;
+    }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256)
     k_heavy(CsrView A, CsrView B, const HeavyItem* __restrict__ items, int nitems,
             int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
             const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
             int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err,
-            RowCtl ctl, int cw_log2) {
+            RowCtl ctl, int cw_log2, HeavyAux aux) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int cw = 1 << cw_log2;
     const int nw = cw >> 5;  // bitmap words
@@ -1123,13 +1179,27 @@ __global__ void __launch_bounds__(256)
             int s = 0, len = 0;
             float av = 0.0f;
             if (j < a1) {
-                int bs, be;
-                row_range(B, A.ci[j], &bs, &be, err);
-                if (be > bs) {
-                    const int first = __ldg(B.ci + bs), last = __ldg(B.ci + be - 1);
-                    if (last >= lo && first < hi) {
-                        s = first >= lo ? bs : seq_lower_bound(B.ci, bs, be, lo);
-                        const int t = last < hi ? be : seq_lower_bound(B.ci, s, be, hi);
+                const int k = A.ci[j];
+                if ((unsigned)k >= (unsigned)B.rows) {
+                    atomicOr(err, ERR_STRUCTURE);
+                } else {
+                    // {start, end, first column, last column} of B row k
+                    const int4 m = aux.meta[k];
+                    const int64_t d = aux.dir ? aux.doff[k] : -1;
+                    if (m.y > m.x && m.w >= lo && m.z < hi) {
+                        int t;
+                        if (d >= 0) {
+                            const int c = it.chunk - (m.z >> cw_log2);
+                            s = m.z >= lo ? m.x : aux.dir[d + c];
+                            t = m.w < hi ? m.y : aux.dir[d + c + 1];
+                            // only an unsorted row (a broken operand) leaves a
+                            // directory entry unwritten: stay inside the row
+                            s = min(max(s, m.x), m.y);
+                            t = min(max(t, s), m.y);
+                        } else {
+                            s = m.z >= lo ? m.x : seq_lower_bound(B.ci, m.x, m.y, lo);
+                            t = m.w < hi ? m.y : seq_lower_bound(B.ci, s, m.y, hi);
+                        }
                         len = t - s;
                         if (MODE != COUNT) av = A.v[j];
                     }

@@ -77,6 +77,19 @@ struct HeavyItem {
     int32_t pad;
 };
 
+// Per-B-row lookups for the heavy kernel, built by the analysis when the
+// product has chunked rows: meta[k] = {row start, row end, first column, last
+// column}; for rows of at least DIR_MIN_LEN entries that span several column
+// chunks, doff[k] >= 0 and dir[doff[k] + i] is the first position of the
+// row whose column is >= (first chunk + i) * chunk width, for i = 0 .. (last
+// chunk - first chunk + 1); doff[k] = -1 otherwise (dir may be null).
+struct HeavyAux {
+    const int4* meta;
+    const int64_t* doff;
+    const int32_t* dir;
+};
+constexpr int DIR_MIN_LEN = 32;
+
 struct BinOffsets {
     int32_t off[NUM_BINS];
 };

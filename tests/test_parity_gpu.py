@@ -227,6 +227,20 @@ def test_rmat_matches_oracle(gpu_lib):
     assert_same(oneshot(R, R), oracle_full(R, R), "rmat s13")
 
 
+def test_rmat16_heavy_rows_sampled(gpu_lib):
+    """R-MAT 2^16: chunked heavy rows over B rows long enough to get a column
+    directory, several scan tiles; the hub rows and a band of middle rows are
+    compared with the oracle bit for bit."""
+    R = gen.rmat(scale=16, edge_factor=16, seed=0)
+    rp, ci, v = oneshot(R, R)
+    for r0, r1 in ((0, 1500), (30000, 30400)):
+        wrp, wci, wv = oracle.spgemm_f32(R, R, r0, r1)
+        lo, hi = int(rp[r0]), int(rp[r1])
+        assert np.array_equal(np.asarray(rp[r0:r1 + 1], np.int64) - lo, wrp), (r0, r1)
+        assert np.array_equal(ci[lo:hi], wci), (r0, r1)
+        assert np.array_equal(bits(v[lo:hi]), bits(wv)), (r0, r1)
+
+
 def test_tall_skinny_heavy_rows(gpu_lib):
     A, B = gen.tall_skinny(a_rows=20000, k=20000, n=20000, b_max=6000, seed=3)
     assert_same(oneshot(A, B), oracle_full(A, B), "tall skinny")
