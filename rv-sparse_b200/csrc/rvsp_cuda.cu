@@ -124,12 +124,33 @@ static void set_mode_attrs() {
     cudaFuncSetAttribute(k_heavy<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
 }
 
+// Resident CTAs of the heavy kernel per SM for every mode and chunk width,
+// and the SM count: the heavy launches are sized to fill the GPU once, with
+// the warps pulling work items from a counter.
+static int g_heavy_ctas[3][HEAVY_CW_LOG2_MAX + 1];
+static int g_sms = 148;
+
 static std::once_flag g_attr_once;
 void init_kernel_attributes() {
     std::call_once(g_attr_once, [] {
         set_mode_attrs<COUNT>();
         set_mode_attrs<FILL>();
         set_mode_attrs<REUSE>();
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+        for (int cl = HEAVY_CW_LOG2_MIN; cl <= HEAVY_CW_LOG2_MAX; ++cl) {
+            const void* fns[3] = {(const void*)k_heavy<COUNT>, (const void*)k_heavy<FILL>,
+                                  (const void*)k_heavy<REUSE>};
+            for (int m = 0; m < 3; ++m) {
+                const int W = heavy_warps(m, cl);
+                int n = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                        &n, fns[m], W * 32, (size_t)W * heavy_smem_bytes(m, 1 << cl)) != cudaSuccess)
+                    n = 1;
+                g_heavy_ctas[m][cl] = n > 0 ? n : 1;
+            }
+        }
         cudaGetLastError();
     });
 }
@@ -219,13 +240,16 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
         } else if (plan->n_items > 0) {
             const int cl = plan->params.heavy_cw_log2;
             const int W = heavy_warps(MODE, cl);
-            const int grid = (plan->n_items + W - 1) / W;
+            const int64_t fill = (int64_t)g_sms * g_heavy_ctas[MODE][cl];
+            const int grid = (int)std::min<int64_t>((plan->n_items + W - 1) / W, fill);
             const HeavyAux aux{plan->bmeta.as<int4>(), plan->bdoff.as<int64_t>(),
                                plan->dir_ok ? plan->bdir.as<int32_t>() : nullptr};
+            int32_t* queue = &plan->misc.as<Misc>()->heavy_queue;
+            cudaMemsetAsync(queue, 0, sizeof(int32_t), plan->stream);
             k_heavy<MODE><<<grid, W * 32, W * heavy_smem_bytes(MODE, 1 << cl), plan->stream>>>(
                 A, B, plan->items.as<HeavyItem>(), plan->n_items, plan->item_cnt.as<int32_t>(),
                 o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, o.ctl, cl,
-                aux);
+                aux, queue);
             note_launch(plan, 1);
         }
     }

@@ -49,6 +49,8 @@ struct Misc {
     int64_t lstats[8];         // learned path statistics (see rvsp_cuda_plan_learned_stats)
     int64_t ltile_total;
     int64_t dir_total;         // heavy-row B directory entries
+    int32_t heavy_queue;       // next heavy work item of the running launch
+    int32_t pad4;
 };
 
 // Output pointers of a row-kernel launch.

@@ -1149,7 +1149,7 @@ __global__ void __launch_bounds__(256)
             int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
             const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
             int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err,
-            RowCtl ctl, int cw_log2, HeavyAux aux) {
+            RowCtl ctl, int cw_log2, HeavyAux aux, int32_t* __restrict__ queue) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int cw = 1 << cw_log2;
     const int nw = cw >> 5;  // bitmap words
@@ -1159,7 +1159,14 @@ __global__ void __launch_bounds__(256)
     float* acc = reinterpret_cast<float*>(mine);
     unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * cw));
 
-    for (int w = blockIdx.x * warps + warp; w < nitems; w += gridDim.x * warps) {
+    (void)warps;
+    for (;;) {
+        // items are pulled one at a time, so a warp that drew a light item
+        // takes the next one instead of idling beside a heavy one
+        int w = 0;
+        if (lane == 0) w = atomicAdd(queue, 1);
+        w = __shfl_sync(FULL, w, 0);
+        if (w >= nitems) break;
         const HeavyItem it = items[w];
         const int row = it.row;
         if (ctl.only && !ctl.only[row]) continue;
