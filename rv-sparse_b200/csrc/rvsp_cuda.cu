@@ -86,12 +86,6 @@ constexpr int warps_for() {
     return w > 8 ? 8 : (w < 1 ? 1 : w);
 }
 
-// warps per CTA of the heavy kernel: as many per-warp accumulators as fit
-// in 64 KB, at most 8
-static int heavy_warps(int mode, int cw_log2) {
-    const int w = 65536 / heavy_smem_bytes(mode, 1 << cw_log2);
-    return w > 8 ? 8 : (w < 1 ? 1 : w);
-}
 
 // warps per CTA of the map-replay reuse kernel (a float per slot)
 template <int CAP>
@@ -100,11 +94,22 @@ constexpr int map_warps() {
     return w > 8 ? 8 : (w < 1 ? 1 : w);
 }
 
+constexpr int HEAVY_SMEM_MAX = 227 * 1024;  // largest dynamic shared memory of one CTA
+
+// resident CTAs per SM of every warp-bin kernel (launches fill the GPU once
+// and the warps pull rows from a counter)
+static int g_warp_ctas[3][NUM_WARP_BINS];
+
 template <int CAP, int MODE>
 static void set_warp_attr() {
     constexpr int W = warps_for<CAP, MODE>();
     cudaFuncSetAttribute(k_warp<CAP, W, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          W * warp_smem_bytes<CAP, MODE>());
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_warp<CAP, W, MODE>, W * 32,
+                                                      W * warp_smem_bytes<CAP, MODE>()) != cudaSuccess)
+        n = 1;
+    g_warp_ctas[MODE][__builtin_ctz(CAP / WARP_CAP_MIN)] = n > 0 ? n : 1;
     if (MODE == REUSE) {
         constexpr int WM = map_warps<CAP>();
         cudaFuncSetAttribute(k_warp_reuse_map<CAP, WM>,
@@ -121,12 +126,15 @@ static void set_mode_attrs() {
     set_warp_attr<1024, MODE>();
     set_warp_attr<2048, MODE>();
     set_warp_attr<4096, MODE>();
-    cudaFuncSetAttribute(k_heavy<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
+    cudaFuncSetAttribute(k_heavy<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         HEAVY_SMEM_MAX);
 }
 
-// Resident CTAs of the heavy kernel per SM for every mode and chunk width,
-// and the SM count: the heavy launches are sized to fill the GPU once, with
-// the warps pulling work items from a counter.
+// Heavy kernel shape for every mode and chunk width: warps per CTA chosen to
+// keep the most warps resident per SM (each warp holds its own accumulator
+// and bitmap in shared memory), and the resident CTAs per SM; the launches
+// fill the GPU once and the warps pull work items from a counter.
+static int g_heavy_w[3][HEAVY_CW_LOG2_MAX + 1];
 static int g_heavy_ctas[3][HEAVY_CW_LOG2_MAX + 1];
 static int g_sms = 148;
 
@@ -143,12 +151,24 @@ void init_kernel_attributes() {
             const void* fns[3] = {(const void*)k_heavy<COUNT>, (const void*)k_heavy<FILL>,
                                   (const void*)k_heavy<REUSE>};
             for (int m = 0; m < 3; ++m) {
-                const int W = heavy_warps(m, cl);
-                int n = 0;
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                        &n, fns[m], W * 32, (size_t)W * heavy_smem_bytes(m, 1 << cl)) != cudaSuccess)
-                    n = 1;
-                g_heavy_ctas[m][cl] = n > 0 ? n : 1;
+                const size_t per = (size_t)heavy_smem_bytes(m, 1 << cl);
+                int best_w = 1, best_n = 1, best = 0;
+                for (int W = 1; W <= HEAVY_MAX_WARPS; ++W) {
+                    if (W * per > (size_t)HEAVY_SMEM_MAX) break;
+                    int n = 0;
+                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fns[m], W * 32, W * per) !=
+                        cudaSuccess) {
+                        cudaGetLastError();
+                        continue;
+                    }
+                    if (n * W > best) {
+                        best = n * W;
+                        best_w = W;
+                        best_n = n;
+                    }
+                }
+                g_heavy_w[m][cl] = best_w;
+                g_heavy_ctas[m][cl] = best_n;
             }
         }
         cudaGetLastError();
@@ -198,10 +218,13 @@ static void launch_warp(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
             A, B, rows, n, o.c_rp, o.c_v, lo, pm, o.err);
     } else {
         constexpr int W = warps_for<CAP, MODE>();
-        k_warp<CAP, W, MODE><<<(n + W - 1) / W, W * 32, W * warp_smem_bytes<CAP, MODE>(),
-                               plan->stream>>>(A, B, rows, n, o.cnt, o.c_rp, o.c_ci, o.c_v,
-                                               o.maps ? lo : nullptr, o.maps ? pm : nullptr,
-                                               o.err, o.ctl);
+        const int fill = g_sms * g_warp_ctas[MODE][b - BIN_WARP0];
+        const int grid = std::min((n + W - 1) / W, fill);
+        int32_t* queue = &plan->misc.as<Misc>()->row_queue;
+        cudaMemsetAsync(queue, 0, sizeof(int32_t), plan->stream);
+        k_warp<CAP, W, MODE><<<grid, W * 32, W * warp_smem_bytes<CAP, MODE>(), plan->stream>>>(
+            A, B, rows, n, o.cnt, o.c_rp, o.c_ci, o.c_v, o.maps ? lo : nullptr,
+            o.maps ? pm : nullptr, o.err, o.ctl, queue);
     }
     note_launch(plan, 1);
 }
@@ -239,7 +262,7 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
             }
         } else if (plan->n_items > 0) {
             const int cl = plan->params.heavy_cw_log2;
-            const int W = heavy_warps(MODE, cl);
+            const int W = g_heavy_w[MODE][cl];
             const int64_t fill = (int64_t)g_sms * g_heavy_ctas[MODE][cl];
             const int grid = (int)std::min<int64_t>((plan->n_items + W - 1) / W, fill);
             const HeavyAux aux{plan->bmeta.as<int4>(), plan->bdoff.as<int64_t>(),

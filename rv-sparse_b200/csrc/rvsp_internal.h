@@ -50,7 +50,7 @@ struct Misc {
     int64_t ltile_total;
     int64_t dir_total;         // heavy-row B directory entries
     int32_t heavy_queue;       // next heavy work item of the running launch
-    int32_t pad4;
+    int32_t row_queue;         // next row of the running warp-bin launch
 };
 
 // Output pointers of a row-kernel launch.

@@ -801,7 +801,7 @@ __global__ void __launch_bounds__(WARPS * 32)
            int32_t* __restrict__ cnt, const int32_t* __restrict__ c_rp,
            int32_t* __restrict__ c_ci, float* __restrict__ c_v,
            const int32_t* __restrict__ list_off, uint16_t* __restrict__ pm,
-           int32_t* __restrict__ err, RowCtl ctl) {
+           int32_t* __restrict__ err, RowCtl ctl, int32_t* __restrict__ queue) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int LOG2CAP = __builtin_ctz(CAP);
     const int warp = threadIdx.x >> 5, lane = lane_id();
@@ -815,7 +815,12 @@ __global__ void __launch_bounds__(WARPS * 32)
     // capacity; the row is flagged for the exact path instead of an error
     const bool learned = MODE != REUSE && ctl.learned;
 
-    for (int w = blockIdx.x * WARPS + warp; w < nrows; w += gridDim.x * WARPS) {
+    for (;;) {
+        // rows are pulled one at a time from the launch's counter
+        int w = 0;
+        if (lane == 0) w = atomicAdd(queue, 1);
+        w = __shfl_sync(FULL, w, 0);
+        if (w >= nrows) break;
         const int row = rows[w];
         if (ctl.only && !ctl.only[row]) continue;
         int a0, a1;
@@ -1143,8 +1148,10 @@ __global__ void k_bdir(CsrView B, int cw_log2, const int4* __restrict__ meta,
     }
 }
 
+constexpr int HEAVY_MAX_WARPS = 32;
+
 template <int MODE>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
     k_heavy(CsrView A, CsrView B, const HeavyItem* __restrict__ items, int nitems,
             int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
             const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
