@@ -88,7 +88,7 @@ RVSP_CUDA_API void *rvsp_cuda_plan_stream(rvsp_cuda_plan_t plan);
  *   [2] warp_cap_max  largest warp hash table, a power of two in 64..4096;
  *                     rows needing more are split into column chunks, a warp each
  *   [3] heavy_cw_log2 log2 of the columns of one chunk (9..13)
- * Defaults: 32, 2, 4096, 11. Results do not depend on the parameters (the
+ * Defaults: 32, 2, 2048, 11. Results do not depend on the parameters (the
  * pattern and the values are bit-identical under every valid setting); only
  * the time does.
  *

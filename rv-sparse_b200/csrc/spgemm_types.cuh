@@ -61,7 +61,7 @@ struct BinParams {
     int32_t heavy_cw_log2;
 };
 constexpr int BIN_PARAMS_N = 4;
-constexpr BinParams DEFAULT_BIN_PARAMS = {TINY_CAP, 2, WARP_CAP_MAX, 11};
+constexpr BinParams DEFAULT_BIN_PARAMS = {TINY_CAP, 2, 2048, 11};
 
 __host__ __device__ inline bool bin_params_valid(const BinParams& p) {
     const bool pow2 = p.warp_cap_max > 0 && (p.warp_cap_max & (p.warp_cap_max - 1)) == 0;

@@ -134,7 +134,7 @@ _PROTOS = {
 
 BIN_PARAMS = 4  # tiny_ops, slack_shift, warp_cap_max, heavy_cw_log2
 BIN_PARAM_NAMES = ("tiny_ops", "slack_shift", "warp_cap_max", "heavy_cw_log2")
-DEFAULT_BIN_PARAMS = (32, 2, 4096, 11)
+DEFAULT_BIN_PARAMS = (32, 2, 2048, 11)
 MLP_PARAMS = 1282
 MLP_FLOATS = 1291  # [mean(4), inv_std(4), z, params(1282)]
 
