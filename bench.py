@@ -143,11 +143,12 @@ def poisson_workload():
     return A, P
 
 
-def algorithmic_bytes(M, nnz_a, nnz_c, b_rows=None, nnz_b=None):
-    """Compulsory bytes: A's arrays once, B's once when B is a distinct matrix,
-    C's row pointer and its col_idx + values once (read+write on reuse)."""
-    b = 0 if b_rows is None else 4 * (b_rows + 1) + 8 * nnz_b
-    return 4 * (M + 1) + 8 * nnz_a + b + 4 * (M + 1) + 8 * nnz_c
+def algorithmic_bytes(M, nnz_a, nnz_c, b_rows, nnz_b):
+    """Compulsory bytes of one product, 4(M+1) + 8 nnzA + 4(K+1) + 8 nnzB +
+    4(M+1) + 8 nnzC: every operand array read once (B counted as its own
+    operand also when it is A), C's row pointer and col_idx + values once
+    (col_idx read and values written on descriptor reuse)."""
+    return 4 * (M + 1) + 8 * nnz_a + 4 * (b_rows + 1) + 8 * nnz_b + 4 * (M + 1) + 8 * nnz_c
 
 
 def run_ours(args):
@@ -245,7 +246,8 @@ def run_ours(args):
         return
 
     hbm, peak_kind = peaks()
-    bytes_alg = algorithmic_bytes(M, nnz_a, nnz_c)
+    bytes_alg = algorithmic_bytes(M, nnz_a, nnz_c, M, nnz_a)
+    bytes_distinct = bytes_alg - (4 * (M + 1) + 8 * nnz_a)  # B's arrays are A's
     achieved = bytes_alg / (ms * 1e-3) / 1e9
     traffic = None
     tr_path = os.path.join(ROOT, "profiles", "traffic.json")
@@ -264,7 +266,8 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_tiny_reuse_map",
-                     "bytes_per_launch": bytes_alg},
+                     "bytes_per_launch": bytes_alg,
+                     "frac_distinct_arrays": round(bytes_distinct / (ms * 1e-3) / 1e9 / hbm, 4)},
         "e2e": e2e,
         "oneshot_exact_vs_learned": oneshot_cmp,
         "gpu_launches": int(launches),
@@ -590,8 +593,7 @@ def run_compare(args):
         res["learned_over_exact"] = times["exact"] / times["learned"]
         res["learned_bit_identical_to_exact"] = bool(same)
         res["ms"] = {k: v * 1e3 for k, v in times.items()}
-        b_alg = algorithmic_bytes(A.rows, A.nnz, nnz_c, None if B is A else B.rows,
-                                  None if B is A else B.nnz)
+        b_alg = algorithmic_bytes(A.rows, A.nnz, nnz_c, B.rows, B.nnz)
         res["bytes_alg"] = b_alg
         res["hbm_frac_learned"] = b_alg / times["learned"] / 1e9 / peaks()[0]
         # FP64 error of the FP32 result on sampled rows
