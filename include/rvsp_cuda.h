@@ -185,6 +185,29 @@ RVSP_CUDA_API int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols,
                          float **c_values_out, int32_t *c_nnz_out, int64_t *op_counts_out);
 
 /*
+ * The reference's other dtypes, one call each. Replace its legacy raw kernels
+ * rvsp_spgemm_csr_scalar_f64_raw and rvsp_spgemm_csr_scalar_i8_raw
+ * (rv-sparse src/kernels/spgemm/legacy/csr_spgemm_kernels.h:80-94,156-170;
+ * csr_scalar_f64.c:49-272, csr_scalar_i8.c:24-196), reached from
+ * rvsp_spgemm_csr with FP64/FP64 or INT8/INT32 dtypes (spgemm.c:181-193).
+ * Same semantics: per column acc += a * b in A-row order from zero (FP64
+ * rounded to nearest without FMA; INT8 products and INT32 sums in two's
+ * complement), columns ascending, and entries whose sum is exactly zero are
+ * not stored, so *c_nnz_out can be below the symbolic count. Ownership and
+ * residency as rvsp_cuda_spgemm_f32.
+ */
+RVSP_CUDA_API int rvsp_cuda_spgemm_f64(int32_t a_rows, int32_t a_cols, int32_t b_cols,
+                         const int32_t *a_row_ptr, const int32_t *a_col_idx, const double *a_values,
+                         const int32_t *b_row_ptr, const int32_t *b_col_idx, const double *b_values,
+                         int32_t **c_row_ptr, int32_t **c_col_idx, double **c_values,
+                         int32_t *c_nnz_out);
+RVSP_CUDA_API int rvsp_cuda_spgemm_i8(int32_t a_rows, int32_t a_cols, int32_t b_cols,
+                         const int32_t *a_row_ptr, const int32_t *a_col_idx, const int8_t *a_values,
+                         const int32_t *b_row_ptr, const int32_t *b_col_idx, const int8_t *b_values,
+                         int32_t **c_row_ptr, int32_t **c_col_idx, int32_t **c_values,
+                         int32_t *c_nnz_out);
+
+/*
  * Canonical-CSR check on the device. Replaces rvsp_csr_check
  * (rv-sparse src/kernels/spgemm/rvsp_support.c:37-127) with the same result
  * codes (0 ok, 1 bad row_ptr, 2 column out of range, 3 unsorted,

@@ -20,6 +20,11 @@ The restatement is pinned against the reference's golden fixtures
 ``tests/golden/csr_fixtures.json``) and against ``libref`` outputs on seeded
 inputs (``tests/golden/ref_outputs.json``).
 
+The reference's legacy FP64 and INT8 -> INT32 one-shot kernels are restated
+too (``spgemm_typed``) and, in ``libref``, compiled from their sources
+(rv-sparse ``src/kernels/spgemm/legacy/csr_scalar_f64.c``, ``csr_scalar_i8.c``;
+``ref_spgemm_typed``).
+
 An FP64 MLP forward/backward (``mlp_forward_backward_f64``) is the gradient
 oracle for the learned row-size predictor; it has no reference counterpart.
 """
@@ -73,6 +78,15 @@ def lib():
         L.oracle_numeric_f64.argtypes = [C.c_int32, C.c_int32, C.c_int32,
                                          _i32p, _i32p, _f32p, _i32p, _i32p, _f32p,
                                          _i64p, _i32p, _f64p]
+        _i8p = np.ctypeslib.ndpointer(np.int8, flags="C_CONTIGUOUS")
+        L.oracle_spgemm_f64.restype = C.c_int
+        L.oracle_spgemm_f64.argtypes = [C.c_int32, C.c_int32, C.c_int32,
+                                        _i32p, _i32p, _f64p, _i32p, _i32p, _f64p,
+                                        _i64p, _i32p, _f64p]
+        L.oracle_spgemm_i8.restype = C.c_int
+        L.oracle_spgemm_i8.argtypes = [C.c_int32, C.c_int32, C.c_int32,
+                                       _i32p, _i32p, _i8p, _i32p, _i32p, _i8p,
+                                       _i64p, _i32p, _i32p]
         L.oracle_numeric_f32.restype = C.c_int
         L.oracle_numeric_f32.argtypes = [C.c_int32, C.c_int32, C.c_int32,
                                          _i32p, _i32p, _f32p, _i32p, _i32p, _f32p,
@@ -104,6 +118,12 @@ def ref():
         L.ref_time_numeric.argtypes = [C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int32,
                                        _i32p, _i32p, _f32p, _i32p, _i32p, _f32p,
                                        _i32p, _i32p, _f32p]
+        for nm in ("rvsp_spgemm_csr_scalar_f64_raw", "rvsp_spgemm_csr_scalar_i8_raw"):
+            fn = getattr(L, nm)
+            fn.restype = C.c_int
+            fn.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                           C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p),
+                           C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int32)]
         L.rvsp_csr_check.restype = C.c_int
         L.rvsp_csr_check.argtypes = [C.c_int32, C.c_int32, _i32p, _i32p, C.POINTER(C.c_int32)]
         _ref = L
@@ -272,3 +292,57 @@ def mlp_forward_backward_f64(params, X, y, w_loss):
     g["W1"] = dz1.T @ X
     g["b1"] = dz1.sum(0)
     return L, g
+
+
+_TYPED = {"f64": (np.float64, np.float64), "i8": (np.int8, np.int32)}
+
+
+def spgemm_typed(A, B, dtype, row_begin=0, row_end=None):
+    """Legacy-dtype product (dtype "f64": FP64 -> FP64, "i8": INT8 -> INT32) of rows
+    [row_begin, row_end): (row_ptr int64 relative, col_idx, values), zero sums dropped."""
+    in_t, out_t = _TYPED[dtype]
+    row_end = A.rows if row_end is None else row_end
+    a_rp = np.ascontiguousarray(A.row_ptr, np.int32)
+    a_ci = np.ascontiguousarray(A.col_idx, np.int32)
+    b_rp = np.ascontiguousarray(B.row_ptr, np.int32)
+    b_ci = np.ascontiguousarray(B.col_idx, np.int32)
+    a_v = np.ascontiguousarray(A.values, in_t)
+    b_v = np.ascontiguousarray(B.values, in_t)
+    _, cnt = symbolic(A, B, row_begin, row_end)
+    total = int(cnt.sum())
+    rp = np.zeros(row_end - row_begin + 1, np.int64)
+    ci = np.zeros(max(total, 1), np.int32)
+    v = np.zeros(max(total, 1), out_t)
+    fn = lib().oracle_spgemm_f64 if dtype == "f64" else lib().oracle_spgemm_i8
+    if fn(row_begin, row_end, B.cols, a_rp, _nz(a_ci), _nz(a_v), b_rp, _nz(b_ci), _nz(b_v),
+          rp, ci, v) != 0:
+        raise MemoryError("oracle legacy-dtype product failed")
+    n = int(rp[-1])
+    return rp, ci[:n], v[:n]
+
+
+def ref_spgemm_typed(A, B, dtype):
+    """The reference's own legacy raw kernel (csr_scalar_f64.c / csr_scalar_i8.c);
+    returns (row_ptr, col_idx, values, status)."""
+    in_t, out_t = _TYPED[dtype]
+    L = ref()
+    fn = L.rvsp_spgemm_csr_scalar_f64_raw if dtype == "f64" else L.rvsp_spgemm_csr_scalar_i8_raw
+    arrs = [np.ascontiguousarray(A.row_ptr, np.int32), _nz(np.ascontiguousarray(A.col_idx, np.int32)),
+            _nz(np.ascontiguousarray(A.values, in_t)), np.ascontiguousarray(B.row_ptr, np.int32),
+            _nz(np.ascontiguousarray(B.col_idx, np.int32)), _nz(np.ascontiguousarray(B.values, in_t))]
+    p_rp, p_ci, p_v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    nnz = C.c_int32(0)
+    st = fn(A.rows, A.cols, B.cols, *[a.ctypes.data for a in arrs], C.byref(p_rp), C.byref(p_ci),
+            C.byref(p_v), C.byref(nnz))
+    if st != 0:
+        return None, None, None, st
+    n = nnz.value
+    ctype = C.c_double if dtype == "f64" else C.c_int32
+    rp = np.ctypeslib.as_array(C.cast(p_rp, C.POINTER(C.c_int32)), (A.rows + 1,)).copy()
+    ci = (np.ctypeslib.as_array(C.cast(p_ci, C.POINTER(C.c_int32)), (n,)).copy()
+          if n else np.zeros(0, np.int32))
+    v = (np.ctypeslib.as_array(C.cast(p_v, C.POINTER(ctype)), (n,)).copy()
+         if n else np.zeros(0, out_t))
+    for p in (p_rp, p_ci, p_v):
+        L.ref_free(p)
+    return rp, ci, v, 0

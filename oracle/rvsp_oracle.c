@@ -26,6 +26,14 @@
  * An FP64 variant of the numeric pass gives the error yardstick for the
  * FP32 results. It has no reference counterpart.
  *
+ * The reference's other two dtypes (its legacy one-shot kernels) are
+ * restated too: FP64 x FP64 -> FP64
+ *       rv-sparse src/kernels/spgemm/legacy/csr_scalar_f64.c:49-272
+ * and INT8 x INT8 -> INT32
+ *       rv-sparse src/kernels/spgemm/legacy/csr_scalar_i8.c:24-196
+ * Both accumulate acc[j] += a * b in A-row order from zero and, unlike the
+ * FP32 path, do not store an output entry whose sum is exactly zero.
+ *
  * Every entry point works on a half-open row range [row_begin, row_end) so a
  * test can check sampled rows of a product too large to redo in full.
  */
@@ -266,3 +274,76 @@ int oracle_numeric_f32(int32_t row_begin, int32_t row_end, int32_t n_cols,
     free(acc);
     return ORACLE_OK;
 }
+
+/*
+ * Legacy-dtype products for rows [row_begin, row_end): distinct columns in
+ * ascending order, acc[j] += a * b in A-row order starting from zero, entries
+ * whose sum is zero dropped (csr_scalar_f64.c:226-245, csr_scalar_i8.c:
+ * 131-175). c_rp is relative (c_rp[0] = 0); c_ci / c_v must hold the
+ * symbolic total for the range (an upper bound). INT8 products and sums are
+ * formed in 32-bit two's complement.
+ */
+#define ORACLE_LEGACY(NAME, IN_T, ACC_T, MUL, ADD)                              \
+    int NAME(int32_t row_begin, int32_t row_end, int32_t n_cols,                \
+             const int32_t *a_rp, const int32_t *a_ci, const IN_T *a_v,         \
+             const int32_t *b_rp, const int32_t *b_ci, const IN_T *b_v,         \
+             int64_t *c_rp, int32_t *c_ci, ACC_T *c_v)                          \
+    {                                                                           \
+        size_t n = (size_t)(n_cols > 0 ? n_cols : 1);                           \
+        uint8_t *seen = (uint8_t *)calloc(n, 1);                                \
+        ACC_T *acc = (ACC_T *)calloc(n, sizeof(ACC_T));                         \
+        int32_t *cols = (int32_t *)malloc(n * sizeof(int32_t));                 \
+        if (!seen || !acc || !cols)                                             \
+        {                                                                       \
+            free(seen);                                                         \
+            free(acc);                                                          \
+            free(cols);                                                         \
+            return ORACLE_ERR_ALLOC;                                            \
+        }                                                                       \
+        int64_t pos = 0;                                                        \
+        c_rp[0] = 0;                                                            \
+        for (int32_t r = row_begin; r < row_end; r++)                           \
+        {                                                                       \
+            int32_t m = 0;                                                      \
+            for (int32_t p = a_rp[r]; p < a_rp[r + 1]; p++)                     \
+            {                                                                   \
+                int32_t k = a_ci[p];                                            \
+                for (int32_t q = b_rp[k]; q < b_rp[k + 1]; q++)                 \
+                {                                                               \
+                    int32_t j = b_ci[q];                                        \
+                    if (!seen[j])                                               \
+                    {                                                           \
+                        seen[j] = 1;                                            \
+                        acc[j] = 0;                                             \
+                        cols[m++] = j;                                          \
+                    }                                                           \
+                    acc[j] = ADD(acc[j], MUL(a_v[p], b_v[q]));                  \
+                }                                                               \
+            }                                                                   \
+            qsort(cols, (size_t)m, sizeof(int32_t), cmp_i32);                   \
+            for (int32_t t = 0; t < m; t++)                                     \
+            {                                                                   \
+                int32_t j = cols[t];                                            \
+                if (acc[j] != 0)                                                \
+                {                                                               \
+                    c_ci[pos] = j;                                              \
+                    c_v[pos] = acc[j];                                          \
+                    pos++;                                                      \
+                }                                                               \
+                seen[j] = 0;                                                    \
+            }                                                                   \
+            c_rp[r - row_begin + 1] = pos;                                      \
+        }                                                                       \
+        free(seen);                                                             \
+        free(acc);                                                              \
+        free(cols);                                                             \
+        return ORACLE_OK;                                                       \
+    }
+
+#define MUL_F64(a, b) ((a) * (b))
+#define ADD_F64(x, y) ((x) + (y))
+#define MUL_I8(a, b) ((int32_t)((uint32_t)(int32_t)(a) * (uint32_t)(int32_t)(b)))
+#define ADD_I32(x, y) ((int32_t)((uint32_t)(x) + (uint32_t)(y)))
+
+ORACLE_LEGACY(oracle_spgemm_f64, double, double, MUL_F64, ADD_F64)
+ORACLE_LEGACY(oracle_spgemm_i8, int8_t, int32_t, MUL_I8, ADD_I32)

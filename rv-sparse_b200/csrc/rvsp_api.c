@@ -156,6 +156,68 @@ static int canonical(const rvsp_csr_matrix_t *M)
 /* One-shot (rv-sparse src/core/spgemm.c:135-211)                            */
 /* ------------------------------------------------------------------------ */
 
+/* FP64 x FP64 -> FP64 and INT8 x INT8 -> INT32 one-shot products with the
+ * checks of the reference's legacy wrappers, in their order and with their
+ * codes: INT8 validates both operands, then a dtype mismatch is
+ * UNSUPPORTED_DTYPE (csr_spgemm_wrappers.c:19-50); FP64 reports a dtype
+ * mismatch as INVALID_ARGUMENT (:352-371); both then check the shapes. */
+static rvsp_status_t spgemm_typed(const rvsp_csr_matrix_t *A, const rvsp_csr_matrix_t *B,
+                                  rvsp_csr_matrix_t *C, rvsp_dtype_t in_dt, rvsp_dtype_t out_dt)
+{
+    if (rvsp_cuda_device_count() == 0)
+        return RVSP_ERROR_UNSUPPORTED_BACKEND;
+    if (in_dt == RVSP_DTYPE_INT8)
+    {
+        rvsp_status_t vs = rvsp_csr_validate(A);
+        if (vs == RVSP_SUCCESS)
+            vs = rvsp_csr_validate(B);
+        if (vs != RVSP_SUCCESS)
+            return vs;
+        if (A->dtype != RVSP_DTYPE_INT8 || B->dtype != RVSP_DTYPE_INT8)
+            return RVSP_ERROR_UNSUPPORTED_DTYPE;
+    }
+    else if (A->dtype != RVSP_DTYPE_FP64 || B->dtype != RVSP_DTYPE_FP64)
+    {
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    }
+    if (A->cols != B->rows)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    if (!A->row_ptr || !A->col_idx || !A->values || !B->row_ptr || !B->col_idx || !B->values)
+        return RVSP_ERROR_NULL_POINTER;
+    if (A->rows <= 0 || A->cols <= 0 || B->cols <= 0)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    int32_t *rp = NULL, *ci = NULL, nnz = 0;
+    void *v = NULL;
+    int st;
+    if (in_dt == RVSP_DTYPE_FP64)
+        st = rvsp_cuda_spgemm_f64(A->rows, A->cols, B->cols, A->row_ptr, A->col_idx,
+                                  (const double *)A->values, B->row_ptr, B->col_idx,
+                                  (const double *)B->values, &rp, &ci, (double **)&v, &nnz);
+    else
+        st = rvsp_cuda_spgemm_i8(A->rows, A->cols, B->cols, A->row_ptr, A->col_idx,
+                                 (const int8_t *)A->values, B->row_ptr, B->col_idx,
+                                 (const int8_t *)B->values, &rp, &ci, (int32_t **)&v, &nnz);
+    if (st != RVSP_SUCCESS)
+    {
+        C->row_ptr = NULL;
+        C->col_idx = NULL;
+        C->values = NULL;
+        C->nnz = 0;
+        C->owns_data = 0;
+        return (rvsp_status_t)st;
+    }
+    C->rows = A->rows;
+    C->cols = B->cols;
+    C->nnz = nnz;
+    C->row_ptr = rp;
+    C->col_idx = ci;
+    C->values = v;
+    C->dtype = out_dt;
+    C->format = RVSP_FORMAT_CSR;
+    C->owns_data = rvsp_cuda_is_device_pointer(rp) ? RVSP_OWNS_DEVICE : RVSP_OWNS_HOST;
+    return RVSP_SUCCESS;
+}
+
 rvsp_status_t rvsp_spgemm_csr(const rvsp_csr_matrix_t *A, const rvsp_csr_matrix_t *B,
                               rvsp_csr_matrix_t *C, const rvsp_spgemm_options_t *options)
 {
@@ -170,6 +232,11 @@ rvsp_status_t rvsp_spgemm_csr(const rvsp_csr_matrix_t *A, const rvsp_csr_matrix_
         in_dt = options->input_dtype;
         out_dt = options->output_dtype;
     }
+    /* the reference's other dtypes (its legacy kernels, spgemm.c:181-193) */
+    if (backend == RVSP_BACKEND_CUDA &&
+        ((in_dt == RVSP_DTYPE_FP64 && out_dt == RVSP_DTYPE_FP64) ||
+         (in_dt == RVSP_DTYPE_INT8 && out_dt == RVSP_DTYPE_INT32)))
+        return spgemm_typed(A, B, C, in_dt, out_dt);
     if ((backend != RVSP_BACKEND_CUDA && backend != RVSP_BACKEND_CUDA_LEARNED) ||
         in_dt != RVSP_DTYPE_FP32 || out_dt != RVSP_DTYPE_FP32)
         return RVSP_ERROR_UNSUPPORTED_BACKEND;

@@ -102,6 +102,12 @@ _PROTOS = {
     "rvsp_cuda_spgemm_f32": (C.c_int, [C.c_int, _I32, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP,
                                        C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
                                        C.POINTER(_I32), _VP]),
+    "rvsp_cuda_spgemm_f64": (C.c_int, [_I32, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP,
+                                       C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
+                                       C.POINTER(_I32)]),
+    "rvsp_cuda_spgemm_i8": (C.c_int, [_I32, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP,
+                                      C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
+                                      C.POINTER(_I32)]),
     "rvsp_cuda_csr_check": (C.c_int, [_I32, _I32, _I32, _VP, _VP, C.POINTER(_I32)]),
     "rvsp_cuda_csr_validate": (C.c_int, [_I32, _I32, _I32, _VP, _VP]),
     "rvsp_cuda_launch_count": (_I64, []),

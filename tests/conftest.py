@@ -91,3 +91,35 @@ def gpu_lib():
     if rvsp_b200.device_count() == 0:
         pytest.skip("no CUDA device")
     return rvsp_b200
+
+
+class TypedMat:
+    """CSR with values of any dtype (the legacy FP64 / INT8 products)."""
+
+    def __init__(self, rows, cols, row_ptr, col_idx, values):
+        self.rows, self.cols = int(rows), int(cols)
+        self.row_ptr = np.ascontiguousarray(row_ptr, np.int32)
+        self.col_idx = np.ascontiguousarray(col_idx, np.int32)
+        self.values = np.ascontiguousarray(values)
+
+    @property
+    def nnz(self):
+        return int(self.row_ptr[-1])
+
+
+def typed_pair(A, B, dtype, seed=0):
+    """A and B's structure with values drawn from a small set, so that some
+    output sums cancel to exactly zero (dtype "f64": +-{0.5, 1, 2}, "i8":
+    -3..3 without 0, and a few -128/127 entries)."""
+    rng = np.random.default_rng(seed)
+
+    def vals(n):
+        if dtype == "f64":
+            return rng.choice([-2.0, -1.0, -0.5, 0.5, 1.0, 2.0], n).astype(np.float64)
+        v = rng.choice([-3, -2, -1, 1, 2, 3], n).astype(np.int8)
+        if n:
+            v[rng.integers(0, n, max(1, n // 500))] = rng.choice([-128, 127])
+        return v
+
+    return (TypedMat(A.rows, A.cols, A.row_ptr, A.col_idx, vals(A.nnz)),
+            TypedMat(B.rows, B.cols, B.row_ptr, B.col_idx, vals(B.nnz)))

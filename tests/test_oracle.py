@@ -94,3 +94,25 @@ def test_oracle_vs_live_reference_rmat():
     assert np.array_equal(orp, rrp.astype(np.int64))
     assert np.array_equal(oci, rci)
     assert np.array_equal(ov.view(np.uint32), rv.view(np.uint32))
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("dtype", ["f64", "i8"])
+def test_legacy_dtypes_match_reference(dtype):
+    """FP64 and INT8 -> INT32 restatements against the reference's own legacy
+    kernels: same structure after zero-sum entries are dropped, values bit for bit."""
+    from conftest import typed_pair
+    cases = [gen.rmat(scale=10, edge_factor=8, seed=2), gen.uniform_fixed(600, 500, 9, seed=4)]
+    for M in cases:
+        A, B = typed_pair(M, M, dtype, seed=7)
+        rrp, rci, rv, st = oracle.ref_spgemm_typed(A, B, dtype)
+        assert st == 0
+        orp, oci, ov = oracle.spgemm_typed(A, B, dtype)
+        assert np.array_equal(orp, rrp.astype(np.int64))
+        assert np.array_equal(oci, rci)
+        if dtype == "f64":
+            assert np.array_equal(ov.view(np.uint64), rv.view(np.uint64))
+        else:
+            assert np.array_equal(ov, rv)
+        _, cnt = oracle.symbolic(A, B)
+        assert int(orp[-1]) < int(cnt.sum())  # some sums cancelled and were dropped
