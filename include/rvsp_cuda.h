@@ -208,6 +208,38 @@ RVSP_CUDA_API int rvsp_cuda_spgemm_i8(int32_t a_rows, int32_t a_cols, int32_t b_
                          int32_t *c_nnz_out);
 
 /*
+ * COO -> canonical CSR on the device. Replaces the canonicalisation half of
+ * the reference's Matrix Market loader assemble_csr_matrix (rv-sparse
+ * tools/include/mtx_to_csr_formatter.h:12; tools/src/mtx_to_csr_formatter.c:
+ * 219-330 with canonicalise_rows :74-151): with symmetric != 0 every
+ * off-diagonal entry's mirror is appended after all stored entries; entries
+ * are ordered by (row, column), stably, so repeated (row, column) entries
+ * keep their COO order and are summed left to right from the first value;
+ * columns ascending within a row. Indices are 0-based; coo_val may be NULL
+ * (every value 1.0f, a "pattern" file). Inputs may be host or device memory;
+ * outputs are allocated on the device when device_out is nonzero (release
+ * with rvsp_cuda_free), with malloc otherwise. An index out of range returns
+ * RVSP_ERROR_INVALID_ARGUMENT (the reference does not check).
+ */
+RVSP_CUDA_API int rvsp_cuda_coo_to_csr(int32_t rows, int32_t cols, int64_t n,
+                         const int32_t *coo_row, const int32_t *coo_col, const float *coo_val,
+                         int symmetric, int device_out, int32_t **row_ptr, int32_t **col_idx,
+                         float **values, int32_t *nnz_out);
+
+/*
+ * Matrix Market files. rvsp_cuda_mtx_read is the parsing half of
+ * assemble_csr_matrix (mtx_to_csr_formatter.c:153-217: banner "pattern" and
+ * "symmetric", comment lines, "M N L", up to L 1-based entries read with the
+ * same scanf formats) into malloc'd 0-based COO arrays; rvsp_cuda_mtx_to_csr
+ * reads a file and canonicalises it with rvsp_cuda_coo_to_csr.
+ */
+RVSP_CUDA_API int rvsp_cuda_mtx_read(const char *path, int32_t *rows, int32_t *cols, int64_t *n,
+                       int32_t **coo_row, int32_t **coo_col, float **coo_val, int *symmetric);
+RVSP_CUDA_API int rvsp_cuda_mtx_to_csr(const char *path, int device_out, int32_t *rows,
+                         int32_t *cols, int32_t *nnz, int32_t **row_ptr, int32_t **col_idx,
+                         float **values);
+
+/*
  * Canonical-CSR check on the device. Replaces rvsp_csr_check
  * (rv-sparse src/kernels/spgemm/rvsp_support.c:37-127) with the same result
  * codes (0 ok, 1 bad row_ptr, 2 column out of range, 3 unsorted,

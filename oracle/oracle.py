@@ -87,6 +87,9 @@ def lib():
         L.oracle_spgemm_i8.argtypes = [C.c_int32, C.c_int32, C.c_int32,
                                        _i32p, _i32p, _i8p, _i32p, _i32p, _i8p,
                                        _i64p, _i32p, _i32p]
+        L.oracle_coo_to_csr.restype = C.c_int64
+        L.oracle_coo_to_csr.argtypes = [C.c_int32, C.c_int32, C.c_int64, _i32p, _i32p, C.c_void_p,
+                                        C.c_int, _i64p, _i32p, _f32p]
         L.oracle_numeric_f32.restype = C.c_int
         L.oracle_numeric_f32.argtypes = [C.c_int32, C.c_int32, C.c_int32,
                                          _i32p, _i32p, _f32p, _i32p, _i32p, _f32p,
@@ -124,6 +127,10 @@ def ref():
             fn.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                            C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p),
                            C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int32)]
+        L.ref_mtx_load.restype = C.c_int
+        L.ref_mtx_load.argtypes = [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                   C.POINTER(C.c_void_p)]
         L.rvsp_csr_check.restype = C.c_int
         L.rvsp_csr_check.argtypes = [C.c_int32, C.c_int32, _i32p, _i32p, C.POINTER(C.c_int32)]
         _ref = L
@@ -346,3 +353,42 @@ def ref_spgemm_typed(A, B, dtype):
     for p in (p_rp, p_ci, p_v):
         L.ref_free(p)
     return rp, ci, v, 0
+
+
+def coo_to_csr(rows, cols, coo_row, coo_col, coo_val=None, symmetric=False):
+    """Canonical CSR of a COO list the way the reference's Matrix Market loader
+    builds it (mirrors appended, stable (row, col) order, runs summed from their
+    first value); returns (row_ptr int64, col_idx, values)."""
+    r = np.ascontiguousarray(coo_row, np.int32)
+    c = np.ascontiguousarray(coo_col, np.int32)
+    n = r.size
+    cap = max(2 * n, 1)
+    rp = np.zeros(rows + 1, np.int64)
+    ci = np.zeros(cap, np.int32)
+    v = np.zeros(cap, np.float32)
+    vv = None if coo_val is None else np.ascontiguousarray(coo_val, np.float32)
+    m = lib().oracle_coo_to_csr(rows, cols, n, _nz(r), _nz(c),
+                                None if vv is None else _nz(vv).ctypes.data, 1 if symmetric else 0,
+                                rp, ci, v)
+    if m < 0:
+        raise ValueError(f"oracle_coo_to_csr failed: {m}")
+    return rp, ci[:m], v[:m]
+
+
+def ref_mtx_load(path):
+    """The reference's own loader (assemble_csr_matrix) on a file: (row_ptr, col_idx, values)."""
+    L = ref()
+    rows, nnz = C.c_int32(), C.c_int32()
+    prp, pci, pv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    if L.ref_mtx_load(path.encode(), C.byref(rows), C.byref(nnz), C.byref(prp), C.byref(pci),
+                      C.byref(pv)) != 0:
+        raise RuntimeError("reference loader failed")
+    n = nnz.value
+    rp = np.ctypeslib.as_array(C.cast(prp, C.POINTER(C.c_int32)), (rows.value + 1,)).copy()
+    ci = (np.ctypeslib.as_array(C.cast(pci, C.POINTER(C.c_int32)), (n,)).copy()
+          if n else np.zeros(0, np.int32))
+    v = (np.ctypeslib.as_array(C.cast(pv, C.POINTER(C.c_float)), (n,)).copy()
+         if n else np.zeros(0, np.float32))
+    for p in (prp, pci, pv):
+        L.ref_free(p)
+    return rp, ci, v

@@ -23,6 +23,7 @@
 #include <string.h>
 #include <time.h>
 
+#include "mtx_to_csr_formatter.h"
 #include "rv_sparse.h"
 #include "rvsp_spgemm.h"
 
@@ -56,6 +57,32 @@ int ref_spgemm_raw(int32_t a_rows, int32_t a_cols, int32_t b_cols,
 void ref_free(void *p)
 {
     free(p);
+}
+
+/* The reference's Matrix Market loader (tools/src/mtx_to_csr_formatter.c:
+ * 153-330); its CSR arrays copied into malloc'd ones. */
+int ref_mtx_load(const char *path, int32_t *rows, int32_t *nnz, int32_t **rp, int32_t **ci,
+                 float **v)
+{
+    struct CSR m = assemble_csr_matrix(path);
+    if (!m.row_ptr || !m.col_ind || !m.val)
+        return -1;
+    size_t nr = vector_size(m.row_ptr), nz = vector_size(m.col_ind);
+    *rows = (int32_t)nr - 1;
+    *nnz = (int32_t)nz;
+    *rp = (int32_t *)malloc(nr * sizeof(int32_t));
+    *ci = (int32_t *)malloc((nz ? nz : 1) * sizeof(int32_t));
+    *v = (float *)malloc((nz ? nz : 1) * sizeof(float));
+    if (*rp && *ci && *v)
+    {
+        memcpy(*rp, m.row_ptr->data, nr * sizeof(int32_t));
+        memcpy(*ci, m.col_ind->data, nz * sizeof(int32_t));
+        memcpy(*v, m.val->data, nz * sizeof(float));
+    }
+    vector_free(m.row_ptr);
+    vector_free(m.col_ind);
+    vector_free(m.val);
+    return (*rp && *ci && *v) ? 0 : -6;
 }
 
 typedef struct

@@ -34,6 +34,10 @@
  * Both accumulate acc[j] += a * b in A-row order from zero and, unlike the
  * FP32 path, do not store an output entry whose sum is exactly zero.
  *
+ * The canonicalisation of the reference's Matrix Market loader (COO ->
+ * sorted CSR with repeated entries summed) is restated as oracle_coo_to_csr
+ *       rv-sparse tools/src/mtx_to_csr_formatter.c:219-330, :74-151
+ *
  * Every entry point works on a half-open row range [row_begin, row_end) so a
  * test can check sampled rows of a product too large to redo in full.
  */
@@ -347,3 +351,90 @@ int oracle_numeric_f32(int32_t row_begin, int32_t row_end, int32_t n_cols,
 
 ORACLE_LEGACY(oracle_spgemm_f64, double, double, MUL_F64, ADD_F64)
 ORACLE_LEGACY(oracle_spgemm_i8, int8_t, int32_t, MUL_I8, ADD_I32)
+
+/*
+ * COO -> canonical CSR (mtx_to_csr_formatter.c:219-330 with canonicalise_rows
+ * :74-151): with symmetric, every off-diagonal entry's mirror is appended
+ * after all stored entries (:221-244); entries are ordered by (row, column)
+ * keeping COO order among equal pairs (row buckets filled in COO order,
+ * :286-300, then a stable sort by column); each run of equal pairs is summed
+ * left to right from its first value (:120-131). coo_val may be NULL (1.0f
+ * each). c_rp has rows + 1 entries; c_ci / c_v hold up to 2n entries.
+ * Returns the output nnz, or a negative code.
+ */
+typedef struct
+{
+    int64_t key;
+    int64_t idx;
+} oracle_ki_t;
+
+static int cmp_ki(const void *x, const void *y)
+{
+    const oracle_ki_t *a = (const oracle_ki_t *)x, *b = (const oracle_ki_t *)y;
+    if (a->key != b->key)
+        return (a->key > b->key) - (a->key < b->key);
+    return (a->idx > b->idx) - (a->idx < b->idx);
+}
+
+int64_t oracle_coo_to_csr(int32_t rows, int32_t cols, int64_t n, const int32_t *coo_row,
+                          const int32_t *coo_col, const float *coo_val, int symmetric,
+                          int64_t *c_rp, int32_t *c_ci, float *c_v)
+{
+    int64_t m = n;
+    if (symmetric)
+        for (int64_t k = 0; k < n; k++)
+            m += coo_row[k] != coo_col[k];
+    oracle_ki_t *e = (oracle_ki_t *)malloc((size_t)(m > 0 ? m : 1) * sizeof(oracle_ki_t));
+    float *val = (float *)malloc((size_t)(m > 0 ? m : 1) * sizeof(float));
+    if (!e || !val)
+    {
+        free(e);
+        free(val);
+        return ORACLE_ERR_ALLOC;
+    }
+    int64_t t = 0;
+    for (int64_t k = 0; k < n; k++)
+    {
+        if (coo_row[k] < 0 || coo_row[k] >= rows || coo_col[k] < 0 || coo_col[k] >= cols)
+        {
+            free(e);
+            free(val);
+            return ORACLE_ERR_INVALID;
+        }
+        e[t].key = (int64_t)coo_row[k] * cols + coo_col[k];
+        e[t].idx = t;
+        val[t] = coo_val ? coo_val[k] : 1.0f;
+        t++;
+    }
+    if (symmetric)
+        for (int64_t k = 0; k < n; k++)
+            if (coo_row[k] != coo_col[k])
+            {
+                e[t].key = (int64_t)coo_col[k] * cols + coo_row[k];
+                e[t].idx = t;
+                val[t] = coo_val ? coo_val[k] : 1.0f;
+                t++;
+            }
+    qsort(e, (size_t)m, sizeof(oracle_ki_t), cmp_ki);
+    int64_t out = 0;
+    for (int32_t r = 0; r <= rows; r++)
+        c_rp[r] = 0;
+    for (int64_t i = 0; i < m;)
+    {
+        const int64_t key = e[i].key;
+        float acc = val[e[i].idx];
+        int64_t j = i + 1;
+        for (; j < m && e[j].key == key; j++)
+            acc += val[e[j].idx];
+        c_ci[out] = (int32_t)(key % cols);
+        c_v[out] = acc;
+        c_rp[key / cols + 1]++;
+        out++;
+        i = j;
+    }
+    for (int32_t r = 0; r < rows; r++)
+        c_rp[r + 1] += c_rp[r];
+    free(e);
+    free(val);
+    return out;
+}

@@ -108,6 +108,15 @@ _PROTOS = {
     "rvsp_cuda_spgemm_i8": (C.c_int, [_I32, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP,
                                       C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
                                       C.POINTER(_I32)]),
+    "rvsp_cuda_coo_to_csr": (C.c_int, [_I32, _I32, _I64, _VP, _VP, _VP, C.c_int, C.c_int,
+                                       C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
+                                       C.POINTER(_I32)]),
+    "rvsp_cuda_mtx_read": (C.c_int, [C.c_char_p, C.POINTER(_I32), C.POINTER(_I32),
+                                     C.POINTER(_I64), C.POINTER(_VP), C.POINTER(_VP),
+                                     C.POINTER(_VP), C.POINTER(C.c_int)]),
+    "rvsp_cuda_mtx_to_csr": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_I32), C.POINTER(_I32),
+                                       C.POINTER(_I32), C.POINTER(_VP), C.POINTER(_VP),
+                                       C.POINTER(_VP)]),
     "rvsp_cuda_csr_check": (C.c_int, [_I32, _I32, _I32, _VP, _VP, C.POINTER(_I32)]),
     "rvsp_cuda_csr_validate": (C.c_int, [_I32, _I32, _I32, _VP, _VP]),
     "rvsp_cuda_launch_count": (_I64, []),
@@ -436,6 +445,34 @@ def spgemm_batched(pairs_dev, algo=RVSP_CUDA_ALGO_EXACT):
                                         C.byref(pci), C.byref(pv), C.byref(nnz), offs.ctypes.data)
     check(st, "rvsp_cuda_spgemm_batched_f32")
     return (prp.value, pci.value, pv.value), nnz.value, offs
+
+
+_libc = None
+
+
+def _host_array(p, n, ctype, np_dtype):
+    """Copy n elements of a library-malloc'd host array and free it."""
+    global _libc
+    if _libc is None:
+        _libc = C.CDLL(None)
+        _libc.free.argtypes = [C.c_void_p]
+    out = (np.ctypeslib.as_array(C.cast(p, C.POINTER(ctype)), (n,)).copy()
+           if n else np.zeros(0, np_dtype))
+    _libc.free(p)
+    return out
+
+
+def mtx_read(path):
+    """Matrix Market file -> (rows, cols, coo_row, coo_col, coo_val, symmetric),
+    0-based COO, parsed by the library's C reader."""
+    rows, cols, n, sym = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int()
+    pr, pc, pv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    check(lib().rvsp_cuda_mtx_read(str(path).encode(), C.byref(rows), C.byref(cols), C.byref(n),
+                                   C.byref(pr), C.byref(pc), C.byref(pv), C.byref(sym)), "mtx_read")
+    k = n.value
+    return (rows.value, cols.value, _host_array(pr, k, C.c_int32, np.int32),
+            _host_array(pc, k, C.c_int32, np.int32), _host_array(pv, k, C.c_float, np.float32),
+            bool(sym.value))
 
 
 def free_device(*ptrs):

@@ -123,3 +123,51 @@ def typed_pair(A, B, dtype, seed=0):
 
     return (TypedMat(A.rows, A.cols, A.row_ptr, A.col_idx, vals(A.nnz)),
             TypedMat(B.rows, B.cols, B.row_ptr, B.col_idx, vals(B.nnz)))
+
+
+def write_mtx(path, rows, cols, entries, field="real", symmetry="general", declared=None):
+    """A Matrix Market file; entries are (row, col[, value]) 1-based, value a
+    string written as is."""
+    with open(path, "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate {field} {symmetry}\n")
+        f.write("% written by the tests\n%\n")
+        f.write(f"{rows} {cols} {len(entries) if declared is None else declared}\n")
+        for e in entries:
+            f.write(" ".join(str(x) for x in e) + "\n")
+
+
+def mtx_cases(tmpdir, seed=0):
+    """Seeded files: general real with repeated entries (pairs and triples),
+    symmetric real, pattern general, and a short file (fewer entries than declared)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    rows, cols = 300, 200
+    n = 4000
+    r = rng.integers(1, rows + 1, n)
+    c = rng.integers(1, cols + 1, n)
+    dup = rng.integers(0, n, 300)  # repeat some entries once or twice more
+    r = np.concatenate([r, r[dup], r[dup[:100]]])
+    c = np.concatenate([c, c[dup], c[dup[:100]]])
+    vals = [f"{x:.7g}" for x in rng.uniform(-10, 10, r.size)]
+    perm = rng.permutation(r.size)
+    ents = [(int(r[i]), int(c[i]), vals[i]) for i in perm]
+    p = os.path.join(tmpdir, "general.mtx")
+    write_mtx(p, rows, cols, ents)
+    out.append(("general", p))
+    m = 250
+    rr = rng.integers(1, m + 1, 3000)
+    cc = rng.integers(1, m + 1, 3000)
+    lo, hi = np.minimum(rr, cc), np.maximum(rr, cc)
+    ents = [(int(hi[i]), int(lo[i]), f"{rng.uniform(-1, 1):.6e}") for i in range(rr.size)]
+    p = os.path.join(tmpdir, "symmetric.mtx")
+    write_mtx(p, m, m, ents, symmetry="symmetric")
+    out.append(("symmetric", p))
+    ents = [(int(rng.integers(1, 120)), int(rng.integers(1, 90))) for _ in range(900)]
+    p = os.path.join(tmpdir, "pattern.mtx")
+    write_mtx(p, 119, 89, ents, field="pattern")
+    out.append(("pattern", p))
+    ents = [(1, 1, "2.5"), (3, 2, "-1"), (3, 2, "4")]
+    p = os.path.join(tmpdir, "short.mtx")
+    write_mtx(p, 3, 3, ents, declared=10)
+    out.append(("short", p))
+    return out

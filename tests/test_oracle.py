@@ -116,3 +116,20 @@ def test_legacy_dtypes_match_reference(dtype):
             assert np.array_equal(ov, rv)
         _, cnt = oracle.symbolic(A, B)
         assert int(orp[-1]) < int(cnt.sum())  # some sums cancelled and were dropped
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built")
+def test_coo_canonicalisation_matches_reference_loader(tmp_path):
+    """The oracle's COO -> CSR restatement against the reference's own Matrix
+    Market loader on seeded files (repeated entries up to three times,
+    symmetric expansion, pattern values, a short file); the files are parsed by
+    the library's C reader (host code only)."""
+    import rvsp_b200 as rv
+    from conftest import mtx_cases
+    for name, path in mtx_cases(str(tmp_path)):
+        rows, cols, r, c, v, sym = rv.mtx_read(path)
+        wrp, wci, wv = oracle.ref_mtx_load(path)
+        orp, oci, ov = oracle.coo_to_csr(rows, cols, r, c, v, sym)
+        assert np.array_equal(orp, wrp.astype(np.int64)), name
+        assert np.array_equal(oci, wci), name
+        assert np.array_equal(ov.view(np.uint32), wv.view(np.uint32)), name
