@@ -2,7 +2,7 @@
 """FP32 CSR SpGEMM benchmark on B200 (one process per GPU).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload poisson_reuse|plain|batched|tall_skinny|rmat]
+                    [--workload poisson_reuse|plain|batched|tall_skinny|rmat|coo]
 
 Default workload (the descriptor-reuse case): C = A * A for the 5-point
 Laplacian on a 1024 x 1024 grid (N = 1,048,576, nnz(A) = 5,238,784,
@@ -554,6 +554,69 @@ def run_rmat(args, rv, gen, torch):
     }
 
 
+def run_coo(args, rv, torch):
+    """COO -> canonical CSR (the Matrix Market loader's canonicalisation) of an
+    R-MAT 2^scale edge list with its repeated edges, device in and out."""
+    import ctypes as C
+    import oracle
+    rng = np.random.default_rng(0)
+    scale, ef = args.rmat_scale, 16
+    n = ef << scale
+    r = np.zeros(n, np.int64)
+    c = np.zeros(n, np.int64)
+    for bit in range(scale):  # the R-MAT recursion of rvsp_b200.gen.rmat, duplicates kept
+        u = rng.random(n)
+        r |= (u >= 0.76).astype(np.int64) << bit
+        c |= (((u >= 0.57) & (u < 0.76)) | (u >= 0.95)).astype(np.int64) << bit
+    r = r.astype(np.int32)
+    c = c.astype(np.int32)
+    v = rng.uniform(-1, 1, n).astype(np.float32)
+    m = 1 << scale
+    dr, dc, dv = (torch.from_numpy(x).cuda() for x in (r, c, v))
+    L = rv.lib()
+    out = {}
+
+    def once():
+        prp, pci, pv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        nnz = C.c_int32()
+        rv.check(L.rvsp_cuda_coo_to_csr(m, m, n, dr.data_ptr(), dc.data_ptr(), dv.data_ptr(), 0, 1,
+                                        C.byref(prp), C.byref(pci), C.byref(pv), C.byref(nnz)),
+                 "coo_to_csr")
+        out["nnz"] = nnz.value
+        out["ptrs"] = (prp.value, pci.value, pv.value)
+
+    def step():
+        once()
+        rv.free_device(*out["ptrs"])
+
+    t = _time(step, args.steps, args.warmup, torch)
+    once()
+    rp = _d2h(out["ptrs"][0], m + 1, np.int32, torch)
+    ci = _d2h(out["ptrs"][1], out["nnz"], np.int32, torch)
+    vv = _d2h(out["ptrs"][2], out["nnz"], np.float32, torch)
+    rv.free_device(*out["ptrs"])
+    t0 = time.perf_counter()
+    wrp, wci, wv = oracle.coo_to_csr(m, m, r, c, v, False)
+    t_cpu = time.perf_counter() - t0
+    same = (np.array_equal(rp.astype(np.int64), wrp) and np.array_equal(ci, wci) and
+            np.array_equal(vv.view(np.uint32), wv.view(np.uint32)))
+    bits = 2 * scale
+    passes = (bits + 7) // 8
+    # per entry: COO in (12 B), keys + payload written (16 B), each radix pass
+    # reads and writes them (32 B), the run sums read them (16 B), CSR out (8 B)
+    per_entry = 12 + 16 + 32 * passes + 16 + 8
+    hbm, kind = peaks()
+    return {"config": {"workload": f"coo_to_csr_rmat{scale}_edges_with_repeats", "entries": n,
+                       "rows": m, "nnz_out": out["nnz"], "radix_passes": passes},
+            "ms": t * 1e3, "entries_per_s": n / t,
+            "roofline": {"bound": "hbm", "bytes_per_entry": per_entry,
+                         "achieved_gbs": per_entry * n / t / 1e9, "peak": hbm,
+                         "frac": per_entry * n / t / 1e9 / hbm, "peak_source": f"{kind} hbm_gbs"},
+            "cpu_baseline": {"ms": t_cpu * 1e3, "cores": 1, "kind": "port",
+                             "sample": "the oracle's canonicalisation of the same list, once"},
+            "bit_exact_vs_oracle": bool(same)}
+
+
 def run_compare(args):
     """One-shot exact vs learned (and batched vs sequential) on a BASELINE config."""
     import torch
@@ -613,6 +676,8 @@ def run_compare(args):
                                        "p99": float(np.quantile(e, 0.99)), "rows_sampled": 400}
     elif args.workload == "rmat":
         res = run_rmat(args, rv, gen, torch)
+    elif args.workload == "coo":
+        res = run_coo(args, rv, torch)
     elif args.workload == "batched":
         pairs = gen.batched_uneven(count=args.batch_count)
         prods = [gen.products(A, B) for A, B in pairs]
@@ -676,7 +741,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson_reuse",
-                    choices=["poisson_reuse", "plain", "batched", "tall_skinny", "rmat"])
+                    choices=["poisson_reuse", "plain", "batched", "tall_skinny", "rmat", "coo"])
     ap.add_argument("--rmat-scale", type=int, default=20)
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--ts-rows", type=int, default=2_000_000)

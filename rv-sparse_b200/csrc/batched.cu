@@ -163,6 +163,7 @@ extern "C" int rvsp_cuda_spgemm_batched_f32(
         plan->map_policy = 0;
     }
     plan->params = default_params();
+    keep_pool_memory();
     std::vector<int32_t> a_shift(count), b_rows(count);
     int64_t kshift = 0;
     int32_t max_n = 1;

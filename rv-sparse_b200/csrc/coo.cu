@@ -226,6 +226,7 @@ extern "C" int rvsp_cuda_coo_to_csr(int32_t rows, int32_t cols, int64_t n, const
     }
     rvsp_cuda_plan_t plan = t_cplan;
     cudaStream_t s = plan->stream;
+    keep_pool_memory();
     cudaError_t e;
     if ((e = plan->misc.ensure(sizeof(Misc))) != cudaSuccess) return fail(e, "misc");
     Misc* misc = plan->misc.as<Misc>();

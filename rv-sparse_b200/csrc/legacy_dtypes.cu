@@ -284,6 +284,7 @@ int typed_spgemm(int32_t a_rows, int32_t a_cols, int32_t b_cols, const int32_t* 
     }
     rvsp_cuda_plan_t plan = t_tplan;
     plan->params = default_params();
+    keep_pool_memory();
     cudaStream_t s = plan->stream;
     const bool dev = is_dev(a_rp);
     cudaError_t e;

@@ -84,6 +84,7 @@ inline void trace_point(const char* what) {
 bool is_dev(const void* p);
 void init_kernel_attributes();
 BinParams default_params();  // the process-wide default of new and internal plans
+void keep_pool_memory();     // the device pool keeps freed blocks (one-shot entry points)
 
 }  // namespace rvsp
 

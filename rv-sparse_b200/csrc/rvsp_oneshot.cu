@@ -39,6 +39,12 @@ thread_local PlanReaper t_reaper;
 
 std::once_flag g_pool_once;
 
+}  // namespace
+
+namespace rvsp {
+// The stream-ordered pool of the current device keeps freed blocks instead
+// of returning them at every synchronisation, so repeated calls reuse memory
+// instead of mapping it again.
 void keep_pool_memory() {
     std::call_once(g_pool_once, [] {
         int dev = 0;
@@ -50,6 +56,9 @@ void keep_pool_memory() {
         cudaGetLastError();
     });
 }
+}  // namespace rvsp
+
+namespace {
 
 int read_i32(const int32_t* p, int32_t* out) {
     if (is_dev(p)) {
