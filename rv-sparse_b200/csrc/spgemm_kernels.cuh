@@ -1167,6 +1167,16 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
     unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * cw));
 
     (void)warps;
+    // The accumulator and the bitmap start at zero once; every item clears
+    // what it set (COUNT and FILL while reading the bitmap out, REUSE by
+    // zeroing its chunk), so no item pays for zeroing a whole chunk.
+    if (MODE != COUNT) {
+        float4* a4 = reinterpret_cast<float4*>(acc);
+        for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (MODE != REUSE)
+        for (int x = lane; x < nw; x += 32) bits[x] = 0u;
+    __syncwarp();
     for (;;) {
         // items are pulled one at a time, so a warp that drew a light item
         // takes the next one instead of idling beside a heavy one
@@ -1179,13 +1189,11 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
         if (ctl.only && !ctl.only[row]) continue;
         const int lo = it.chunk << cw_log2;
         const int hi = (int)min((int64_t)lo + cw, (int64_t)B.cols);
-        if (MODE != COUNT) {
+        if (MODE == REUSE) {
             float4* a4 = reinterpret_cast<float4*>(acc);
             for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
+            __syncwarp();
         }
-        if (MODE != REUSE)
-            for (int x = lane; x < nw; x += 32) bits[x] = 0u;
-        __syncwarp();
         int a0, a1;
         row_range(A, row, &a0, &a1, err);
         for (int base = a0; base < a1; base += 32) {
@@ -1299,7 +1307,10 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
         __syncwarp();
         if (MODE == COUNT) {
             int c = 0;
-            for (int x = lane; x < nw; x += 32) c += __popc(bits[x]);
+            for (int x = lane; x < nw; x += 32) {
+                c += __popc(bits[x]);
+                bits[x] = 0u;
+            }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
             if (lane == 0) {
@@ -1311,7 +1322,11 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
             // words' popcounts give each lane its first output position
             int64_t out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
             for (int x0 = 0; x0 < nw; x0 += 32) {
-                unsigned word = x0 + lane < nw ? bits[x0 + lane] : 0u;
+                unsigned word = 0u;
+                if (x0 + lane < nw) {
+                    word = bits[x0 + lane];
+                    bits[x0 + lane] = 0u;
+                }
                 const int pc = __popc(word);
                 const int incl = warp_incl_scan(pc);
                 int64_t pos = out + (incl - pc);
@@ -1321,6 +1336,7 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
                     const int col = (x0 + lane) * 32 + b;
                     c_ci[pos] = lo + col;
                     c_v[pos] = acc[col];
+                    acc[col] = 0.0f;
                     ++pos;
                 }
                 out += __shfl_sync(FULL, incl, 31);
