@@ -651,6 +651,11 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
                       &p->lbin_rows, &p->need, &p->pflag, &p->bmeta, &p->bdcount,
                       &p->bdscan, &p->bdoff, &p->bdir};
     for (DevBuf* b : bufs) b->release();
+    if (p->side) {
+        cudaStreamSynchronize(p->side);
+        cudaStreamDestroy(p->side);
+    }
+    if (p->side_fork) cudaEventDestroy(p->side_fork);
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;
 }
@@ -760,6 +765,30 @@ int rvsp_cuda_symbolic(rvsp_cuda_plan_t plan, int32_t a_rows, int32_t a_cols, in
     return RVSP_SUCCESS;
 }
 
+// Waits, when it goes out of scope, for the side stream's copy into the
+// caller's host memory.
+struct SideCopy {
+    cudaStream_t s = nullptr;
+    ~SideCopy() {
+        if (s) cudaStreamSynchronize(s);
+    }
+};
+
+static bool side_stream(rvsp_cuda_plan* plan) {
+    if (plan->side) return true;
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        if (s) cudaStreamDestroy(s);
+        cudaGetLastError();
+        return false;  // the copy stays on the plan's stream
+    }
+    plan->side = s;
+    plan->side_fork = ev;
+    return true;
+}
+
 int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t* a_ci,
                       const float* a_v, const int32_t* b_rp, const int32_t* b_ci,
                       const float* b_v, int32_t* c_rp, int32_t* c_ci, float* c_v,
@@ -768,17 +797,29 @@ int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t*
     if (!plan || !a_rp || !b_rp || !c_rp || !c_ci || !c_v) return RVSP_ERROR_NULL_POINTER;
     if (!a_ci || !a_v || !b_ci || !b_v) return RVSP_ERROR_NULL_POINTER;
     if (!plan->analysed) return RVSP_ERROR_INVALID_ARGUMENT;
-    CsrView A, B;
-    int st = stage_operands(plan, a_rp, a_ci, a_v, b_rp, b_ci, b_v, true, &A, &B);
-    if (st) return st;
     cudaError_t e;
     const int64_t M = plan->a_rows, nnz = plan->c_nnz;
     const bool dev_rp = is_dev(c_rp), dev_ci = is_dev(c_ci), dev_v = is_dev(c_v);
-    // row pointer: the analysed structure
-    if ((e = cudaMemcpyAsync(c_rp, plan->c_rp.p, (M + 1) * 4,
-                             dev_rp ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                             plan->stream)) != cudaSuccess)
+    // Row pointer: the analysed structure, final before this call. Into host
+    // memory it is copied on the side stream, so the device->host copy runs
+    // beside the operands' host->device copies (PCIe carries both directions
+    // at once); every return waits for it.
+    SideCopy side_rp;
+    if (!dev_rp && side_stream(plan)) {
+        if ((e = cudaEventRecord(plan->side_fork, plan->stream)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(plan->side, plan->side_fork, 0)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(c_rp, plan->c_rp.p, (M + 1) * 4, cudaMemcpyDeviceToHost,
+                                 plan->side)) != cudaSuccess)
+            return fail(e, "row_ptr copy");
+        side_rp.s = plan->side;
+    } else if ((e = cudaMemcpyAsync(c_rp, plan->c_rp.p, (M + 1) * 4,
+                                    dev_rp ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                    plan->stream)) != cudaSuccess) {
         return fail(e, "row_ptr copy");
+    }
+    CsrView A, B;
+    int st = stage_operands(plan, a_rp, a_ci, a_v, b_rp, b_ci, b_v, true, &A, &B);
+    if (st) return st;
     int32_t* d_ci = c_ci;
     float* d_v = c_v;
     if (!dev_ci) {

@@ -92,6 +92,10 @@ struct rvsp_cuda_plan {
     int algo = 4;
     int async = 0;
     cudaStream_t stream = nullptr;
+    // side stream for a host-resident C row pointer's copy, which overlaps
+    // the operands' host->device copies (created on first use)
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_fork = nullptr;
     bool analysed = false;
     bool capturing = false;
     int32_t a_rows = 0, a_cols = 0, a_nnz = 0, b_rows = 0, b_cols = 0, b_nnz = 0;

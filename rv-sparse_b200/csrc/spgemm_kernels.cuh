@@ -1167,13 +1167,11 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
     extern __shared__ __align__(16) unsigned char smem[];
     const int cw = 1 << cw_log2;
     const int nw = cw >> 5;  // bitmap words
-    const int warps = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = lane_id();
     unsigned char* mine = smem + warp * heavy_smem_bytes(MODE, cw);
     float* acc = reinterpret_cast<float*>(mine);
     unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * cw));
 
-    (void)warps;
     // The accumulator and the bitmap start at zero once; every item clears
     // what it set (COUNT and FILL while reading the bitmap out, REUSE by
     // zeroing its chunk), so no item pays for zeroing a whole chunk.
