@@ -223,8 +223,8 @@ static void launch_warp(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
         int32_t* queue = &plan->misc.as<Misc>()->row_queue;
         cudaMemsetAsync(queue, 0, sizeof(int32_t), plan->stream);
         k_warp<CAP, W, MODE><<<grid, W * 32, W * warp_smem_bytes<CAP, MODE>(), plan->stream>>>(
-            A, B, rows, n, o.cnt, o.c_rp, o.c_ci, o.c_v, o.maps ? lo : nullptr,
-            o.maps ? pm : nullptr, o.err, o.ctl, queue);
+            A, B, rows, n, plan->ops.as<int64_t>(), o.cnt, o.c_rp, o.c_ci, o.c_v,
+            o.maps ? lo : nullptr, o.maps ? pm : nullptr, o.err, o.ctl, queue);
     }
     note_launch(plan, 1);
 }

@@ -805,7 +805,8 @@ __device__ void warp_radix_sort(int32_t* keys, int32_t* tmp, int n, int32_t* his
 template <int CAP, int WARPS, int MODE>
 __global__ void __launch_bounds__(WARPS * 32)
     k_warp(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
-           int32_t* __restrict__ cnt, const int32_t* __restrict__ c_rp,
+           const int64_t* __restrict__ ops, int32_t* __restrict__ cnt,
+           const int32_t* __restrict__ c_rp,
            int32_t* __restrict__ c_ci, float* __restrict__ c_v,
            const int32_t* __restrict__ list_off, uint16_t* __restrict__ pm,
            int32_t* __restrict__ err, RowCtl ctl, int32_t* __restrict__ queue) {
@@ -839,7 +840,72 @@ __global__ void __launch_bounds__(WARPS * 32)
             n = min(c_rp[row + 1] - (int)o, CAP);
             for (int x = lane; x < n; x += 32) keys[x] = c_ci[o + x];
         } else {
-            if (MODE == FILL && !pm) {
+            bool wide = false;  // columns span 2^20 or more: the two-walk path
+            if (MODE == FILL && !pm && !learned && ops[row] <= CAP &&
+                2 * (int64_t)(c_rp[row + 1] - c_rp[row]) >= ops[row]) {
+                // Every product fits the table and at most every other one
+                // repeats a column: expand, sort, compress. Each product's
+                // column and value go to its row-local index; a stable sort
+                // of packed (column - min) << 12 | index words brings equal
+                // columns together in A-row order, and each run is summed
+                // left to right from +0.0f, the reference's order. No
+                // hashing, no ordered combine, no compaction; the sort holds
+                // the products instead of the distinct columns, which costs
+                // more than the hashing saves once most products repeat.
+                const int P = (int)ops[row];
+                int mn = INT_MAX, mx = INT_MIN;
+                walk_products<true>(A, B, a0, a1, err, [&](int k, bool pv, int col, float bv,
+                                                           float av, bool) {
+                    if (pv && k < P) {
+                        keys[k] = col;
+                        vals[k] = __fmul_rn(av, bv);
+                        mn = min(mn, col);
+                        mx = max(mx, col);
+                    } else if (pv) {
+                        atomicOr(err, ERR_STRUCTURE);  // more products than analysed
+                    }
+                    return false;
+                });
+                __syncwarp();
+                mn = __reduce_min_sync(FULL, mn);
+                mx = __reduce_max_sync(FULL, mx);
+                const uint32_t range = (uint32_t)mx - (uint32_t)mn;
+                if (mn <= mx && range < (1u << 20)) {
+                    for (int x = lane; x < P; x += 32)
+                        keys[x] = (int32_t)((((uint32_t)keys[x] - (uint32_t)mn) << 12) | (uint32_t)x);
+                    __syncwarp();
+                    const int passes = range < (1u << 8) ? 1 : range < (1u << 16) ? 2 : 3;
+                    if (P > 1) warp_radix_sort_core(keys, sorttmp, P, 0u, 12, passes, hist);
+                    o = c_rp[row];
+                    const int nexp = c_rp[row + 1] - (int)o;
+                    int out = 0;
+                    for (int b0 = 0; b0 < P; b0 += 32) {
+                        const int x = b0 + lane;
+                        const uint32_t w = x < P ? (uint32_t)keys[x] : 0u;
+                        const bool head = x < P && (x == 0 || ((uint32_t)keys[x - 1] >> 12) != (w >> 12));
+                        const unsigned hm = __ballot_sync(FULL, head);
+                        if (head) {
+                            float sum = __fadd_rn(0.0f, vals[w & 4095u]);
+                            for (int y = x + 1; y < P; ++y) {
+                                const uint32_t wy = (uint32_t)keys[y];
+                                if ((wy >> 12) != (w >> 12)) break;
+                                sum = __fadd_rn(sum, vals[wy & 4095u]);
+                            }
+                            const int d = out + __popc(hm & ((1u << lane) - 1));
+                            if (d < nexp) {
+                                c_ci[o + d] = (int32_t)((w >> 12) + (uint32_t)mn);
+                                c_v[o + d] = sum;
+                            }
+                        }
+                        out += __popc(hm);
+                    }
+                    if (out != nexp && lane == 0) atomicOr(err, ERR_STRUCTURE);
+                    __syncwarp();
+                    continue;
+                }
+                wide = mn <= mx;
+            }
+            if (MODE == FILL && !pm && !wide) {
                 // One walk: each product finds or inserts its column's slot
                 // and is added to the slot's accumulator in A-row order; then
                 // the occupied slots are compacted and sorted by column as

@@ -222,6 +222,39 @@ def test_every_bin_matches_oracle(gpu_lib):
     assert_same(out, oracle_full(A, B), "bin sweep descriptor")
 
 
+def _rows_of(rows, cols, per_row, col_pool, rng, vals=True):
+    """CSR with per_row distinct columns a row, drawn from col_pool."""
+    ci = np.concatenate([np.sort(rng.choice(col_pool, per_row, replace=False)) for _ in range(rows)])
+    rp = np.arange(rows + 1) * per_row
+    return Mat(rows, cols, rp, ci, rng.uniform(-1, 1, rows * per_row))
+
+
+def test_warp_rows_fill_paths(gpu_lib):
+    """Warp-table rows take one of three fill paths by what the analysis
+    knows of them: few repeated columns (expand, sort, compress), mostly
+    repeated columns (hash table), columns spanning 2^20 or more (two walks).
+    Each is built here from rows of 20 A entries times 10-entry B rows
+    (200 products, a 256-slot table) and compared with the oracle."""
+    rng = np.random.default_rng(11)
+    A = _rows_of(96, 256, 20, np.arange(256), rng)
+    cases = {
+        "distinct": _rows_of(256, 1 << 16, 10, np.arange(1 << 16), rng),
+        "repeats": _rows_of(256, 4096, 10, np.arange(40) * 97, rng),
+        "wide": _rows_of(256, 1 << 22, 10, np.arange(1 << 22), rng),
+    }
+    for name, B in cases.items():
+        ops = gen.row_products(A, B)
+        assert (ops == 200).all() and B.cols > 200, name
+        want = oracle_full(A, B)
+        nnz = np.diff(np.asarray(want[0], np.int64))
+        if name == "repeats":
+            assert (2 * nnz < ops).all()
+        else:
+            assert (2 * nnz >= ops).all()
+        assert_same(oneshot(A, B), want, name)
+        assert_same(oneshot(A, B, device=False), want, name + " host")
+
+
 def test_rmat_matches_oracle(gpu_lib):
     R = gen.rmat(scale=13, edge_factor=8, seed=5)
     assert_same(oneshot(R, R), oracle_full(R, R), "rmat s13")
