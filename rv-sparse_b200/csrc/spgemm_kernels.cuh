@@ -841,8 +841,11 @@ __global__ void __launch_bounds__(WARPS * 32)
             for (int x = lane; x < n; x += 32) keys[x] = c_ci[o + x];
         } else {
             bool wide = false;  // columns span 2^20 or more: the two-walk path
-            if (MODE == FILL && !pm && !learned && ops[row] <= CAP &&
-                2 * (int64_t)(c_rp[row + 1] - c_rp[row]) >= ops[row]) {
+            // the row's length: counted (exact) or its predicted slots (learned)
+            const int64_t room = MODE != FILL ? 0
+                                 : learned   ? ctl.slot_off[row + 1] - ctl.slot_off[row]
+                                             : (int64_t)(c_rp[row + 1] - c_rp[row]);
+            if (MODE == FILL && !pm && ops[row] <= CAP && 2 * room >= ops[row]) {
                 // Every product fits the table and at most every other one
                 // repeats a column: expand, sort, compress. Each product's
                 // column and value go to its row-local index; a stable sort
@@ -876,8 +879,22 @@ __global__ void __launch_bounds__(WARPS * 32)
                     __syncwarp();
                     const int passes = range < (1u << 8) ? 1 : range < (1u << 16) ? 2 : 3;
                     if (P > 1) warp_radix_sort_core(keys, sorttmp, P, 0u, 12, passes, hist);
-                    o = c_rp[row];
-                    const int nexp = c_rp[row + 1] - (int)o;
+                    int nexp = (int)room;
+                    if (learned) {
+                        // the distinct columns must fit the predicted slots
+                        int heads = 0;
+                        for (int x = lane; x < P; x += 32)
+                            heads += x == 0 || ((uint32_t)keys[x - 1] >> 12) != ((uint32_t)keys[x] >> 12);
+                        heads = __reduce_add_sync(FULL, heads);
+                        if (heads > room) {
+                            if (lane == 0) cnt[row] = -1;
+                            __syncwarp();
+                            continue;
+                        }
+                        nexp = heads;
+                        if (lane == 0) cnt[row] = heads;
+                    }
+                    o = learned ? ctl.slot_off[row] : (int64_t)c_rp[row];
                     int out = 0;
                     for (int b0 = 0; b0 < P; b0 += 32) {
                         const int x = b0 + lane;
