@@ -621,8 +621,10 @@ __global__ void __launch_bounds__(TRM_WARPS * 32)
 template <int CAP, int MODE>
 __host__ __device__ constexpr int warp_smem_bytes() {
     // COUNT: keys; REUSE: keys + values; FILL: keys + values + radix
-    // histogram + the radix sort's ping-pong buffer
-    return (MODE == COUNT ? 4 : MODE == REUSE ? 8 : 12) * CAP + (MODE == FILL ? 4 * 256 : 0);
+    // histogram (9-bit digits from 1024 slots up, where the extra 1 KB does
+    // not cost a CTA per SM) + the radix sort's ping-pong buffer
+    return (MODE == COUNT ? 4 : MODE == REUSE ? 8 : 12) * CAP +
+           (MODE == FILL ? 4 * (CAP >= 1024 ? 512 : 256) : 0);
 }
 
 // Lane's product p of the current 32-entry A chunk: its B position and the
@@ -723,31 +725,33 @@ __device__ __forceinline__ void walk_products(const CsrView& A, const CsrView& B
 }
 
 // One warp's stable LSD radix sort of the 32-bit words keys[0, n) by the
-// 8-bit digits of (word - sub) >> base_shift, `passes` of them, with tmp[0, n)
-// as the ping-pong buffer and hist 256 ints. Ranks within a digit follow lane
+// DB-bit digits of (word - sub) >> base_shift, `passes` of them, with tmp[0, n)
+// as the ping-pong buffer and hist 2^DB ints. Ranks within a digit follow lane
 // order chunk by chunk, so each pass is stable. Result in keys.
+template <int DB>
 __device__ void warp_radix_sort_core(int32_t* keys, int32_t* tmp, int n, uint32_t sub,
                                      int base_shift, int passes, int32_t* hist) {
+    constexpr int NB = 1 << DB, PER = NB / 32;
     const int lane = lane_id();
     int32_t* src = keys;
     int32_t* dst = tmp;
     for (int pass = 0; pass < passes; ++pass) {
-        const int shift = base_shift + 8 * pass;
-        for (int i = lane; i < 256; i += 32) hist[i] = 0;
+        const int shift = base_shift + DB * pass;
+        for (int i = lane; i < NB; i += 32) hist[i] = 0;
         __syncwarp();
         for (int i = lane; i < n; i += 32)
-            atomicAdd(&hist[(((uint32_t)src[i] - sub) >> shift) & 255], 1);
+            atomicAdd(&hist[(((uint32_t)src[i] - sub) >> shift) & (NB - 1)], 1);
         __syncwarp();
-        int v[8], s = 0;
+        int v[PER], s = 0;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            v[j] = hist[lane * 8 + j];
+        for (int j = 0; j < PER; ++j) {
+            v[j] = hist[lane * PER + j];
             s += v[j];
         }
         int run = warp_incl_scan(s) - s;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            hist[lane * 8 + j] = run;
+        for (int j = 0; j < PER; ++j) {
+            hist[lane * PER + j] = run;
             run += v[j];
         }
         __syncwarp();
@@ -755,7 +759,7 @@ __device__ void warp_radix_sort_core(int32_t* keys, int32_t* tmp, int n, uint32_
             const int i = base + lane;
             const bool ok = i < n;
             const int32_t k = ok ? src[i] : 0;
-            const int d = ok ? (int)((((uint32_t)k - sub) >> shift) & 255) : 256 + lane;
+            const int d = ok ? (int)((((uint32_t)k - sub) >> shift) & (NB - 1)) : NB + lane;
             const unsigned peers = __match_any_sync(FULL, d);
             const int leader = __ffs(peers) - 1;
             int start = 0;
@@ -777,6 +781,21 @@ __device__ void warp_radix_sort_core(int32_t* keys, int32_t* tmp, int n, uint32_
     }
 }
 
+// Packed (column - min) << 12 | index words of one row, columns spanning
+// range < 2^20: 8-bit digits, except that with a 512-entry histogram (H9) a
+// span of 2^16..2^18 takes two 9-bit passes instead of three 8-bit ones
+// (and no copy back from the ping-pong buffer).
+template <bool H9>
+__device__ __forceinline__ void sort_packed_columns(int32_t* keys, int32_t* tmp, int n,
+                                                    uint32_t range, int32_t* hist) {
+    if (n <= 1) return;
+    if (H9 && range >= (1u << 16) && range < (1u << 18))
+        warp_radix_sort_core<9>(keys, tmp, n, 0u, 12, 2, hist);
+    else
+        warp_radix_sort_core<8>(keys, tmp, n, 0u, 12, range < (1u << 8) ? 1 : range < (1u << 16) ? 2 : 3,
+                                hist);
+}
+
 // Keys[0, n) ascending: digits of key - min, as many passes as the key range
 // needs.
 __device__ void warp_radix_sort(int32_t* keys, int32_t* tmp, int n, int32_t* hist) {
@@ -791,7 +810,7 @@ __device__ void warp_radix_sort(int32_t* keys, int32_t* tmp, int n, int32_t* his
     mx = __reduce_max_sync(FULL, mx);
     const uint32_t range = (uint32_t)mx - (uint32_t)mn;
     const int passes = range < (1u << 8) ? 1 : range < (1u << 16) ? 2 : range < (1u << 24) ? 3 : 4;
-    warp_radix_sort_core(keys, tmp, n, (uint32_t)mn, 0, passes, hist);
+    warp_radix_sort_core<8>(keys, tmp, n, (uint32_t)mn, 0, passes, hist);
 }
 
 // Medium rows: one warp per row, a CAP-slot shared-memory table per warp.
@@ -817,7 +836,8 @@ __global__ void __launch_bounds__(WARPS * 32)
     int32_t* keys = reinterpret_cast<int32_t*>(mine);
     float* vals = reinterpret_cast<float*>(keys + CAP);
     int32_t* hist = reinterpret_cast<int32_t*>(mine + 8 * CAP);
-    int32_t* sorttmp = reinterpret_cast<int32_t*>(mine + 8 * CAP + 4 * 256);  // FILL only
+    constexpr bool HIST9 = CAP >= 1024;  // histogram of 512 entries: 9-bit digits
+    int32_t* sorttmp = reinterpret_cast<int32_t*>(mine + 8 * CAP + 4 * (HIST9 ? 512 : 256));  // FILL only
     volatile int32_t* vkeys = keys;
     // learned: a table that fills up means the row outgrew its predicted
     // capacity; the row is flagged for the exact path instead of an error
@@ -877,8 +897,7 @@ __global__ void __launch_bounds__(WARPS * 32)
                     for (int x = lane; x < P; x += 32)
                         keys[x] = (int32_t)((((uint32_t)keys[x] - (uint32_t)mn) << 12) | (uint32_t)x);
                     __syncwarp();
-                    const int passes = range < (1u << 8) ? 1 : range < (1u << 16) ? 2 : 3;
-                    if (P > 1) warp_radix_sort_core(keys, sorttmp, P, 0u, 12, passes, hist);
+                    sort_packed_columns<HIST9>(keys, sorttmp, P, range, hist);
                     int nexp = (int)room;
                     if (learned) {
                         // the distinct columns must fit the predicted slots
@@ -1000,9 +1019,7 @@ __global__ void __launch_bounds__(WARPS * 32)
                     for (int x = lane; x < n; x += 32)
                         keys[x] = (int32_t)((((uint32_t)keys[x] - (uint32_t)mn) << 12) | (uint32_t)x);
                     __syncwarp();
-                    const int passes = range < (1u << 8) ? 1 : range < (1u << 16) ? 2 : 3;
-                    if (n > 1)
-                        warp_radix_sort_core(keys, sorttmp, n, 0u, 12, passes, hist);
+                    sort_packed_columns<HIST9>(keys, sorttmp, n, range, hist);
                     o = learned ? ctl.slot_off[row] : (int64_t)c_rp[row];
                     for (int x = lane; x < n; x += 32) {
                         const uint32_t w = (uint32_t)keys[x];
