@@ -4,9 +4,12 @@ Output rows of C = A * B are independent, so nothing in the product needs a
 collective: a product larger than one GPU is split into row panels
 (contiguous row ranges, each holding at most 2^31 - 1 intermediate products
 so its nnz fits an int32 row pointer), and the panels are dealt to the ranks
-in contiguous groups of about equal products. B is read whole by every rank.
-The only collectives are the timing ones: a barrier around the timed region,
-the maximum of the per-rank times and the sum of the per-rank output sizes.
+in contiguous groups of about equal products. B is read whole by every rank:
+each rank loads it, or one rank broadcasts it (broadcast_operand). The only
+other collectives are the timing ones (a barrier around the timed region, the
+maximum of the per-rank times, the sum of the per-rank output sizes) and, to
+place each rank's C rows in one global C, an exclusive scan of the per-rank
+nnz built from one gathered int64 per rank (c_offsets).
 """
 
 from __future__ import annotations
@@ -85,3 +88,29 @@ def sum_over_ranks(dist, value: int) -> int:
 def barrier(dist) -> None:
     if dist is not None:
         dist.barrier()
+
+
+def broadcast_operand(dist, t, src: int = 0):
+    """Replicates rank src's tensor t (one of B's arrays) on every rank, in
+    place: an NCCL broadcast over NVLink between GPUs (t on the device), a
+    gloo broadcast on CPU. Returns t."""
+    if dist is not None:
+        dist.broadcast(t, src=src)
+    return t
+
+
+def c_offsets(dist, local_nnz: int, device: str = "cpu"):
+    """(first, total): where this rank's C entries start in the global C (the
+    exclusive scan of the ranks' nnz, in rank order, which is row order since
+    ranks own contiguous panel groups) and the global nnz. One int64 per rank
+    is gathered; device is where the gathered tensors live (the GPU under
+    NCCL)."""
+    if dist is None:
+        return 0, int(local_nnz)
+    import torch
+    t = torch.tensor([int(local_nnz)], dtype=torch.int64, device=device)
+    parts = [torch.zeros(1, dtype=torch.int64, device=device) for _ in range(dist.get_world_size())]
+    dist.all_gather(parts, t)
+    sizes = [int(p[0]) for p in parts]
+    return sum(sizes[:dist.get_rank()]), sum(sizes)
+

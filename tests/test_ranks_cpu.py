@@ -1,10 +1,12 @@
 """Multi-rank host logic on CPU: two gloo ranks on 127.0.0.1.
 
 Over several GPUs a product is split into row panels and each rank computes
-its own contiguous group of panels (rvsp_b200.ranks); the only collectives are
-the timing barrier, the max of the per-rank times and the sum of the per-rank
-nnz. Here each rank computes its panels with the oracle instead of a GPU, and
-rank 0 checks that the gathered panels are exactly the whole product.
+its own contiguous group of panels (rvsp_b200.ranks). B is broadcast from rank
+0; the collectives are that broadcast, the timing barrier, the max of the
+per-rank times, the sum of the per-rank nnz and the gather of one int64 a rank
+that places each rank's C in the global C. Here each rank computes its panels
+with the oracle instead of a GPU, and rank 0 checks that the gathered panels,
+put at their global offsets, are exactly the whole product.
 """
 
 import os
@@ -41,6 +43,13 @@ def _worker(rank, port):
         assert ranks.max_over_ranks(dist, rank + 1.5) == WORLD + 0.5
         assert ranks.sum_over_ranks(dist, rank + 1) == WORLD * (WORLD + 1) // 2
         A, B = _product()
+        # B's arrays from rank 0: the other ranks start from zeros
+        import torch
+        b_arrays = [torch.from_numpy(np.ascontiguousarray(a)) for a in (B.row_ptr, B.col_idx, B.values)]
+        got = [a.clone() if rank == 0 else torch.zeros_like(a) for a in b_arrays]
+        for t in got:
+            ranks.broadcast_operand(dist, t, src=0)
+        assert all(torch.equal(g, a) for g, a in zip(got, b_arrays))
         ops = gen.row_products(A, B)
         panels = ranks.row_panels(ops, limit=max(1, int(ops.sum()) // 7))
         mine = ranks.shard_panels(panels, ops, rank, WORLD)
@@ -48,16 +57,23 @@ def _worker(rank, port):
         for r0, r1 in mine:
             rp, ci, v = oracle.spgemm_f32(A, B, r0, r1)
             parts.append((r0, r1, rp, ci, v))
-        nnz = ranks.sum_over_ranks(dist, sum(int(p[2][-1]) for p in parts))
+        local = sum(int(p[2][-1]) for p in parts)
+        nnz = ranks.sum_over_ranks(dist, local)
+        first, total = ranks.c_offsets(dist, local)
+        assert total == nnz
         gathered = [None] * WORLD
         import torch.distributed as td
-        td.all_gather_object(gathered, parts)
+        td.all_gather_object(gathered, (first, parts))
         ranks.barrier(dist)
         if rank == 0:
-            allp = sorted((p for g in gathered for p in g), key=lambda p: p[0])
+            allp = sorted((p for g in gathered for p in g[1]), key=lambda p: p[0])
             assert [(p[0], p[1]) for p in allp] == panels  # every panel exactly once
             w_rp, w_ci, w_v = oracle.spgemm_f32(A, B)
             assert nnz == w_ci.size
+            # each rank's C entries start at its exclusive-scan offset
+            for first_r, parts_r in gathered:
+                if parts_r:
+                    assert first_r == int(w_rp[parts_r[0][0]])
             ci = np.concatenate([p[3] for p in allp])
             v = np.concatenate([p[4] for p in allp])
             rp, off = [np.zeros(1, np.int64)], 0
