@@ -506,7 +506,7 @@ def run_rmat(args, rv, gen, torch):
         for name, algo in (("tuned_exact", rv.RVSP_CUDA_ALGO_EXACT),
                            ("tuned_learned", rv.RVSP_CUDA_ALGO_LEARNED)):
             times[name] = timed(algo)
-        # misprediction rate of the learned sizing, judged by the exact recount
+        # misprediction rate of the learned sizing, measured against the exact recount
         lp = rv.Plan(rv.RVSP_CUDA_ALGO_LEARNED)
         st, lnnz = lp.symbolic(views[heavy], dA)
         rv.check(st, "learned symbolic")
