@@ -163,8 +163,8 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
 
 // Copy finished rows from their slots into C: one warp per 32 consecutive
 // list entries; the lanes load the 32 rows' counts and offsets together, then
-// copy the rows one after the other, 32 entries per step (coalesced on both
-// sides).
+// copy the rows one after the other, 128 entries per step (coalesced on both
+// sides; each lane's four loads are issued before its stores).
 __global__ void __launch_bounds__(256)
     k_compact(const int32_t* __restrict__ rows, int32_t n, const uint8_t* __restrict__ need,
               const int32_t* __restrict__ cnt, const int64_t* __restrict__ slot_off,
@@ -189,9 +189,25 @@ __global__ void __launch_bounds__(256)
         const int kj = __shfl_sync(FULL, k, j);
         const int64_t sj = __shfl_sync(FULL, src, j);
         const int dj = __shfl_sync(FULL, dst, j);
-        for (int x = lane; x < kj; x += 32) {
-            c_ci[dj + x] = tmp_ci[sj + x];
-            c_v[dj + x] = tmp_v[sj + x];
+        for (int x0 = 0; x0 < kj; x0 += 128) {
+            int32_t ci[4];
+            float v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int x = x0 + 32 * u + lane;
+                if (x < kj) {
+                    ci[u] = tmp_ci[sj + x];
+                    v[u] = tmp_v[sj + x];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int x = x0 + 32 * u + lane;
+                if (x < kj) {
+                    c_ci[dj + x] = ci[u];
+                    c_v[dj + x] = v[u];
+                }
+            }
         }
     }
 }
