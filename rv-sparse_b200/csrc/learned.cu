@@ -163,8 +163,9 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
 
 // Copy finished rows from their slots into C: one warp per 32 consecutive
 // list entries; the lanes load the 32 rows' counts and offsets together, then
-// copy the rows one after the other, 128 entries per step (coalesced on both
-// sides; each lane's four loads are issued before its stores).
+// copy either the 32 rows' entries as one list (up to 64 entries a row on
+// average) or the rows one after the other, 128 entries per step (each lane's
+// four loads issued before its stores). Coalesced on both sides.
 __global__ void __launch_bounds__(256)
     k_compact(const int32_t* __restrict__ rows, int32_t n, const uint8_t* __restrict__ need,
               const int32_t* __restrict__ cnt, const int64_t* __restrict__ slot_off,
@@ -184,6 +185,33 @@ __global__ void __launch_bounds__(256)
             src = slot_off[row];
             dst = c_rp[row];
         }
+    }
+    int incl = k;  // inclusive scan of the counts over the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
+    if (total <= 32 * 64) {
+        // short rows (tiny rows: a dozen entries): the 32 rows' entries as one
+        // list, 32 per step; each lane finds its row in the counts' scan
+        for (int e0 = 0; e0 < total; e0 += 32) {
+            const int e = e0 + lane;
+            int j = 0;
+#pragma unroll
+            for (int st = 16; st >= 1; st >>= 1)
+                if (__shfl_sync(FULL, incl, j + st - 1) <= e) j += st;
+            j = min(j, 31);
+            const int first = __shfl_sync(FULL, incl, j) - __shfl_sync(FULL, k, j);
+            const int64_t sj = __shfl_sync(FULL, src, j);
+            const int dj = __shfl_sync(FULL, dst, j);
+            if (e < total) {
+                c_ci[dj + (e - first)] = tmp_ci[sj + (e - first)];
+                c_v[dj + (e - first)] = tmp_v[sj + (e - first)];
+            }
+        }
+        return;
     }
     for (int j = 0; j < 32; ++j) {
         const int kj = __shfl_sync(FULL, k, j);
