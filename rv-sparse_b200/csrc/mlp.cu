@@ -151,6 +151,12 @@ __global__ void __launch_bounds__(256)
                 const uint8_t* __restrict__ bin, int32_t n, float* __restrict__ mu_out,
                 float* __restrict__ sig_out, int32_t* __restrict__ cap_out) {
     __shared__ float sP[MLP_NPARAM];
+    // a block none of whose rows needs a prediction (all tiny or empty, as in
+    // stencil products) leaves before loading the parameters
+    bool any = bin == nullptr;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n && !any; r += gridDim.x * blockDim.x)
+        any = bin[r] >= BIN_WARP0;
+    if (!__syncthreads_or(any)) return;
     for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) sP[i] = model.params[i];
     __syncthreads();
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
