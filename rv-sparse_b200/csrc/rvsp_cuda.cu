@@ -266,7 +266,9 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
             const int64_t fill = (int64_t)g_sms * g_heavy_ctas[MODE][cl];
             const int grid = (int)std::min<int64_t>((plan->n_items + W - 1) / W, fill);
             const HeavyAux aux{plan->bmeta.as<int4>(), plan->bdoff.as<int64_t>(),
-                               plan->dir_ok ? plan->bdir.as<int32_t>() : nullptr};
+                               plan->dir_ok ? plan->bdir.as<int32_t>() : nullptr,
+                               plan->ameta_ok ? plan->ameta.as<int4>() : nullptr,
+                               plan->ameta_ok ? plan->adoff.as<int32_t>() : nullptr};
             int32_t* queue = &plan->misc.as<Misc>()->heavy_queue;
             cudaMemsetAsync(queue, 0, sizeof(int32_t), plan->stream);
             k_heavy<MODE><<<grid, W * 32, W * heavy_smem_bytes(MODE, 1 << cl), plan->stream>>>(
@@ -418,15 +420,16 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     launch_bin_scatter(plan, plan->bin.as<uint8_t>(), plan->tile_off.as<int32_t>(),
                        plan->bin_rows.as<int32_t>(), true);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "analysis launch");
-    if (plan->n_items > 0 && (st = build_heavy_aux(plan, B))) return st;
+    if (plan->n_items > 0 && (st = build_heavy_aux(plan, A, B))) return st;
     return RVSP_SUCCESS;
 }
 
 // Per-B-row lookups of the heavy kernel (HeavyAux): metadata of every B row,
 // and the chunk directory of long rows spanning several chunks, unless the
-// directory would pass 2^28 entries (the kernel then binary-searches). One
-// device->host read of the directory size.
-int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& B) {
+// directory would pass 2^28 entries (the kernel then binary-searches); then
+// both copied beside the heavy rows' A entries when that fits in a quarter
+// of the free memory. One device->host read of the directory size.
+int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
     const int64_t K = plan->b_rows;
     const int cl = plan->params.heavy_cw_log2;
     cudaError_t e;
@@ -454,6 +457,21 @@ int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& B) {
         k_bdir<<<(unsigned)((K * 32 + 255) / 256), 256, 0, plan->stream>>>(
             B, cl, plan->bmeta.as<int4>(), plan->bdcount.as<int32_t>(),
             plan->bdscan.as<int64_t>(), plan->bdoff.as<int64_t>(), plan->bdir.as<int32_t>());
+        note_launch(plan, 1);
+    }
+    const int32_t nh = plan->bin_count[BIN_HEAVY];
+    const size_t abytes = 20 * (size_t)plan->a_nnz;
+    size_t free_b = 0, total_b = 0;
+    plan->ameta_ok = nh > 0 && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+                     abytes <= free_b / 4 &&
+                     plan->ameta.ensure(16 * (size_t)plan->a_nnz) == cudaSuccess &&
+                     plan->adoff.ensure(4 * (size_t)plan->a_nnz) == cudaSuccess;
+    cudaGetLastError();  // without the copies the walk looks up through A.ci
+    if (plan->ameta_ok) {
+        k_ameta<<<(unsigned)(((int64_t)nh * 32 + 255) / 256), 256, 0, plan->stream>>>(
+            A, B, plan->bin_rows.as<int32_t>() + plan->offs.off[BIN_HEAVY], nh,
+            plan->bmeta.as<int4>(), plan->dir_ok ? plan->bdoff.as<int64_t>() : nullptr,
+            plan->ameta.as<int4>(), plan->adoff.as<int32_t>(), &misc->err);
         note_launch(plan, 1);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "heavy lookups launch");
@@ -649,7 +667,7 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
                       &p->tile_hist, &p->tile_off, &p->pm8, &p->pm16, &p->list_ops,
                       &p->list_off, &p->lbin, &p->lcap, &p->ltile_hist, &p->ltile_off,
                       &p->lbin_rows, &p->need, &p->pflag, &p->bmeta, &p->bdcount,
-                      &p->bdscan, &p->bdoff, &p->bdir};
+                      &p->bdscan, &p->bdoff, &p->bdir, &p->ameta, &p->adoff};
     for (DevBuf* b : bufs) b->release();
     if (p->side) {
         cudaStreamSynchronize(p->side);

@@ -114,6 +114,8 @@ struct rvsp_cuda_plan {
     // per-B-row lookups of the heavy kernel (HeavyAux), built by the analysis
     // when the product has chunked rows; dir_ok when the directory exists
     rvsp::DevBuf bmeta, bdcount, bdscan, bdoff, bdir;
+    rvsp::DevBuf ameta, adoff;  // per A entry of heavy rows (HeavyAux)
+    bool ameta_ok = false;
     bool dir_ok = false;
     int32_t bin_count[rvsp::NUM_BINS] = {};
     rvsp::BinOffsets offs = {};
@@ -167,7 +169,7 @@ int scan_counts(rvsp_cuda_plan* plan, const int32_t* in, int64_t n, int64_t* out
                 int32_t* out32, int64_t* total_dev);
 void note_launch(rvsp_cuda_plan* plan, int n);
 void reset_graph(rvsp_cuda_plan* plan);
-int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& B);
+int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B);
 void launch_bin_scatter(rvsp_cuda_plan* plan, const uint8_t* bin, const int32_t* tile_off,
                         int32_t* bin_rows, bool heavy_items);
 int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool fused);

@@ -1255,6 +1255,35 @@ __global__ void k_bdir(CsrView B, int cw_log2, const int4* __restrict__ meta,
     }
 }
 
+// Heavy rows' A entries with their B row's metadata and directory offset
+// copied beside them (HeavyAux::ameta / adoff): the heavy walk then reads one
+// coalesced word pair per entry instead of a column index followed by two
+// gathers. One warp per heavy row; a column out of range flags
+// ERR_STRUCTURE and records an empty row.
+__global__ void k_ameta(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
+                        const int4* __restrict__ meta, const int64_t* __restrict__ doff,
+                        int4* __restrict__ ameta, int32_t* __restrict__ adoff,
+                        int32_t* __restrict__ err) {
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = lane_id();
+    if (w >= nrows) return;
+    int a0, a1;
+    row_range(A, rows[w], &a0, &a1, err);
+    for (int j = a0 + lane; j < a1; j += 32) {
+        const int k = A.ci[j];
+        int4 m = make_int4(0, 0, 0, -1);
+        int d = -1;
+        if ((unsigned)k < (unsigned)B.rows) {
+            m = meta[k];
+            if (doff) d = (int)doff[k];
+        } else {
+            atomicOr(err, ERR_STRUCTURE);
+        }
+        ameta[j] = m;
+        adoff[j] = d;
+    }
+}
+
 constexpr int HEAVY_MAX_WARPS = 32;
 
 template <int MODE>
@@ -1306,30 +1335,38 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
             int s = 0, len = 0;
             float av = 0.0f;
             if (j < a1) {
-                const int k = A.ci[j];
-                if ((unsigned)k >= (unsigned)B.rows) {
-                    atomicOr(err, ERR_STRUCTURE);
+                // {start, end, first column, last column} of B row A.ci[j],
+                // and its directory offset
+                int4 m = make_int4(0, 0, 0, -1);
+                int64_t d = -1;
+                if (aux.ameta) {
+                    m = aux.ameta[j];
+                    if (aux.dir) d = aux.adoff[j];
                 } else {
-                    // {start, end, first column, last column} of B row k
-                    const int4 m = aux.meta[k];
-                    const int64_t d = aux.dir ? aux.doff[k] : -1;
-                    if (m.y > m.x && m.w >= lo && m.z < hi) {
-                        int t;
-                        if (d >= 0) {
-                            const int c = it.chunk - (m.z >> cw_log2);
-                            s = m.z >= lo ? m.x : aux.dir[d + c];
-                            t = m.w < hi ? m.y : aux.dir[d + c + 1];
-                            // only an unsorted row (a broken operand) leaves a
-                            // directory entry unwritten: stay inside the row
-                            s = min(max(s, m.x), m.y);
-                            t = min(max(t, s), m.y);
-                        } else {
-                            s = m.z >= lo ? m.x : seq_lower_bound(B.ci, m.x, m.y, lo);
-                            t = m.w < hi ? m.y : seq_lower_bound(B.ci, s, m.y, hi);
-                        }
-                        len = t - s;
-                        if (MODE != COUNT) av = A.v[j];
+                    const int k = A.ci[j];
+                    if ((unsigned)k >= (unsigned)B.rows) {
+                        atomicOr(err, ERR_STRUCTURE);
+                    } else {
+                        m = aux.meta[k];
+                        if (aux.dir) d = aux.doff[k];
                     }
+                }
+                if (m.y > m.x && m.w >= lo && m.z < hi) {
+                    int t;
+                    if (d >= 0) {
+                        const int c = it.chunk - (m.z >> cw_log2);
+                        s = m.z >= lo ? m.x : aux.dir[d + c];
+                        t = m.w < hi ? m.y : aux.dir[d + c + 1];
+                        // only an unsorted row (a broken operand) leaves a
+                        // directory entry unwritten: stay inside the row
+                        s = min(max(s, m.x), m.y);
+                        t = min(max(t, s), m.y);
+                    } else {
+                        s = m.z >= lo ? m.x : seq_lower_bound(B.ci, m.x, m.y, lo);
+                        t = m.w < hi ? m.y : seq_lower_bound(B.ci, s, m.y, hi);
+                    }
+                    len = t - s;
+                    if (MODE != COUNT) av = A.v[j];
                 }
             }
             const int incl = warp_incl_scan(len);

@@ -87,6 +87,10 @@ struct HeavyAux {
     const int4* meta;
     const int64_t* doff;
     const int32_t* dir;
+    // the same per A entry of the heavy rows (ameta[j] = meta[A.ci[j]], adoff
+    // likewise, -1: no directory), or null: looked up through A.ci
+    const int4* ameta;
+    const int32_t* adoff;
 };
 constexpr int DIR_MIN_LEN = 32;
 
