@@ -679,6 +679,7 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
         cudaStreamDestroy(p->side);
     }
     if (p->side_fork) cudaEventDestroy(p->side_fork);
+    if (p->host_pin) cudaFreeHost(p->host_pin);
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;
 }

@@ -96,6 +96,7 @@ struct rvsp_cuda_plan {
     // the operands' host->device copies (created on first use)
     cudaStream_t side = nullptr;
     cudaEvent_t side_fork = nullptr;
+    int32_t* host_pin = nullptr;  // pinned words for small device->host reads
     bool analysed = false;
     bool capturing = false;
     int32_t a_rows = 0, a_cols = 0, a_nnz = 0, b_rows = 0, b_cols = 0, b_nnz = 0;

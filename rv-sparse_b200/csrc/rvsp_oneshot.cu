@@ -60,12 +60,32 @@ void keep_pool_memory() {
 
 namespace {
 
-int read_i32(const int32_t* p, int32_t* out) {
-    if (is_dev(p)) {
-        cudaError_t e = cudaMemcpy(out, p, 4, cudaMemcpyDeviceToHost);
-        return e == cudaSuccess ? RVSP_SUCCESS : fail(e, "row_ptr read");
+// The last entries of A's and B's row pointers (their nnz), wherever they
+// live: device values come back together, one host round trip for both,
+// through the plan's pinned word pair.
+int read_ends(rvsp_cuda_plan* plan, const int32_t* pa, const int32_t* pb, int32_t* a,
+              int32_t* b) {
+    const bool da = is_dev(pa), db = is_dev(pb);
+    if (!da) *a = *pa;
+    if (!db) *b = *pb;
+    if (!da && !db) return RVSP_SUCCESS;
+    cudaError_t e = cudaSuccess;
+    if (!plan->host_pin && (e = cudaMallocHost((void**)&plan->host_pin, 16)) != cudaSuccess) {
+        plan->host_pin = nullptr;
+        cudaGetLastError();
+        if (da && (e = cudaMemcpy(a, pa, 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
+            return fail(e, "row_ptr read");
+        if (db && (e = cudaMemcpy(b, pb, 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
+            return fail(e, "row_ptr read");
+        return RVSP_SUCCESS;
     }
-    *out = *p;
+    if (da) e = cudaMemcpyAsync(plan->host_pin, pa, 4, cudaMemcpyDeviceToHost, plan->stream);
+    if (e == cudaSuccess && db)
+        e = cudaMemcpyAsync(plan->host_pin + 1, pb, 4, cudaMemcpyDeviceToHost, plan->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(plan->stream);
+    if (e != cudaSuccess) return fail(e, "row_ptr read");
+    if (da) *a = plan->host_pin[0];
+    if (db) *b = plan->host_pin[1];
     return RVSP_SUCCESS;
 }
 
@@ -89,14 +109,13 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
     *c_v_out = nullptr;
     *c_nnz_out = 0;
     int st;
-    int32_t a_nnz = 0, b_nnz = 0;
-    if ((st = read_i32(a_rp + a_rows, &a_nnz))) return st;
-    if ((st = read_i32(b_rp + a_cols, &b_nnz))) return st;
     rvsp_cuda_plan_t& plan = t_plan[algo == RVSP_CUDA_ALGO_LEARNED ? 1 : 0];
     if (!plan) {
         if ((st = rvsp_cuda_plan_create(&plan, algo))) return st;
         plan->map_policy = 0;  // a one-shot product is never reused
     }
+    int32_t a_nnz = 0, b_nnz = 0;
+    if ((st = read_ends(plan, a_rp + a_rows, b_rp + a_cols, &a_nnz, &b_nnz))) return st;
     plan->params = default_params();
     const bool dev = is_dev(a_rp);
     keep_pool_memory();
