@@ -244,7 +244,7 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
             if (MODE == REUSE && o.maps)
                 k_tiny_reuse_map<<<(n + 32 * TRM_WARPS - 1) / (32 * TRM_WARPS), 32 * TRM_WARPS, 0,
                                    plan->stream>>>(A, B, r, n, o.c_rp, o.c_v, lo,
-                                                   plan->pm8.as<uint8_t>(), o.err);
+                                                   plan->pm8.as<uint8_t>(), o.rp_out, o.err);
             else
                 k_tiny<MODE><<<grid, TINY_TPB, 0, plan->stream>>>(
                     A, B, r, n, o.cnt, o.c_rp, o.c_ci, o.c_v, o.maps ? lo : nullptr,
@@ -578,8 +578,8 @@ void reset_graph(rvsp_cuda_plan* plan) {
 // Numeric-only pass on a known pattern, replayed from a CUDA graph keyed on
 // the device pointers it reads and writes.
 int reuse_numeric(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, const int32_t* c_ci,
-                  float* c_v) {
-    const void* key[8] = {A.rp, A.ci, A.v, B.rp, B.ci, B.v, c_ci, c_v};
+                  float* c_v, int32_t* rp_out) {
+    const void* key[9] = {A.rp, A.ci, A.v, B.rp, B.ci, B.v, c_ci, c_v, rp_out};
     cudaError_t e;
     if (!(plan->gexec && memcmp(key, plan->gkey, sizeof(key)) == 0)) {
         reset_graph(plan);
@@ -590,6 +590,7 @@ int reuse_numeric(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, cons
         plan->capturing = true;
         RowOut o{nullptr, plan->c_rp.as<int32_t>(), const_cast<int32_t*>(c_ci), c_v,
                  &plan->misc.as<Misc>()->err, plan->maps_ready};
+        o.rp_out = rp_out;
         run_rows(plan, REUSE, A, B, o);
         plan->capturing = false;
         e = cudaStreamEndCapture(plan->stream, &g);
@@ -829,17 +830,23 @@ int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t*
     // beside the operands' host->device copies (PCIe carries both directions
     // at once); every return waits for it.
     SideCopy side_rp;
-    if (!dev_rp && side_stream(plan)) {
-        if ((e = cudaEventRecord(plan->side_fork, plan->stream)) != cudaSuccess ||
-            (e = cudaStreamWaitEvent(plan->side, plan->side_fork, 0)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(c_rp, plan->c_rp.p, (M + 1) * 4, cudaMemcpyDeviceToHost,
-                                 plan->side)) != cudaSuccess)
+    // Value-only reuse of a product whose rows are all tiny: the map-replay
+    // kernel writes the row pointer beside the values, no separate copy.
+    const bool rp_fused = dev_rp && !fill_structure && nnz > 0 && plan->maps_ready &&
+                          plan->bin_count[BIN_TINY] == M;
+    if (!rp_fused) {
+        if (!dev_rp && side_stream(plan)) {
+            if ((e = cudaEventRecord(plan->side_fork, plan->stream)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(plan->side, plan->side_fork, 0)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(c_rp, plan->c_rp.p, (M + 1) * 4, cudaMemcpyDeviceToHost,
+                                     plan->side)) != cudaSuccess)
+                return fail(e, "row_ptr copy");
+            side_rp.s = plan->side;
+        } else if ((e = cudaMemcpyAsync(c_rp, plan->c_rp.p, (M + 1) * 4,
+                                        dev_rp ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                        plan->stream)) != cudaSuccess) {
             return fail(e, "row_ptr copy");
-        side_rp.s = plan->side;
-    } else if ((e = cudaMemcpyAsync(c_rp, plan->c_rp.p, (M + 1) * 4,
-                                    dev_rp ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                                    plan->stream)) != cudaSuccess) {
-        return fail(e, "row_ptr copy");
+        }
     }
     CsrView A, B;
     int st = stage_operands(plan, a_rp, a_ci, a_v, b_rp, b_ci, b_v, true, &A, &B);
@@ -898,7 +905,7 @@ int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t*
                     return fail(e, "col_idx upload");
                 plan->filled_host = c_ci;
             }
-            if ((st = reuse_numeric(plan, A, B, d_ci, d_v))) return st;
+            if ((st = reuse_numeric(plan, A, B, d_ci, d_v, rp_fused ? c_rp : nullptr))) return st;
         }
         if (!dev_v &&
             (e = cudaMemcpyAsync(c_v, d_v, (size_t)nnz * 4, cudaMemcpyDeviceToHost,

@@ -63,6 +63,9 @@ struct RowOut {
     bool maps;           // FILL: record position maps; REUSE: replay them
     RowCtl ctl = {nullptr, nullptr, 0};
     bool learned_bins = false;  // iterate the predicted-capacity bins instead
+    // REUSE, every row a tiny row: the map-replay kernel also writes the
+    // caller's row pointer (the copy of the analysed one is skipped)
+    int32_t* rp_out = nullptr;
 };
 
 extern thread_local std::string g_err;
@@ -153,7 +156,7 @@ struct rvsp_cuda_plan {
 
     // numeric-only CUDA graph
     cudaGraphExec_t gexec = nullptr;
-    const void* gkey[8] = {};
+    const void* gkey[9] = {};
     int graph_kernels = 0;
 };
 

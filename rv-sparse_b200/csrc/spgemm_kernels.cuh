@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(TRM_WARPS * 32)
     k_tiny_reuse_map(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
                      const int32_t* __restrict__ c_rp, float* __restrict__ c_v,
                      const int32_t* __restrict__ list_off, const uint8_t* __restrict__ pm,
-                     int32_t* __restrict__ err) {
+                     int32_t* __restrict__ rp_out, int32_t* __restrict__ err) {
     __shared__ float s_acc[TRM_WARPS][TRM_CCAP];
     const int w = threadIdx.x >> 5, lane = lane_id();
     const int i = (blockIdx.x * TRM_WARPS + w) * 32 + lane;
@@ -525,6 +525,10 @@ __global__ void __launch_bounds__(TRM_WARPS * 32)
         c1 = c_rp[row + 1];
         row_range(A, row, &a0, &a1, err);
         pb = list_off[i] - list_off[0];
+        if (rp_out) {  // every row of C is a tiny row: this launch writes the row pointer
+            rp_out[row] = c0;
+            if (row == A.rows - 1) rp_out[A.rows] = c1;
+        }
     }
     const int n = min(c1 - c0, TINY_CAP);
     const int last = __popc(__ballot_sync(FULL, live)) - 1;  // live lanes are a prefix

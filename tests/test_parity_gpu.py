@@ -185,13 +185,17 @@ def test_descriptor_reuse_rescaled_values(gpu_lib, device):
         scaled = (A.values * rng.uniform(0.5, 1.5, A.nnz).astype(np.float32)).astype(np.float32)
         if device:
             dv.copy_(dev(scaled))
+            crp.fill_(-1)  # every compute writes C's row pointer
         else:
             vals[:] = scaled
+            crp[:] = -1
         rv.check(d.compute(a, a, c, wsb), f"compute {rep}")
         M = Mat(A.rows, A.cols, A.row_ptr, A.col_idx, scaled)
         want = oracle.numeric_f32(M, M, wrp, wci)
         got_v = cv.cpu().numpy() if device else cv
         got_ci = cci.cpu().numpy() if device else cci
+        got_rp = crp.cpu().numpy() if device else crp
+        assert np.array_equal(got_rp.astype(np.int64), np.asarray(wrp, np.int64)), rep
         assert np.array_equal(got_ci, wci)
         assert np.array_equal(bits(got_v), bits(want)), rep
     d.close()
