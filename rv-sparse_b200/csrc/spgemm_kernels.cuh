@@ -362,6 +362,60 @@ __global__ void k_list_ops(const int32_t* __restrict__ bin_rows, int32_t n,
 // ---------------------------------------------------------------------------
 constexpr int TINY_TPB = 128;
 constexpr int TINY_LD = TINY_TPB + 1;
+constexpr int TINY_AB = 8;    // A entries whose B-row ranges are loaded together
+constexpr int TINY_VALS = 5;  // B entries loaded together
+
+// One tiny row's products in the reference order, with many loads in flight:
+// A's entries TINY_AB at a time (column indices and values, then the B-row
+// ranges, as two batches), each B row TINY_VALS entries at a time.
+// f(col, product value) runs once per product, in A-row order then B-row
+// order; VALUES loads A's and B's values too.
+template <bool VALUES, class F>
+__device__ __forceinline__ void tiny_walk(const CsrView& A, const CsrView& B, int a0, int a1,
+                                          int32_t* err, F&& f) {
+    for (int p0 = a0; p0 < a1; p0 += TINY_AB) {
+        int k[TINY_AB];
+        float a[TINY_AB];
+#pragma unroll
+        for (int u = 0; u < TINY_AB; ++u) {
+            k[u] = p0 + u < a1 ? A.ci[p0 + u] : -1;
+            a[u] = VALUES && p0 + u < a1 ? A.v[p0 + u] : 0.0f;
+        }
+        int q0[TINY_AB], q1[TINY_AB];
+#pragma unroll
+        for (int u = 0; u < TINY_AB; ++u) {
+            q0[u] = q1[u] = 0;
+            if (p0 + u < a1) {
+                if ((unsigned)k[u] < (unsigned)B.rows) {
+                    q0[u] = B.rp[k[u]];
+                    q1[u] = B.rp[k[u] + 1];
+                } else {
+                    atomicOr(err, ERR_STRUCTURE);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TINY_AB; ++u) {
+            if (q0[u] < 0 || q1[u] < q0[u] || q1[u] > B.nnz) {
+                atomicOr(err, ERR_STRUCTURE);
+                q1[u] = q0[u] = 0;
+            }
+            for (int m0 = q0[u]; m0 < q1[u]; m0 += TINY_VALS) {
+                int c[TINY_VALS];
+                float v[TINY_VALS];
+#pragma unroll
+                for (int t = 0; t < TINY_VALS; ++t) {
+                    const bool in = m0 + t < q1[u];
+                    c[t] = in ? __ldg(B.ci + m0 + t) : -1;
+                    v[t] = VALUES && in ? __ldg(B.v + m0 + t) : 0.0f;
+                }
+#pragma unroll
+                for (int t = 0; t < TINY_VALS; ++t)
+                    if (m0 + t < q1[u]) f(c[t], __fmul_rn(a[u], v[t]));
+            }
+        }
+    }
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(TINY_TPB)
@@ -391,16 +445,13 @@ __global__ void __launch_bounds__(TINY_TPB)
             // one walk: (column, product) pairs in A-row order, a stable
             // insertion sort by column, then each run of equal columns summed
             // left to right from +0.0f -- the reference's order per column
-            for (int p = a0; p < a1; ++p) {
-                const float a = A.v[p];
-                int q0, q1;
-                row_range(B, A.ci[p], &q0, &q1, err);
-                for (int q = q0; q < q1 && n < TINY_CAP; ++q) {
-                    COL(n) = B.ci[q];
-                    VAL(n) = __fmul_rn(a, B.v[q]);
+            tiny_walk<true>(A, B, a0, a1, err, [&](int col, float pv) {
+                if (n < TINY_CAP) {
+                    COL(n) = col;
+                    VAL(n) = pv;
                     ++n;
                 }
-            }
+            });
             for (int x = 1; x < n; ++x) {
                 const int key = COL(x);
                 const float v = VAL(x);
@@ -430,11 +481,9 @@ __global__ void __launch_bounds__(TINY_TPB)
                 c0 = c_rp[row];
             }
         } else {
-            for (int p = a0; p < a1; ++p) {
-                int q0, q1;
-                row_range(B, A.ci[p], &q0, &q1, err);
-                for (int q = q0; q < q1 && n < TINY_CAP; ++q) COL(n++) = B.ci[q];
-            }
+            tiny_walk<false>(A, B, a0, a1, err, [&](int col, float) {
+                if (n < TINY_CAP) COL(n++) = col;
+            });
             for (int x = 1; x < n; ++x) {  // insertion sort
                 const int key = COL(x);
                 int y = x - 1;
