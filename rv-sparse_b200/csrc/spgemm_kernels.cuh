@@ -511,19 +511,13 @@ __global__ void __launch_bounds__(TINY_TPB)
         if (MODE == REUSE || (MODE == FILL && pm)) {
             uint8_t* pp = pm ? pm + (list_off[i] - list_off[0]) : nullptr;
             for (int x = 0; x < n; ++x) VAL(x) = 0.0f;
-            for (int p = a0; p < a1; ++p) {
-                const float a = A.v[p];
-                int q0, q1;
-                row_range(B, A.ci[p], &q0, &q1, err);
-                for (int q = q0; q < q1; ++q) {
-                    const int col = B.ci[q];
-                    int pos = 0, step = 16;
-                    for (; step > 0; step >>= 1)
-                        if (pos + step <= n && COL(pos + step - 1) < col) pos += step;
-                    if (pp) *pp++ = (uint8_t)pos;
-                    if (pos < n) VAL(pos) = __fadd_rn(VAL(pos), __fmul_rn(a, B.v[q]));
-                }
-            }
+            tiny_walk<true>(A, B, a0, a1, err, [&](int col, float pv) {
+                int pos = 0, step = 16;
+                for (; step > 0; step >>= 1)
+                    if (pos + step <= n && COL(pos + step - 1) < col) pos += step;
+                if (pp) *pp++ = (uint8_t)pos;
+                if (pos < n) VAL(pos) = __fadd_rn(VAL(pos), pv);
+            });
         }
     }
     if (MODE == COUNT) return;
