@@ -18,7 +18,7 @@ tests):
   distinct uniform columns; used for the batched uneven products.
 * ``tall_skinny``     A rows with geometric(mean 8) nnz and uniform columns;
   B rows with a truncated power-law length distribution (mean about 24, the
-  longest row forced to ``b_max``), uniform distinct columns.
+  longest row drawing ``b_max`` columns), uniform columns with repeats merged.
 
 Columns that a row draws twice are merged; rows that must hold an exact count
 are topped up until they do.
