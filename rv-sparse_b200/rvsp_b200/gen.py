@@ -63,6 +63,18 @@ def from_keys(rows: int, cols: int, keys: np.ndarray, values: np.ndarray | None,
     return CSR(rows, cols, rp.astype(np.int32), c, values.astype(np.float32))
 
 
+def _sorted_unique(x: np.ndarray) -> np.ndarray:
+    """np.unique(x) by sorting (the same array; numpy's hash-based unique is
+    much slower on tens of millions of int64 keys)."""
+    x = np.sort(x)
+    if x.size > 1:
+        keep = np.empty(x.size, bool)
+        keep[0] = True
+        np.not_equal(x[1:], x[:-1], out=keep[1:])
+        x = x[keep]
+    return x
+
+
 def _distinct_rows(counts: np.ndarray, cols: int, rng: np.random.Generator,
                    exact: bool = True) -> np.ndarray:
     """Sorted unique keys row*cols+col with counts[r] distinct uniform columns per row."""
@@ -76,7 +88,7 @@ def _distinct_rows(counts: np.ndarray, cols: int, rng: np.random.Generator,
             break
         r = np.repeat(np.arange(rows, dtype=np.int64), need)
         new = r * cols + rng.integers(0, cols, size=tot, dtype=np.int64)
-        keys = np.unique(np.concatenate([keys, new]))
+        keys = _sorted_unique(np.concatenate([keys, new]))
         if not exact:
             break
         have = np.bincount(keys // cols, minlength=rows)
@@ -128,7 +140,7 @@ def rmat(scale: int = 20, edge_factor: int = 16, a: float = 0.57, b: float = 0.1
             cc |= cbit.astype(np.int64) << bit
         row[lo:hi] = rr
         col[lo:hi] = cc
-    keys = np.unique(row * n + col)
+    keys = _sorted_unique(row * n + col)
     return from_keys(n, n, keys, None, rng)
 
 
