@@ -6,11 +6,17 @@
  * the CUDA backend only:
  *
  *   - rvsp_spgemm_csr accepts RVSP_BACKEND_CUDA and RVSP_BACKEND_CUDA_LEARNED
- *     (options == NULL selects RVSP_BACKEND_CUDA); the CPU backends return
- *     RVSP_ERROR_UNSUPPORTED_BACKEND, as the reference does for vector
- *     strategies on a build without them (rv-sparse src/core/spgemm_descr.c:43-64).
- *   - the descriptor accepts RVSP_SPGEMM_ALGO_CUDA (the default a new
- *     descriptor starts with) and RVSP_SPGEMM_ALGO_CUDA_LEARNED.
+ *     (options == NULL selects RVSP_BACKEND_CUDA). The reference's scalar
+ *     backends (RVSP_BACKEND_SCALAR for FP32, FP64 and INT8 -> INT32,
+ *     RVSP_BACKEND_SCALAR_UNROLL4 for FP32; rv-sparse src/core/spgemm.c:160-193)
+ *     run on the CUDA exact path, whose results are bit-identical to theirs.
+ *     RVSP_BACKEND_RVV_INTRINSICS returns RVSP_ERROR_UNSUPPORTED_BACKEND, as
+ *     the reference does on a build without the vector extension.
+ *   - the descriptor accepts RVSP_SPGEMM_ALGO_DEFAULT (the strategy a new
+ *     descriptor starts with, rv-sparse src/core/spgemm_descr.c:83) and
+ *     RVSP_SPGEMM_ALGO_CUDA, both the CUDA exact path, and
+ *     RVSP_SPGEMM_ALGO_CUDA_LEARNED; the vector strategies return
+ *     RVSP_ERROR_UNSUPPORTED_BACKEND (rv-sparse src/core/spgemm_descr.c:43-64).
  *
  * Residency: every array of A, B and C may live in host memory or in device
  * memory of the current CUDA device; the backend detects which per pointer.

@@ -98,7 +98,8 @@ typedef struct rvsp_spgemm_descr *rvsp_spgemm_descr_t;
 
 typedef enum
 {
-    RVSP_SPGEMM_ALGO_DEFAULT = 0, /* scalar CPU kernel: not provided by this build */
+    RVSP_SPGEMM_ALGO_DEFAULT = 0, /* the reference's scalar kernel; here the CUDA exact path,
+                                     whose results are bit-identical */
     RVSP_SPGEMM_ALGO_RVV,         /* RISC-V vector: not provided by this build */
     RVSP_SPGEMM_ALGO_CONTIG,      /* RISC-V vector: not provided by this build */
     RVSP_SPGEMM_ALGO_ADAPTIVE,    /* RISC-V vector: not provided by this build */

@@ -51,11 +51,13 @@ _ref = None
 
 
 def build(ref_dir: str | None = None) -> None:
-    """Compile the restatement, and the reference library when its sources exist."""
+    """Compile the restatement; with a reference checkout (ref_dir, or
+    $RVSP_REFERENCE_DIR) also the reference library and the reference's own
+    C tests and examples (against both libraries)."""
     targets = ["oracle"]
-    ref_dir = ref_dir or os.environ.get("RVSP_REFERENCE_DIR", "/root/reference")
-    if os.path.isdir(os.path.join(ref_dir, "src", "kernels", "spgemm")):
-        targets.append("ref")
+    ref_dir = ref_dir or os.environ.get("RVSP_REFERENCE_DIR", "")
+    if ref_dir and os.path.isdir(os.path.join(ref_dir, "src", "kernels", "spgemm")):
+        targets += ["ref", "reftests"]
     subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_dir}"] + targets, check=True)
 
 

@@ -232,6 +232,13 @@ rvsp_status_t rvsp_spgemm_csr(const rvsp_csr_matrix_t *A, const rvsp_csr_matrix_
         in_dt = options->input_dtype;
         out_dt = options->output_dtype;
     }
+    /* The reference's scalar backends (spgemm.c:160-167, :181-193) run on the
+     * CUDA exact path, whose results are bit-identical to the scalar kernels'
+     * (FP32 and the FP64 / INT8 -> INT32 legacy products alike). */
+    if (backend == RVSP_BACKEND_SCALAR ||
+        (backend == RVSP_BACKEND_SCALAR_UNROLL4 && in_dt == RVSP_DTYPE_FP32 &&
+         out_dt == RVSP_DTYPE_FP32))
+        backend = RVSP_BACKEND_CUDA;
     /* the reference's other dtypes (its legacy kernels, spgemm.c:181-193) */
     if (backend == RVSP_BACKEND_CUDA &&
         ((in_dt == RVSP_DTYPE_FP64 && out_dt == RVSP_DTYPE_FP64) ||
@@ -298,9 +305,21 @@ struct rvsp_spgemm_descr
     size_t workspace_bytes;
 };
 
+/* The reference's default strategy is its scalar kernel
+ * (spgemm_descr.c:43-64, :83). The CUDA exact path computes bit-identical
+ * results (same structure, same FP32 operation order), so DEFAULT selects it:
+ * code written against the reference runs unchanged, on the GPU. The vector
+ * strategies are refused as the reference refuses them on a build without
+ * the vector extension. */
+static int plan_algo(rvsp_spgemm_algo_t algo)
+{
+    return algo == RVSP_SPGEMM_ALGO_CUDA_LEARNED ? RVSP_CUDA_ALGO_LEARNED : RVSP_CUDA_ALGO_EXACT;
+}
+
 static int algo_available(rvsp_spgemm_algo_t algo)
 {
-    if (algo != RVSP_SPGEMM_ALGO_CUDA && algo != RVSP_SPGEMM_ALGO_CUDA_LEARNED)
+    if (algo != RVSP_SPGEMM_ALGO_DEFAULT && algo != RVSP_SPGEMM_ALGO_CUDA &&
+        algo != RVSP_SPGEMM_ALGO_CUDA_LEARNED)
         return 0;
     if (rvsp_cuda_device_count() == 0)
         return 0;
@@ -316,7 +335,7 @@ rvsp_status_t rvsp_spgemm_descr_create(rvsp_spgemm_descr_t *descr)
     struct rvsp_spgemm_descr *d = (struct rvsp_spgemm_descr *)calloc(1, sizeof(*d));
     if (d == NULL)
         return RVSP_ERROR_ALLOCATION_FAILED;
-    d->algo = RVSP_SPGEMM_ALGO_CUDA;
+    d->algo = RVSP_SPGEMM_ALGO_DEFAULT; /* as the reference (spgemm_descr.c:83) */
     *descr = d;
     return RVSP_SUCCESS;
 }
@@ -381,7 +400,7 @@ rvsp_status_t rvsp_spgemm_work_estimation(rvsp_spgemm_descr_t descr, const rvsp_
     descr->c_nnz = 0;
     if (descr->plan == NULL)
     {
-        int cst = rvsp_cuda_plan_create(&descr->plan, (int)descr->algo);
+        int cst = rvsp_cuda_plan_create(&descr->plan, plan_algo(descr->algo));
         if (cst != RVSP_SUCCESS)
             return (rvsp_status_t)cst;
     }

@@ -1,9 +1,8 @@
 """Regenerates the golden fixtures in this directory from the reference.
 
-Run next to a reference checkout (default /root/reference, or
-$RVSP_REFERENCE_DIR):
+Run next to a reference checkout named by $RVSP_REFERENCE_DIR:
 
-    python tests/golden/make_golden.py
+    RVSP_REFERENCE_DIR=<checkout> python tests/golden/make_golden.py
 
 Writes:
 
@@ -34,7 +33,7 @@ sys.path.insert(0, os.path.join(ROOT, "rv-sparse_b200"))
 import oracle  # noqa: E402
 from rvsp_b200 import gen  # noqa: E402
 
-REF = os.environ.get("RVSP_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("RVSP_REFERENCE_DIR", "")
 
 DUMP_C = r"""
 #include <stdio.h>
@@ -107,6 +106,8 @@ def small_cases():
 
 
 def main():
+    if not os.path.isdir(os.path.join(REF, "tests")):
+        sys.exit("set RVSP_REFERENCE_DIR to a reference checkout")
     oracle.build(REF)
     dump_fixtures()
     arrays = {}

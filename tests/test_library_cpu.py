@@ -82,11 +82,14 @@ def test_descriptor_contract_host_side():
     h = C.c_void_p()
     assert L.rvsp_spgemm_descr_create(C.byref(h)) == 0 and h
     assert L.rvsp_spgemm_set_algo(None, rv.RVSP_SPGEMM_ALGO_CUDA) == rv.RVSP_ERROR_NULL_POINTER
-    # CPU strategies are not provided by this build, as RVV is not by a scalar build
-    for algo in (rv.RVSP_SPGEMM_ALGO_DEFAULT, rv.RVSP_SPGEMM_ALGO_RVV, rv.RVSP_SPGEMM_ALGO_CONTIG,
+    # vector strategies are not provided by this build, as the reference
+    # refuses them on a build without the vector extension
+    for algo in (rv.RVSP_SPGEMM_ALGO_RVV, rv.RVSP_SPGEMM_ALGO_CONTIG,
                  rv.RVSP_SPGEMM_ALGO_ADAPTIVE, 99):
         assert L.rvsp_spgemm_set_algo(h, algo) == rv.RVSP_ERROR_UNSUPPORTED_BACKEND
+    # the default strategy (the reference's scalar kernel) is the CUDA exact path
     expect = 0 if have_gpu() else rv.RVSP_ERROR_UNSUPPORTED_BACKEND
+    assert L.rvsp_spgemm_set_algo(h, rv.RVSP_SPGEMM_ALGO_DEFAULT) == expect
     assert L.rvsp_spgemm_set_algo(h, rv.RVSP_SPGEMM_ALGO_CUDA) == expect
     rp, ci, v, A = _host_matrix([0, 2, 3], [0, 1, 1], 2, 2)
     crp, cci, cv, Cm = _host_matrix([0, 0, 0], [], 2, 2)
@@ -115,11 +118,16 @@ def test_oneshot_backend_selection_host_side():
     L = rv.lib()
     rp, ci, v, A = _host_matrix([0, 2, 3], [0, 1, 1], 2, 2)
     out = rv.CsrMatrix()
-    for be in (rv.RVSP_BACKEND_SCALAR, rv.RVSP_BACKEND_SCALAR_UNROLL4, rv.RVSP_BACKEND_RVV_INTRINSICS):
-        opts = rv.SpgemmOptions(be, rv.RVSP_DTYPE_FP32, rv.RVSP_DTYPE_FP32)
-        assert L.rvsp_spgemm_csr(C.byref(A), C.byref(A), C.byref(out), C.byref(opts)) == -5
-    opts = rv.SpgemmOptions(rv.RVSP_BACKEND_CUDA, rv.RVSP_DTYPE_INT8, rv.RVSP_DTYPE_INT32)
+    opts = rv.SpgemmOptions(rv.RVSP_BACKEND_RVV_INTRINSICS, rv.RVSP_DTYPE_FP32, rv.RVSP_DTYPE_FP32)
     assert L.rvsp_spgemm_csr(C.byref(A), C.byref(A), C.byref(out), C.byref(opts)) == -5
+    # the unrolled scalar alias has no legacy dtypes in the reference either
+    opts = rv.SpgemmOptions(rv.RVSP_BACKEND_SCALAR_UNROLL4, rv.RVSP_DTYPE_FP64, rv.RVSP_DTYPE_FP64)
+    assert L.rvsp_spgemm_csr(C.byref(A), C.byref(A), C.byref(out), C.byref(opts)) == -5
+    if not have_gpu():
+        # the scalar backends run on the GPU, so without one they are refused
+        for be in (rv.RVSP_BACKEND_SCALAR, rv.RVSP_BACKEND_SCALAR_UNROLL4):
+            opts = rv.SpgemmOptions(be, rv.RVSP_DTYPE_FP32, rv.RVSP_DTYPE_FP32)
+            assert L.rvsp_spgemm_csr(C.byref(A), C.byref(A), C.byref(out), C.byref(opts)) == -5
     assert L.rvsp_spgemm_csr(None, C.byref(A), C.byref(out), None) == -1
     if not have_gpu():
         assert L.rvsp_spgemm_csr(C.byref(A), C.byref(A), C.byref(out), None) == -5
