@@ -2,38 +2,46 @@
 """FP32 CSR SpGEMM benchmark on B200 (one process per GPU).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload poisson_reuse|plain|batched|tall_skinny|rmat|coo]
+                    [--workload rmat|poisson_reuse|plain|batched|tall_skinny|coo|profile]
 
-Default workload (the descriptor-reuse case): C = A * A for the 5-point
-Laplacian on a 1024 x 1024 grid (N = 1,048,576, nnz(A) = 5,238,784,
-nnz(C) = 13,611,012, 26,177,544 intermediate products). The structure is
-analysed once; every step rescales A's values entry-wise by U(0.5, 1.5)
-(seeded) and re-executes the numeric phase only, replayed from a CUDA graph.
+Default workload (the power-law product the metric is quoted on): C = A * A
+for an R-MAT graph of 2^20 vertices, 16 * 2^20 edge samples with
+(a, b, c, d) = (0.57, 0.19, 0.19, 0.05), duplicates merged, values U(-1, 1),
+seed 0 (nnz(A) = 16,086,301, 2.09e10 intermediate products, nnz(C) = 9.7e9).
+Its C is too large for one int32 CSR (the reference refuses such a product,
+rvsp_symbolic.c:69), so it runs as A row panels of at most 2^31 - 1 products,
+each panel one call of the one-shot entry point on device-resident operands
+(the panel's row pointer offset into the full arrays). One step is the whole
+product, every panel; the next step starts on a flushed L2.
 
 Printed as one JSON line by rank 0:
-  value   GFLOP/s = 2 * products / step time, device-timed with CUDA events on
-          the plan's stream, operands resident in HBM, L2 flushed (256 MiB
-          write) before every step
-  e2e     the same metric through the public C API (rvsp_spgemm_compute) with
-          pinned host buffers: the H2D copy of the new values and the D2H copy
-          of C inside the timed region (wall clock)
-  roofline  algorithmic bytes of one numeric pass / its kernel time vs the
-          measured HBM copy bandwidth (MEASURED_PEAKS.json)
-  cpu_baseline  the reference's scalar numeric pass (oracle/_ref, compiled
-          from the reference sources) on 1 host core, bounded sample
-With --impl reference the reference's CPU implementation is timed instead,
-on all host cores (row panels), with the same workload, metric and unit.
+  value   learned-binned GFLOP/s = 2 * products / step time (the MLP-sized
+          path, RVSP_CUDA_ALGO_LEARNED), device-timed with CUDA events,
+          operands resident in HBM; exact_gflops beside it is the
+          exact-symbolic path (RVSP_CUDA_ALGO_EXACT) timed the same way
+  roofline  the dominant kernel's algorithmic bytes per launch over its mean
+          launch duration (per-family CUDA events inside the library, live in
+          the timed region) against the measured HBM copy bandwidth
+  e2e     the same metric through the public C API (rvsp_spgemm_csr with the
+          learned backend) on host buffers: every panel's A upload, B upload
+          and C download inside the timed region
+  cpu_baseline  the reference's scalar kernel (oracle/_ref, compiled from the
+          reference sources) on 1 host core over a seeded sample of A's rows
+  parity  sampled rows bit-exact against the oracle, learned C bit-identical
+          to exact C over the whole product, FP32-vs-FP64 error
+With --impl reference the reference's own CPU implementation is timed on all
+host cores over a seeded row sample of the same product, same metric and unit.
 
-The other workloads (--workload) print one JSON line of one-shot comparisons:
-exact-symbolic vs learned-binned, default vs autotuned bin parameters, and
-batched vs sequential products, with the FP32-vs-FP64 error of sampled rows.
-rmat is C = A * A for an R-MAT graph of 2^scale vertices (default 20, 16
-edges per vertex); its intermediate products exceed the int32 range of one
-CSR, so it runs as row panels of at most 2^31 - 1 products each.
+The other workloads print one JSON line each: poisson_reuse (descriptor
+reuse of the 1024^2 5-point Laplacian, numeric-only, CUDA graph), plain,
+tall_skinny, batched (one-shot comparisons: exact vs learned, batched vs
+sequential), coo (Matrix Market canonicalisation) and profile (one product of
+a named matrix, optionally a row range, for capturing a kernel).
 
-N > 1 (torchrun): every rank runs its own full-size product on its own GPU
-(independent products, no data-path collective; weak scaling); a gloo
-barrier brackets the timed loop and the step time is the max over ranks.
+N > 1 (torchrun): the product's panels are dealt to the ranks in contiguous
+groups of about equal products (strong scaling; no data-path collective,
+output rows are independent); a gloo barrier brackets each timed loop and the
+step time is the max over ranks.
 """
 
 from __future__ import annotations
@@ -46,7 +54,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -64,6 +71,10 @@ import numpy as np  # noqa: E402
 
 METRIC = "SpGEMM GFLOP/s, HBM % of roofline: learned-binned vs exact-symbolic, 1 B200"
 UNIT = "GFLOP/s"
+RMAT_DATA = ("synthetic R-MAT (a,b,c,d)=(0.57,0.19,0.19,0.05), 16 edge samples per vertex, "
+             "duplicates merged, values U(-1,1), seed 0")
+# default bin parameters of the library (tiny_ops, slack_shift, warp_cap_max, heavy_cw_log2)
+DEFAULT_PARAMS = (32, 2, 2048, 11)
 
 
 def log(*a):
@@ -132,8 +143,414 @@ def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
+def algorithmic_bytes(M, nnz_a, nnz_c, b_rows, nnz_b):
+    """Compulsory bytes of one product, 4(M+1) + 8 nnzA + 4(K+1) + 8 nnzB +
+    4(M+1) + 8 nnzC: every operand array read once (B counted as its own
+    operand also when it is A), C's row pointer and col_idx + values once
+    (col_idx read and values written on descriptor reuse)."""
+    return 4 * (M + 1) + 8 * nnz_a + 4 * (b_rows + 1) + 8 * nnz_b + 4 * (M + 1) + 8 * nnz_c
+
+
+def heavy_rows(ops, b_cols, params=DEFAULT_PARAMS):
+    """Rows the library bins as heavy (a warp per column chunk) under the bin
+    parameters: more products than the tiny bin and an upper bound
+    ub = min(ops, cols) whose table ub + (ub >> slack) passes warp_cap_max."""
+    tiny, slack, wmax, _ = params
+    ops = np.asarray(ops, np.int64)
+    ub = np.minimum(ops, b_cols)
+    return (ub > 0) & (ops > tiny) & (ub + (ub >> slack) > wmax)
+
+
 # ---------------------------------------------------------------------------
-# workloads
+# device helpers
+# ---------------------------------------------------------------------------
+
+class DevMat:
+    def __init__(self, M, torch):
+        self.rows, self.cols, self.nnz = M.rows, M.cols, M.nnz
+        d = lambda a: torch.from_numpy(np.ascontiguousarray(a if a.size else np.zeros(1, a.dtype))).cuda()  # noqa: E731
+        self.row_ptr, self.col_idx, self.values = d(M.row_ptr), d(M.col_idx), d(M.values)
+
+
+class PanelView:
+    """Rows [r0, r1) of a device CSR: the row pointer is a view into the full
+    one, so its offsets index the full column and value arrays directly."""
+
+    def __init__(self, M, r0, r1):
+        self.rows, self.cols = r1 - r0, M.cols
+        self.row_ptr = M.row_ptr[r0:r1 + 1]
+        self.col_idx, self.values = M.col_idx, M.values
+
+
+def _oneshot_dev(rv, A, B, algo):
+    import ctypes as C
+    L = rv.lib()
+    prp, pci, pv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    nnz = C.c_int32()
+    st = L.rvsp_cuda_spgemm_f32(algo, A.rows, A.cols, B.cols, A.row_ptr.data_ptr(),
+                                A.col_idx.data_ptr(), A.values.data_ptr(), B.row_ptr.data_ptr(),
+                                B.col_idx.data_ptr(), B.values.data_ptr(), C.byref(prp),
+                                C.byref(pci), C.byref(pv), C.byref(nnz), None)
+    rv.check(st, "rvsp_cuda_spgemm_f32")
+    return (prp.value, pci.value, pv.value), nnz.value
+
+
+class _DevArray:
+    """__cuda_array_interface__ view of a library-owned device array."""
+
+    def __init__(self, p, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (p, False),
+                                         "version": 3}
+
+
+def dev_tensor(torch, p, n, dtype):
+    """Zero-copy torch view of n elements at device address p."""
+    ts = {np.int32: "<i4", np.float32: "<f4"}[dtype]
+    if n == 0:
+        return torch.zeros(0, dtype=torch.int32 if dtype == np.int32 else torch.float32,
+                           device="cuda")
+    return torch.as_tensor(_DevArray(p, n, ts), device="cuda")
+
+
+def _time(fn, steps, warmup, torch):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    return statistics.median(ts)
+
+
+def _d2h(ptr_, n, dtype, torch):
+    """Copy n elements of a library-owned device array to the host."""
+    if n == 0:
+        return np.zeros(0, dtype)
+    return dev_tensor(torch, ptr_, n, dtype).cpu().numpy()
+
+
+def _fp64_errors(oracle, A, B, rows, rp, ci, v, base=0):
+    """Per-entry relative error of FP32 C rows against the FP64 oracle, with
+    a check that their columns match the oracle's."""
+    errs, same = [], True
+    for r in rows:
+        srp, sci, sv = oracle.spgemm_f32(A, B, int(r), int(r) + 1)
+        lo, hi = int(rp[r - base]), int(rp[r - base + 1])
+        same &= bool(np.array_equal(sci, ci[lo:hi]) and
+                     np.array_equal(sv.view(np.uint32), v[lo:hi].view(np.uint32)))
+        if sci.size:
+            d = oracle.numeric_f64(A, B, srp, sci, int(r), int(r) + 1)
+            errs.append(np.abs(v[lo:hi] - d) / np.maximum(np.abs(d), 1e-30))
+    e = np.concatenate(errs) if errs else np.zeros(1)
+    return same, {"max": float(e.max()), "median": float(np.median(e)),
+                  "p99": float(np.quantile(e, 0.99))}
+
+
+# ---------------------------------------------------------------------------
+# the R-MAT product (headline)
+# ---------------------------------------------------------------------------
+
+def rmat_product(scale):
+    from rvsp_b200 import gen, ranks
+    A = gen.rmat(scale=scale, edge_factor=16, seed=0)
+    ops = gen.row_products(A, A)
+    return A, ops, ranks.row_panels(ops)
+
+
+def row_sample(A, ops, frac, seed):
+    """A seeded uniform sample of A's rows as its own CSR (rows in order),
+    and its product count against B = A."""
+    from rvsp_b200.gen import CSR
+    rng = np.random.default_rng(seed)
+    m = max(1, int(round(A.rows * frac)))
+    rows = np.sort(rng.choice(A.rows, m, replace=False))
+    lens = np.diff(A.row_ptr.astype(np.int64))[rows]
+    rp = np.zeros(m + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    # entry k of the sample is entry k - rp[i] of sampled row i
+    idx = np.repeat(A.row_ptr[rows].astype(np.int64) - rp[:-1], lens) + np.arange(rp[-1])
+    S = CSR(m, A.cols, rp.astype(np.int32), A.col_idx[idx], A.values[idx])
+    return S, int(ops[rows].sum()), rows
+
+
+def reference_sample_rate(A, ops, threads, target_s, seed):
+    """The reference's one-shot kernel over a seeded row sample sized so one
+    call takes about target_s on `threads` host threads; (GFLOP/s, sample
+    description, seconds per call)."""
+    import oracle
+    frac = 1.0 / 1024  # pilot
+    S, Ps, rows = row_sample(A, ops, frac, seed)
+    t = oracle.ref_time_oneshot(S, A, nthreads=threads, repeats=1)
+    frac = min(0.25, frac * target_s / max(t, 1e-3))
+    S, Ps, rows = row_sample(A, ops, frac, seed)
+    t = oracle.ref_time_oneshot(S, A, nthreads=threads, repeats=1)
+    if t < 0:
+        raise RuntimeError("reference kernel failed on the sample")
+    desc = (f"{S.rows} seeded uniform rows of A ({frac:.5f} of {A.rows}) times A, "
+            f"{Ps} products, rvsp_spgemm_scalar_f32 one-shot")
+    return 2.0 * Ps / t / 1e9, desc, t, S, Ps
+
+
+def run_headline(args):
+    import torch
+
+    import oracle
+    import rvsp_b200 as rv
+    from rvsp_b200 import ranks
+
+    dist = ranks.init("gloo", timeout_s=1800)
+    torch.cuda.set_device(0)
+    torch.zeros(1, device="cuda")
+    rv.lib()
+    t0 = time.time()
+    A, ops, panels_all = rmat_product(args.rmat_scale)
+    P_all = int(ops.sum())
+    panels = ranks.shard_panels(panels_all, ops, RANK, WORLD)
+    log(f"rmat 2^{args.rmat_scale}: {A.rows} rows, nnz {A.nnz}, {P_all} products, "
+        f"{len(panels_all)} panels ({len(panels)} on this rank), generated in "
+        f"{time.time() - t0:.1f} s")
+    dA = DevMat(A, torch)
+    views = [PanelView(dA, r0, r1) for r0, r1 in panels]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def product(algo):
+        for v in views:
+            ptrs, n = _oneshot_dev(rv, v, dA, algo)
+            rv.free_device(*ptrs)
+
+    def timed(algo, steps, warmup):
+        for _ in range(warmup):
+            product(algo)
+        torch.cuda.synchronize()
+        ranks.barrier(dist)
+        torch.cuda.synchronize()
+        rv.kernel_timing(True)
+        l0 = rv.launch_count()
+        evs = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            product(algo)
+            e1.record()
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        launches = rv.launch_count() - l0
+        kt = rv.kernel_times()
+        rv.kernel_timing(False)
+        ranks.barrier(dist)
+        ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
+        return ranks.max_over_ranks(dist, ms), launches, kt
+
+    sampler = ClockSampler()
+    sampler.start()
+    ms_l, launches, kt_l = timed(rv.RVSP_CUDA_ALGO_LEARNED, args.steps, args.warmup)
+    ms_x, _, kt_x = timed(rv.RVSP_CUDA_ALGO_EXACT, args.steps, args.warmup)
+    clocks = sampler.stop()
+    value = 2.0 * P_all / (ms_l * 1e-3) / 1e9
+    exact_gflops = 2.0 * P_all / (ms_x * 1e-3) / 1e9
+
+    # verification pass (untimed): every panel exact and learned, compared on
+    # the device; C's row pointer kept for the byte counts; sampled rows of
+    # the first and the heaviest panel against the oracle
+    heavy_panel = int(np.argmax([ops[r0:r1].sum() for r0, r1 in panels]))
+    rng = np.random.default_rng(1)
+    identical = True
+    row_nnz = np.zeros(A.rows, np.int64)
+    parity_ok, errs = True, []
+    for pi, (v, (r0, r1)) in enumerate(zip(views, panels)):
+        px, nx = _oneshot_dev(rv, v, dA, rv.RVSP_CUDA_ALGO_EXACT)
+        pl, nl = _oneshot_dev(rv, v, dA, rv.RVSP_CUDA_ALGO_LEARNED)
+        m = r1 - r0
+        same = nx == nl
+        if same:
+            for k, (dt, n) in enumerate(((np.int32, m + 1), (np.int32, nx), (np.float32, nx))):
+                a = dev_tensor(torch, px[k], n, dt)
+                b = dev_tensor(torch, pl[k], n, dt)
+                same &= bool(torch.equal(a.view(torch.int32), b.view(torch.int32)))
+        identical &= same
+        rp = _d2h(px[0], m + 1, np.int32, torch).astype(np.int64)
+        row_nnz[r0:r1] = np.diff(rp)
+        if pi in (0, heavy_panel):
+            rows = np.sort(rng.choice(np.arange(r0, r1), min(args.check_rows, m), replace=False))
+            ci = _d2h(px[1], nx, np.int32, torch)
+            vv = _d2h(px[2], nx, np.float32, torch)
+            ok, e = _fp64_errors(oracle, A, A, rows, rp, ci, vv, base=r0)
+            parity_ok &= ok
+            errs.append(e)
+            del ci, vv
+        rv.free_device(*px)
+        rv.free_device(*pl)
+    nnz_c = int(ranks.sum_over_ranks(dist, int(row_nnz.sum())))
+    # misprediction of the learned sizing on the heaviest panel
+    lp = rv.Plan(rv.RVSP_CUDA_ALGO_LEARNED)
+    rv.check(lp.symbolic(views[heavy_panel], dA)[0], "learned symbolic")
+    ls = lp.learned_stats()
+    lp.close()
+
+    e2e = run_rmat_e2e(rv, A, ops, panels, args, torch)
+    if RANK != 0:
+        ranks.barrier(dist)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # roofline of the dominant kernel (largest share of the exact path's
+    # kernel time): algorithmic bytes of the rows it processes per launch
+    hbm, peak_kind = peaks()
+    fam, (fam_ms, fam_n) = max(kt_x.items(), key=lambda kv: kv[1][0])
+    heavy = heavy_rows(ops, A.cols)
+    a_len = np.diff(A.row_ptr.astype(np.int64))
+    per_panel = []
+    for r0, r1 in panels:
+        h = heavy[r0:r1]
+        per_panel.append(algorithmic_bytes(int(h.sum()), int(a_len[r0:r1][h].sum()),
+                                           int(row_nnz[r0:r1][h].sum()), A.rows, A.nnz))
+    bytes_heavy = sum(per_panel) / len(per_panel)
+    fam_launch_ms = fam_ms / max(fam_n, 1)
+    achieved = bytes_heavy / (fam_launch_ms * 1e-3) / 1e9 if fam.startswith("k_heavy") else None
+    bytes_product = sum(algorithmic_bytes(r1 - r0, int(a_len[r0:r1].sum()),
+                                          int(row_nnz[r0:r1].sum()), A.rows, A.nnz)
+                        for r0, r1 in panels)
+    steps_k = args.steps
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": WORLD,
+        "steps": steps_k, "warmup": args.warmup, "ms_per_step": round(ms_l, 3),
+        "higher_is_better": True, "scaling": "strong" if WORLD > 1 else "weak",
+        "vs_baseline": None, "dtype": "f32", "data": RMAT_DATA,
+        "config": {"workload": f"rmat_scale{args.rmat_scale}_ef16_c_eq_a_times_a",
+                   "rows": A.rows, "nnz_a": A.nnz, "products": P_all, "nnz_c": nnz_c,
+                   "panels": len(panels_all),
+                   "path": "one-shot rvsp_cuda_spgemm_f32 per row panel, device-resident operands",
+                   "l2": "flushed (256 MiB write) before every timed step; C (78 GB) >> L2",
+                   "parallelism": f"row panels over {WORLD} GPU(s), no data-path collective"},
+        "exact_gflops": round(exact_gflops, 3), "exact_ms_per_step": round(ms_x, 3),
+        "learned_over_exact": round(ms_x / ms_l, 4),
+        "learned_bit_identical_to_exact": bool(identical),
+        "parity": {"sampled_rows_bit_exact_vs_oracle": bool(parity_ok),
+                   "rows_checked": int(2 * args.check_rows),
+                   "fp32_vs_fp64_rel_err": errs},
+        "mispredict": {"panel": heavy_panel, **ls,
+                       "rate": ls["underpredicted_rows"] / max(ls["predicted_rows"], 1)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
+                     "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4) if achieved else None,
+                     "traffic": None, "traffic_source": "not measured in this run",
+                     "peak_source": f"{peak_kind} hbm_gbs", "kernel": fam,
+                     "bytes_per_launch": int(bytes_heavy), "launch_ms": round(fam_launch_ms, 3),
+                     "whole_product_frac_learned": round(
+                         bytes_product / (ms_l * 1e-3) / 1e9 / hbm, 4)},
+        "kernel_ms_per_step": {
+            "learned": {k: round(v[0] / steps_k, 3) for k, v in kt_l.items() if v[1]},
+            "exact": {k: round(v[0] / steps_k, 3) for k, v in kt_x.items() if v[1]}},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if WORLD == 1:
+        out["cpu_baseline"] = cpu_baseline_rmat(A, ops)
+    if args.extras:
+        out["extras"] = run_extras(args, rv, torch)
+    print(json.dumps(out), flush=True)
+    ranks.barrier(dist)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_rmat_e2e(rv, A, ops, panels, args, torch):
+    """The product through rvsp_spgemm_csr (learned backend) on host CSR:
+    each panel's A (its row pointer rebased, its entries a view) and B = A are
+    host arrays; the library uploads them and hands C back in malloc'd host
+    memory, freed by rvsp_csr_destroy. Wall time of all panels per step."""
+    import ctypes as C
+    L = rv.lib()
+    hb = rv.csr_struct(A.rows, A.cols, A.nnz, A.row_ptr, A.col_idx, A.values)
+    pa = []
+    for r0, r1 in panels:
+        s, e = int(A.row_ptr[r0]), int(A.row_ptr[r1])
+        rp = (A.row_ptr[r0:r1 + 1] - A.row_ptr[r0]).astype(np.int32)
+        ci, v = A.col_idx[s:e], A.values[s:e]
+        pa.append((rp, ci, v, rv.csr_struct(r1 - r0, A.cols, e - s, rp, ci, v)))
+    opts = rv.SpgemmOptions(rv.RVSP_BACKEND_CUDA_LEARNED, rv.RVSP_DTYPE_FP32, rv.RVSP_DTYPE_FP32)
+    h2d = d2h = 0
+
+    def step():
+        nonlocal h2d, d2h
+        h2d = d2h = 0
+        for (rp, ci, v, a), (r0, r1) in zip(pa, panels):
+            c = rv.CsrMatrix()
+            rv.check(L.rvsp_spgemm_csr(C.byref(a), C.byref(hb), C.byref(c), C.byref(opts)),
+                     "rvsp_spgemm_csr")
+            h2d += 4 * (rp.size + A.rows + 1) + 8 * (ci.size + A.nnz)
+            d2h += 4 * (r1 - r0 + 1) + 8 * c.nnz
+            L.rvsp_csr_destroy(C.byref(c))
+
+    steps = max(1, min(args.steps, args.e2e_steps))
+    step()  # warm-up
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        step()
+        ts.append(time.perf_counter() - t0)
+    t = statistics.mean(ts)
+    P = int(sum(ops[r0:r1].sum() for r0, r1 in panels))
+    return {"value": round(2.0 * P / t / 1e9, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "steps": steps,
+            "api": "rvsp_spgemm_csr (RVSP_BACKEND_CUDA_LEARNED) per row panel, host A/B/C",
+            "ms_per_step": round(t * 1e3, 1)}
+
+
+def cpu_baseline_rmat(A, ops):
+    """Reference scalar one-shot (oracle/_ref) on 1 host core, seeded row sample."""
+    import oracle
+    if not oracle.ref_available():
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    g, desc, t, _, _ = reference_sample_rate(A, ops, 1, 12.0, seed=7)
+    return {"value": round(g, 4), "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{desc}, {t:.1f} s, 1 thread"}
+
+
+def run_reference(args):
+    """The reference's own CPU kernel on all host cores (rank 0 only)."""
+    if RANK != 0:
+        return
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/librvsp_ref.so not built"}), flush=True)
+        return
+    if args.workload == "poisson_reuse":
+        return run_reference_poisson(args)
+    cores = len(os.sched_getaffinity(0))
+    A, ops, _ = rmat_product(args.rmat_scale)
+    _, desc, _, S, Ps = reference_sample_rate(A, ops, cores, 1.5, seed=11)
+    for _ in range(args.warmup):
+        oracle.ref_time_oneshot(S, A, nthreads=cores, repeats=1)
+    times = [oracle.ref_time_oneshot(S, A, nthreads=cores, repeats=1) for _ in range(args.steps)]
+    t = sum(times) / len(times)
+    value = 2.0 * Ps / t / 1e9
+    out = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": WORLD,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": RMAT_DATA,
+           "config": {"workload": f"rmat_scale{args.rmat_scale}_ef16_c_eq_a_times_a",
+                      "rows": A.rows, "nnz_a": A.nnz, "products": int(ops.sum()),
+                      "path": "reference rvsp_spgemm_scalar_f32 one-shot, row sample"},
+           "impl": "reference",
+           "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores,
+                            "kind": "reference",
+                            "sample": f"{desc}, {cores} threads on row panels per step"},
+           "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# descriptor reuse of the Poisson product
 # ---------------------------------------------------------------------------
 
 def poisson_workload():
@@ -143,32 +560,16 @@ def poisson_workload():
     return A, P
 
 
-def algorithmic_bytes(M, nnz_a, nnz_c, b_rows, nnz_b):
-    """Compulsory bytes of one product, 4(M+1) + 8 nnzA + 4(K+1) + 8 nnzB +
-    4(M+1) + 8 nnzC: every operand array read once (B counted as its own
-    operand also when it is A), C's row pointer and col_idx + values once
-    (col_idx read and values written on descriptor reuse)."""
-    return 4 * (M + 1) + 8 * nnz_a + 4 * (b_rows + 1) + 8 * nnz_b + 4 * (M + 1) + 8 * nnz_c
-
-
-def run_ours(args):
+def poisson_reuse(args, rv, torch, steps, warmup):
+    """Numeric-only reuse of the 1024^2 Poisson product (graph replay): device
+    time per step, roofline of the map-replay kernel, parity of the first fill
+    against the reference's output digests."""
     import ctypes as C
-
-    import torch
-
-    import rvsp_b200 as rv
-
-    from rvsp_b200 import ranks
-    dist = ranks.init("gloo", timeout_s=300)
-    torch.cuda.set_device(0)
-    torch.zeros(1, device="cuda")  # context current on this thread for both runtimes
     L = rv.lib()
-
     A, P = poisson_workload()
     M, nnz_a = A.rows, A.nnz
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
     drp, dci, dv = dev(A.row_ptr), dev(A.col_idx), dev(A.values.copy())
-
     plan = C.c_void_p()
     rv.check(L.rvsp_cuda_plan_create(C.byref(plan), rv.RVSP_CUDA_ALGO_EXACT), "plan")
     nnz = C.c_int64()
@@ -184,7 +585,6 @@ def run_ours(args):
                     dci.data_ptr(), dv.data_ptr(), crp.data_ptr(), cci.data_ptr(), cv.data_ptr())
     rv.check(L.rvsp_cuda_numeric(plan, *ptrs(), 1, None), "numeric fill")
     torch.cuda.synchronize()
-    # parity of the first pass against the reference kernel's output digests
     parity = None
     gold = os.path.join(ROOT, "tests", "golden", "ref_outputs.json")
     if os.path.exists(gold):
@@ -194,7 +594,6 @@ def run_ours(args):
                   sha(cv.cpu().numpy()) == d["values_sha256"])
     rv.check(L.rvsp_cuda_plan_set_async(plan, 1), "async")
     stream = torch.cuda.ExternalStream(L.rvsp_cuda_plan_stream(plan))
-
     rng = np.random.default_rng(1000 + RANK)
     R = 4
     variants = [dev((A.values * rng.uniform(0.5, 1.5, nnz_a)).astype(np.float32)) for _ in range(R)]
@@ -211,105 +610,43 @@ def run_ours(args):
                 ev1.record(stream)
         rv.check(st, "numeric reuse")
 
-    sampler = ClockSampler()
-    sampler.start()
-    for i in range(args.warmup):
+    for i in range(warmup):
         step(i)
     torch.cuda.synchronize()
-    ranks.barrier(dist)
-    torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
+           for _ in range(steps)]
     l0 = rv.launch_count()
-    for i in range(args.steps):
-        step(args.warmup + i, *evs[i])
+    for i in range(steps):
+        step(warmup + i, *evs[i])
     torch.cuda.synchronize()
     launches = rv.launch_count() - l0
-    ranks.barrier(dist)
-    times = [a.elapsed_time(b) for a, b in evs]  # ms
-    ms = sum(times) / len(times)
-    ms_max = ranks.max_over_ranks(dist, ms)
-    value = 2.0 * P * WORLD / (ms_max * 1e-3) / 1e9
-
-    # end to end through the public API with pinned host buffers
-    e2e = run_e2e(rv, A, P, args, torch)
-    # the one-shot product of the same matrices, exact-symbolic vs learned-binned
-    oneshot_cmp = compare_oneshot(rv, A, P, torch, args)
-    clocks = sampler.stop()
-
+    ms = sum(a.elapsed_time(b) for a, b in evs) / steps
     rv.check(L.rvsp_cuda_plan_set_async(plan, 0))
     L.rvsp_cuda_plan_destroy(plan)
-    ranks.barrier(dist)
-    if RANK != 0:
-        if dist:
-            dist.destroy_process_group()
-        return
-
     hbm, peak_kind = peaks()
     bytes_alg = algorithmic_bytes(M, nnz_a, nnz_c, M, nnz_a)
     bytes_distinct = bytes_alg - (4 * (M + 1) + 8 * nnz_a)  # B's arrays are A's
     achieved = bytes_alg / (ms * 1e-3) / 1e9
-    traffic = None
-    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tr_path):
-        traffic = json.load(open(tr_path)).get("poisson2d_1024_reuse")
-    out = {
-        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": WORLD,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 5),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (5-point Laplacian, values rescaled U(0.5,1.5) per step, seeded)",
-        "config": {"workload": "poisson2d_1024_descriptor_reuse", "grid": 1024, "rows": M,
-                   "nnz_a": nnz_a, "nnz_c": nnz_c, "products": P, "path": "numeric-only, CUDA graph",
-                   "l2": "flushed (256 MiB write) before every timed step",
-                   "parallelism": f"{WORLD} independent products, one per GPU"},
-        "parity_first_pass_vs_reference": parity,
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                     "frac": round(achieved / hbm, 4), "traffic": traffic,
-                     "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_tiny_reuse_map",
-                     "bytes_per_launch": bytes_alg,
-                     "frac_distinct_arrays": round(bytes_distinct / (ms * 1e-3) / 1e9 / hbm, 4)},
-        "e2e": e2e,
-        "oneshot_exact_vs_learned": oneshot_cmp,
-        "gpu_launches": int(launches),
-        "clocks": clocks,
-    }
-    if WORLD == 1:
-        out["cpu_baseline"] = cpu_baseline(A, P)
-    print(json.dumps(out), flush=True)
-    if dist:
-        dist.destroy_process_group()
+    return {"gflops": round(2.0 * P / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms, 5),
+            "steps": steps, "gpu_launches": int(launches),
+            "config": {"workload": "poisson2d_1024_descriptor_reuse", "rows": M, "nnz_a": nnz_a,
+                       "nnz_c": nnz_c, "products": P, "path": "numeric-only, CUDA graph",
+                       "l2": "flushed (256 MiB write) before every timed step"},
+            "parity_first_pass_vs_reference": parity,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                         "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_tiny_reuse_map",
+                         "bytes_per_launch": bytes_alg,
+                         "frac_distinct_arrays": round(
+                             bytes_distinct / (ms * 1e-3) / 1e9 / hbm, 4)}}
 
 
-def compare_oneshot(rv, A, P, torch, args):
-    """One-shot C = A*A (analysis + C allocation + fill), exact-symbolic vs
-    learned-binned, device-resident inputs, median wall time per product."""
-    dA = DevMat(A, torch)
-    out = {}
-    ref = None
-    for name, algo in (("exact", rv.RVSP_CUDA_ALGO_EXACT), ("learned", rv.RVSP_CUDA_ALGO_LEARNED)):
-        def fn(algo=algo):
-            ptrs, n = _oneshot_dev(rv, dA, dA, algo)
-            rv.free_device(*ptrs)
-        t = _time(fn, max(5, args.steps // 10), args.warmup, torch)
-        ptrs, n = _oneshot_dev(rv, dA, dA, algo)
-        v = _d2h(ptrs[2], n, np.float32, torch)
-        rv.free_device(*ptrs)
-        if ref is None:
-            ref = v
-        out[name + "_gflops"] = round(2.0 * P / t / 1e9, 3)
-        out[name + "_ms"] = round(t * 1e3, 4)
-    out["learned_over_exact"] = round(out["learned_gflops"] / out["exact_gflops"], 4)
-    out["learned_values_bit_identical"] = bool(np.array_equal(ref.view(np.uint32), v.view(np.uint32)))
-    return out
-
-
-def run_e2e(rv, A, P, args, torch):
-    import ctypes as C
-    L = rv.lib()
+def poisson_e2e(rv, A, P, steps, warmup):
+    """rvsp_spgemm_compute (descriptor reuse) with pinned host A and C."""
+    import torch
 
     def pinned(a):
-        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-        return t
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
 
     hrp, hci, hv = pinned(A.row_ptr), pinned(A.col_idx), pinned(A.values.copy())
     a = rv.csr_struct(A.rows, A.cols, A.nnz, hrp, hci, hv)
@@ -325,11 +662,11 @@ def run_e2e(rv, A, P, args, torch):
     rng = np.random.default_rng(2000 + RANK)
     variants = [(A.values * rng.uniform(0.5, 1.5, A.nnz)).astype(np.float32) for _ in range(4)]
     hvn = hv.numpy()
-    for i in range(args.warmup):
+    for i in range(warmup):
         hvn[:] = variants[i % 4]
         rv.check(d.compute(a, a, c, wsb))
     times = []
-    for i in range(args.steps):
+    for i in range(steps):
         hvn[:] = variants[i % 4]
         t0 = time.perf_counter()
         st = d.compute(a, a, c, wsb)
@@ -344,7 +681,42 @@ def run_e2e(rv, A, P, args, torch):
             "ms_per_step": round(t * 1e3, 4)}
 
 
-def cpu_baseline(A, P, budget_s=10.0):
+def run_poisson_line(args):
+    """--workload poisson_reuse: the descriptor-reuse product as its own line."""
+    import torch
+
+    import rvsp_b200 as rv
+    from rvsp_b200 import ranks
+    dist = ranks.init("gloo", timeout_s=300)
+    torch.cuda.set_device(0)
+    torch.zeros(1, device="cuda")
+    sampler = ClockSampler()
+    sampler.start()
+    ranks.barrier(dist)
+    r = poisson_reuse(args, rv, torch, args.steps, args.warmup)
+    ms_max = ranks.max_over_ranks(dist, r["ms_per_step"])
+    A, P = poisson_workload()
+    e2e = poisson_e2e(rv, A, P, args.steps, args.warmup)
+    clocks = sampler.stop()
+    ranks.barrier(dist)
+    if RANK == 0:
+        out = {"metric": METRIC, "value": round(2.0 * P * WORLD / (ms_max * 1e-3) / 1e9, 3),
+               "unit": UNIT, "n_gpus": WORLD, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (5-point Laplacian, values rescaled U(0.5,1.5) per step, seeded)",
+               "config": dict(r["config"], parallelism=f"{WORLD} independent products, one per GPU"),
+               "parity_first_pass_vs_reference": r["parity_first_pass_vs_reference"],
+               "roofline": r["roofline"], "e2e": e2e, "gpu_launches": r["gpu_launches"],
+               "clocks": clocks}
+        if WORLD == 1:
+            out["cpu_baseline"] = cpu_baseline_poisson(A, P)
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def cpu_baseline_poisson(A, P, budget_s=10.0):
     """Reference scalar numeric pass (oracle/_ref) on 1 host core, bounded sample."""
     import oracle
     if not oracle.ref_available():
@@ -361,15 +733,8 @@ def cpu_baseline(A, P, budget_s=10.0):
                       f"{t:.1f} s, 1 thread"}
 
 
-def run_reference(args):
-    """The reference's own CPU numeric pass on all host cores (row panels)."""
-    if RANK != 0:
-        return
+def run_reference_poisson(args):
     import oracle
-    if not oracle.ref_available():
-        print(json.dumps({"impl": "reference",
-                          "unavailable": "oracle/_ref/librvsp_ref.so not built"}), flush=True)
-        return
     A, P = poisson_workload()
     cores = len(os.sched_getaffinity(0))
     rp, ci, _, _, st = oracle.ref_spgemm(A, A)
@@ -403,155 +768,112 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
-# other BASELINE workloads: exact vs learned (and batched vs sequential)
+# the other configurations: exact vs learned, batched vs sequential
 # ---------------------------------------------------------------------------
 
-class DevMat:
-    def __init__(self, M, torch):
-        self.rows, self.cols, self.nnz = M.rows, M.cols, M.nnz
-        d = lambda a: torch.from_numpy(np.ascontiguousarray(a if a.size else np.zeros(1, a.dtype))).cuda()  # noqa: E731
-        self.row_ptr, self.col_idx, self.values = d(M.row_ptr), d(M.col_idx), d(M.values)
-
-
-def _oneshot_dev(rv, A, B, algo):
-    import ctypes as C
-    L = rv.lib()
-    prp, pci, pv = C.c_void_p(), C.c_void_p(), C.c_void_p()
-    nnz = C.c_int32()
-    st = L.rvsp_cuda_spgemm_f32(algo, A.rows, A.cols, B.cols, A.row_ptr.data_ptr(),
-                                A.col_idx.data_ptr(), A.values.data_ptr(), B.row_ptr.data_ptr(),
-                                B.col_idx.data_ptr(), B.values.data_ptr(), C.byref(prp),
-                                C.byref(pci), C.byref(pv), C.byref(nnz), None)
-    rv.check(st, "rvsp_cuda_spgemm_f32")
-    return (prp.value, pci.value, pv.value), nnz.value
-
-
-def _time(fn, steps, warmup, torch):
-    for _ in range(warmup):
-        fn()
-    torch.cuda.synchronize()
-    ts = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        fn()
-        torch.cuda.synchronize()
-        ts.append(time.perf_counter() - t0)
-    return statistics.median(ts)
-
-
-def _d2h(ptr_, n, dtype, torch):
-    """Copy n elements of a library-owned device array to the host."""
-    import ctypes as C
-    if n == 0:
-        return sha(np.zeros(0, dtype))
-    out = np.empty(n, dtype)
-    cuda = C.CDLL("libcuda.so.1")
-    cuda.cuMemcpyDtoH_v2.argtypes = [C.c_void_p, C.c_uint64, C.c_size_t]
-    assert cuda.cuMemcpyDtoH_v2(out.ctypes.data, ptr_, out.nbytes) == 0
-    return out
-
-
-class PanelView:
-    """Rows [r0, r1) of a device CSR: the row pointer is a view into the full
-    one, so its offsets index the full column and value arrays directly."""
-
-    def __init__(self, M, r0, r1):
-        self.rows, self.cols = r1 - r0, M.cols
-        self.row_ptr = M.row_ptr[r0:r1 + 1]
-        self.col_idx, self.values = M.col_idx, M.values
-
-
-def run_rmat(args, rv, gen, torch):
-    """Power-law C = A * A by row panels: exact vs learned, default vs tuned."""
+def compare_plain(rv, torch, steps, warmup, which="plain", ts_rows=2_000_000, fp64_rows=400):
+    """One-shot product of the plain or tall-skinny configuration, exact vs
+    learned, device-resident operands, median wall time per product."""
     import oracle
-    from rvsp_b200 import ranks
-    dist = ranks.init("gloo", timeout_s=900)
-    t0 = time.time()
-    A = gen.rmat(scale=args.rmat_scale, edge_factor=16, seed=0)
-    ops = gen.row_products(A, A)
-    P = int(ops.sum())
-    # every rank computes its contiguous group of row panels (strong scaling)
-    panels = ranks.shard_panels(ranks.row_panels(ops), ops, RANK, WORLD)
-    log(f"rmat scale {args.rmat_scale}: {A.rows} rows, nnz {A.nnz}, {P} products, "
-        f"{len(panels)} panels, generated in {time.time() - t0:.1f} s")
-    dA = DevMat(A, torch)
-    views = [PanelView(dA, r0, r1) for r0, r1 in panels]
-    heavy = int(np.argmax([ops[r0:r1].sum() for r0, r1 in panels]))
-
-    def run_all(algo):
-        nnz = 0
-        for v in views:
-            ptrs, n = _oneshot_dev(rv, v, dA, algo)
-            rv.free_device(*ptrs)
-            nnz += n
-        return nnz
-
-    steps = max(1, min(args.steps, 3))
-    times = {}
-    def timed(algo):
-        # all ranks start together; the job's time is the slowest rank's
-        ranks.barrier(dist)
-        return ranks.max_over_ranks(dist, _time(lambda: run_all(algo), steps, 1, torch))
-
-    nnz_c = ranks.sum_over_ranks(dist, run_all(rv.RVSP_CUDA_ALGO_EXACT))
+    from rvsp_b200 import gen
+    if which == "plain":
+        A = gen.uniform_fixed()
+        B = A
+        cfg = {"workload": "plain_4096x4096_16_per_row", "seed": 0}
+    else:
+        A, B = gen.tall_skinny(a_rows=ts_rows)
+        cfg = {"workload": f"tall_skinny_{ts_rows}x100000_x_100000^2", "a_rows": A.rows,
+               "nnz_a": A.nnz, "nnz_b": B.nnz}
+    P = gen.products(A, B)
+    dA, dB = DevMat(A, torch), DevMat(B, torch)
+    times, outs = {}, {}
     for name, algo in (("exact", rv.RVSP_CUDA_ALGO_EXACT), ("learned", rv.RVSP_CUDA_ALGO_LEARNED)):
-        times[name] = timed(algo)
-    # autotune on the panel with the most products, then every panel under the choice
-    plan = rv.Plan()
-    st, _, best, trials = plan.autotune(views[heavy], dA, reps=1)
-    rv.check(st, "autotune")
-    plan.close()
-    rv.check(rv.set_default_params(best))
+        def fn(algo=algo):
+            ptrs, n = _oneshot_dev(rv, dA, dB, algo)
+            rv.free_device(*ptrs)
+        times[name] = _time(fn, steps, warmup, torch)
+        ptrs, n = _oneshot_dev(rv, dA, dB, algo)
+        outs[name] = (_d2h(ptrs[0], A.rows + 1, np.int32, torch),
+                      _d2h(ptrs[1], n, np.int32, torch), _d2h(ptrs[2], n, np.float32, torch))
+        rv.free_device(*ptrs)
+    same = all(np.array_equal(a, b) for a, b in zip(outs["exact"], outs["learned"]))
+    nnz_c = int(outs["exact"][0][-1])
+    res = {"config": dict(cfg, rows=A.rows, products=P, nnz_c=nnz_c),
+           "exact_gflops": 2 * P / times["exact"] / 1e9,
+           "learned_gflops": 2 * P / times["learned"] / 1e9,
+           "learned_over_exact": times["exact"] / times["learned"],
+           "learned_bit_identical_to_exact": bool(same),
+           "ms": {k: v * 1e3 for k, v in times.items()}}
+    b_alg = algorithmic_bytes(A.rows, A.nnz, nnz_c, B.rows, B.nnz)
+    res["bytes_alg"] = b_alg
+    res["hbm_frac_exact"] = b_alg / times["exact"] / 1e9 / peaks()[0]
+    rng = np.random.default_rng(0)
+    rows = np.sort(rng.choice(A.rows, min(fp64_rows, A.rows), replace=False))
+    rp, ci, v = outs["exact"]
+    ok, e = _fp64_errors(oracle, A, B, rows, rp.astype(np.int64), ci, v)
+    res["sampled_rows_bit_exact_vs_oracle"] = bool(ok)
+    res["fp32_vs_fp64_rel_err"] = dict(e, rows_sampled=int(rows.size))
+    return res
+
+
+def compare_batched(rv, torch, steps, warmup, count=512):
+    """512 uneven products: 512 sequential one-shot calls vs the batched
+    entry point (exact and learned), spot-checked against the oracle."""
+    import oracle
+    from rvsp_b200 import gen
+    pairs = gen.batched_uneven(count=count)
+    prods = [gen.products(A, B) for A, B in pairs]
+    P = sum(prods)
+    dev_pairs = [(DevMat(A, torch), DevMat(B, torch)) for A, B in pairs]
+
+    def seq():
+        for dA, dB in dev_pairs:
+            ptrs, n = _oneshot_dev(rv, dA, dB, rv.RVSP_CUDA_ALGO_EXACT)
+            rv.free_device(*ptrs)
+    times = {"sequential_exact": _time(seq, max(1, steps // 3), 1, torch)}
+    for name, algo in (("batched_exact", rv.RVSP_CUDA_ALGO_EXACT),
+                       ("batched_learned", rv.RVSP_CUDA_ALGO_LEARNED)):
+        def fn(algo=algo):
+            ptrs, n, offs, coffs = rv.spgemm_batched(dev_pairs, algo)
+            rv.free_device(*ptrs)
+        times[name] = _time(fn, steps, warmup, torch)
+    ptrs, n, offs, coffs = rv.spgemm_batched(dev_pairs, rv.RVSP_CUDA_ALGO_LEARNED)
+    total_rows = int(offs[-1])
+    crp = _d2h(ptrs[0], total_rows + len(pairs), np.int32, torch).astype(np.int64)
+    ok = True
+    order = np.argsort(prods)
+    check = sorted({int(order[-1]), int(order[0]), 0, len(pairs) // 2, len(pairs) - 1})
+    for i in check:
+        A, B = pairs[i]
+        r0 = int(offs[i]) + i
+        e0, e1 = int(coffs[i]), int(coffs[i + 1])
+        wrp, wci, wv = oracle.spgemm_f32(A, B)
+        ci = _d2h(ptrs[1] + 4 * e0, e1 - e0, np.int32, torch)
+        v = _d2h(ptrs[2] + 4 * e0, e1 - e0, np.float32, torch)
+        ok &= bool(np.array_equal(crp[r0:r0 + A.rows + 1], wrp) and np.array_equal(ci, wci) and
+                   np.array_equal(v.view(np.uint32), wv.view(np.uint32)))
+    rv.free_device(*ptrs)
+    return {"config": {"workload": f"batched_{len(dev_pairs)}_uneven", "products": P,
+                       "rows": total_rows, "nnz_c": int(n), "calls": 1},
+            "gflops": {k: 2 * P / t / 1e9 for k, t in times.items()},
+            "ms": {k: t * 1e3 for k, t in times.items()},
+            "batched_learned_over_sequential": times["sequential_exact"] / times["batched_learned"],
+            "batched_learned_over_batched_exact": times["batched_exact"] / times["batched_learned"],
+            "products_checked_vs_oracle": check,
+            "spot_check_bit_exact_vs_oracle": bool(ok)}
+
+
+def run_extras(args, rv, torch):
+    """The other configurations' headline numbers, briefly: descriptor reuse
+    (Poisson), batched vs sequential, plain 4096^2."""
+    out = {}
     try:
-        for name, algo in (("tuned_exact", rv.RVSP_CUDA_ALGO_EXACT),
-                           ("tuned_learned", rv.RVSP_CUDA_ALGO_LEARNED)):
-            times[name] = timed(algo)
-        # misprediction rate of the learned sizing, measured against the exact recount
-        lp = rv.Plan(rv.RVSP_CUDA_ALGO_LEARNED)
-        st, lnnz = lp.symbolic(views[heavy], dA)
-        rv.check(st, "learned symbolic")
-        ls = lp.learned_stats()
-        lp.close()
-        # parity: sampled rows of the first and the heaviest panel, bit-exact
-        rng = np.random.default_rng(1)
-        ok, errs = True, []
-        for pi in sorted({0, heavy}):
-            r0, r1 = panels[pi]
-            for algo in (rv.RVSP_CUDA_ALGO_EXACT, rv.RVSP_CUDA_ALGO_LEARNED):
-                ptrs, n = _oneshot_dev(rv, views[pi], dA, algo)
-                rp = _d2h(ptrs[0], r1 - r0 + 1, np.int32, torch)
-                ci = _d2h(ptrs[1], n, np.int32, torch)
-                v = _d2h(ptrs[2], n, np.float32, torch)
-                rv.free_device(*ptrs)
-                for r in np.sort(rng.choice(np.arange(r0, r1), min(100, r1 - r0), replace=False)):
-                    srp, sci, sv = oracle.spgemm_f32(A, A, int(r), int(r) + 1)
-                    lo, hi = rp[r - r0], rp[r - r0 + 1]
-                    ok &= np.array_equal(sci, ci[lo:hi]) and \
-                        np.array_equal(sv.view(np.uint32), v[lo:hi].view(np.uint32))
-                    if algo == rv.RVSP_CUDA_ALGO_EXACT and sci.size:
-                        d = oracle.numeric_f64(A, A, srp, sci, int(r), int(r) + 1)
-                        errs.append(np.abs(v[lo:hi] - d) / np.maximum(np.abs(d), 1e-30))
-    finally:
-        rv.check(rv.set_default_params(None))
-    e = np.concatenate(errs) if errs else np.zeros(1)
-    g = {k: 2 * P / t / 1e9 for k, t in times.items()}
-    return {
-        "config": {"workload": f"rmat_scale{args.rmat_scale}_ef16_a0.57_b0.19_c0.19", "rows": A.rows,
-                   "nnz_a": A.nnz, "products": P, "nnz_c": nnz_c, "panels_this_rank": len(panels),
-                   "max_row_products": int(ops.max())},
-        "n_gpus": WORLD, "scaling": "strong",
-        "gflops": g, "ms": {k: t * 1e3 for k, t in times.items()},
-        "learned_over_exact": times["exact"] / times["learned"],
-        "tuned_learned_over_exact": times["exact"] / times["tuned_learned"],
-        "tuned_params": list(best),
-        "autotune_trials": [[list(p), round(ms, 3)] for p, ms in trials],
-        "mispredict": {"panel": heavy, **ls,
-                       "rate": ls["underpredicted_rows"] / max(ls["predicted_rows"], 1),
-                       "rerun_rate": ls["overflowed_rows"] / max(ls["predicted_rows"], 1)},
-        "sampled_rows_bit_exact_vs_oracle": bool(ok),
-        "fp32_vs_fp64_rel_err": {"max": float(e.max()), "median": float(np.median(e)),
-                                 "p99": float(np.quantile(e, 0.99))},
-    }
+        out["poisson_reuse"] = poisson_reuse(args, rv, torch, 20, 5)
+        out["plain_4096"] = compare_plain(rv, torch, 10, 3, "plain", fp64_rows=100)
+        out["batched_512"] = compare_batched(rv, torch, 3, 1)
+    except Exception as e:  # an extra never hides the headline
+        out["error"] = repr(e)
+    return out
 
 
 def run_coo(args, rv, torch):
@@ -600,8 +922,7 @@ def run_coo(args, rv, torch):
     t_cpu = time.perf_counter() - t0
     same = (np.array_equal(rp.astype(np.int64), wrp) and np.array_equal(ci, wci) and
             np.array_equal(vv.view(np.uint32), wv.view(np.uint32)))
-    bits = 2 * scale
-    passes = (bits + 7) // 8
+    passes = (2 * scale + 7) // 8
     # per entry: COO in (12 B), keys + payload written (16 B), each radix pass
     # reads and writes them (32 B), the run sums read them (16 B), CSR out (8 B)
     per_entry = 12 + 16 + 32 * passes + 16 + 8
@@ -617,119 +938,71 @@ def run_coo(args, rv, torch):
             "bit_exact_vs_oracle": bool(same)}
 
 
+def profile_matrices(name):
+    from rvsp_b200 import gen
+    if name.startswith("rmat"):
+        A = gen.rmat(scale=int(name[4:]), edge_factor=16, seed=0)
+        return A, A
+    if name == "tall":
+        return gen.tall_skinny(a_rows=2_000_000)
+    if name == "plain":
+        A = gen.uniform_fixed()
+        return A, A
+    if name == "poisson":
+        A = gen.poisson2d(1024)
+        return A, A
+    raise SystemExit(f"unknown matrix {name}")
+
+
+def run_profile(args, rv, torch):
+    """One-shot products of a named matrix (rmatS, tall, plain, poisson),
+    optionally a row range of A (a device panel), for capturing one kernel:
+    the first step is a warm-up; prints the median time and the per-family
+    kernel times of the timed steps."""
+    from rvsp_b200 import gen
+    A, B = profile_matrices(args.case)
+    r0, r1 = (0, A.rows) if args.rows is None else (int(x) for x in args.rows.split(":"))
+    dA, dB = DevMat(A, torch), DevMat(B, torch)
+    view = PanelView(dA, r0, r1)
+    P = int(gen.row_products(A, B)[r0:r1].sum())
+    if args.params:
+        rv.check(rv.set_default_params([int(x) for x in args.params.split(",")]), "params")
+    algo = rv.RVSP_CUDA_ALGO_EXACT if args.algo == "exact" else rv.RVSP_CUDA_ALGO_LEARNED
+    times = []
+    nnz = 0
+    for i in range(max(args.steps, 1)):
+        if i == 1:
+            rv.kernel_timing(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ptrs, nnz = _oneshot_dev(rv, view, dB, algo)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+        rv.free_device(*ptrs)
+    kt = rv.kernel_times()
+    rv.kernel_timing(False)
+    timed = times[1:] if len(times) > 1 else times
+    t = statistics.median(timed)
+    return {"case": args.case, "rows": [r0, r1], "algo": args.algo, "params": args.params,
+            "products": P, "nnz_c": nnz, "ms": t * 1e3, "gflops": 2 * P / t / 1e9,
+            "kernel_ms_per_step": {k: round(v[0] / len(timed), 3) for k, v in kt.items() if v[1]}}
+
+
 def run_compare(args):
-    """One-shot exact vs learned (and batched vs sequential) on a BASELINE config."""
     import torch
 
     import rvsp_b200 as rv
-    from rvsp_b200 import gen
     torch.zeros(1, device="cuda")
-    L = rv.lib()
-    res = {}
+    rv.lib()
     if args.workload in ("plain", "tall_skinny"):
-        if args.workload == "plain":
-            A = gen.uniform_fixed()
-            B = A
-            cfg = {"workload": "plain_4096x4096_16_per_row", "seed": 0}
-        else:
-            A, B = gen.tall_skinny(a_rows=args.ts_rows)
-            cfg = {"workload": f"tall_skinny_{args.ts_rows}x100000_x_100000^2", "a_rows": A.rows,
-                   "nnz_a": A.nnz, "nnz_b": B.nnz}
-        P = gen.products(A, B)
-        dA, dB = DevMat(A, torch), DevMat(B, torch)
-        times = {}
-        outs = {}
-        for name, algo in (("exact", rv.RVSP_CUDA_ALGO_EXACT), ("learned", rv.RVSP_CUDA_ALGO_LEARNED)):
-            def fn(algo=algo):
-                ptrs, n = _oneshot_dev(rv, dA, dB, algo)
-                rv.free_device(*ptrs)
-            times[name] = _time(fn, args.steps, args.warmup, torch)
-            ptrs, n = _oneshot_dev(rv, dA, dB, algo)
-            outs[name] = (_d2h(ptrs[0], A.rows + 1, np.int32, torch),
-                          _d2h(ptrs[1], n, np.int32, torch), _d2h(ptrs[2], n, np.float32, torch))
-            rv.free_device(*ptrs)
-        same = all(np.array_equal(a, b) for a, b in zip(outs["exact"], outs["learned"]))
-        nnz_c = int(outs["exact"][0][-1])
-        res["config"] = dict(cfg, rows=A.rows, products=P, nnz_c=nnz_c)
-        res["exact_gflops"] = 2 * P / times["exact"] / 1e9
-        res["learned_gflops"] = 2 * P / times["learned"] / 1e9
-        res["learned_over_exact"] = times["exact"] / times["learned"]
-        res["learned_bit_identical_to_exact"] = bool(same)
-        res["ms"] = {k: v * 1e3 for k, v in times.items()}
-        b_alg = algorithmic_bytes(A.rows, A.nnz, nnz_c, B.rows, B.nnz)
-        res["bytes_alg"] = b_alg
-        res["hbm_frac_learned"] = b_alg / times["learned"] / 1e9 / peaks()[0]
-        # FP64 error of the FP32 result on sampled rows
-        import oracle
-        rng = np.random.default_rng(0)
-        rows = np.sort(rng.choice(A.rows, min(2000, A.rows), replace=False))
-        errs = []
-        rp, ci, v = outs["exact"]
-        for r in rows[:400]:
-            srp, sci, sv = oracle.spgemm_f32(A, B, int(r), int(r) + 1)
-            d = oracle.numeric_f64(A, B, srp, sci, int(r), int(r) + 1)
-            got = v[rp[r]:rp[r + 1]]
-            assert np.array_equal(sci, ci[rp[r]:rp[r + 1]])
-            errs.append(np.abs(got - d) / np.maximum(np.abs(d), 1e-30))
-        e = np.concatenate(errs) if errs else np.zeros(1)
-        res["fp32_vs_fp64_rel_err"] = {"max": float(e.max()), "median": float(np.median(e)),
-                                       "p99": float(np.quantile(e, 0.99)), "rows_sampled": 400}
-    elif args.workload == "rmat":
-        res = run_rmat(args, rv, gen, torch)
+        res = compare_plain(rv, torch, args.steps, args.warmup,
+                            "plain" if args.workload == "plain" else "tall", args.ts_rows)
+    elif args.workload == "batched":
+        res = compare_batched(rv, torch, args.steps, args.warmup, args.batch_count)
     elif args.workload == "coo":
         res = run_coo(args, rv, torch)
-    elif args.workload == "batched":
-        pairs = gen.batched_uneven(count=args.batch_count)
-        prods = [gen.products(A, B) for A, B in pairs]
-        P = sum(prods)
-        dev_pairs = [(DevMat(A, torch), DevMat(B, torch)) for A, B in pairs]
-        # one batched call per group whose products (an upper bound on nnz)
-        # fit the int32 row pointer of a packed C
-        groups, cur, acc = [], [], 0
-        for i, p in enumerate(prods):
-            if cur and acc + p > (1 << 31) - 1:
-                groups.append(cur)
-                cur, acc = [], 0
-            cur.append(i)
-            acc += p
-        groups.append(cur)
-        def seq():
-            for dA, dB in dev_pairs:
-                ptrs, n = _oneshot_dev(rv, dA, dB, rv.RVSP_CUDA_ALGO_EXACT)
-                rv.free_device(*ptrs)
-        times = {"sequential_exact": _time(seq, max(1, args.steps // 10), 1, torch)}
-        for name, algo in (("batched_exact", rv.RVSP_CUDA_ALGO_EXACT),
-                           ("batched_learned", rv.RVSP_CUDA_ALGO_LEARNED)):
-            def fn(algo=algo):
-                for g in groups:
-                    ptrs, n, offs = rv.spgemm_batched([dev_pairs[i] for i in g], algo)
-                    rv.free_device(*ptrs)
-            times[name] = _time(fn, args.steps, args.warmup, torch)
-        # correctness: the group holding product 0 (and its spot checks)
-        g0 = groups[0]
-        pairs = [pairs[i] for i in g0]
-        ptrs, n, offs = rv.spgemm_batched([dev_pairs[i] for i in g0], rv.RVSP_CUDA_ALGO_LEARNED)
-        crp = _d2h(ptrs[0], int(offs[-1]) + 1, np.int32, torch)
-        cci = _d2h(ptrs[1], n, np.int32, torch)
-        cv = _d2h(ptrs[2], n, np.float32, torch)
-        rv.free_device(*ptrs)
-        # spot-check three products against the oracle
-        import oracle
-        ok = True
-        for i in (0, len(pairs) // 2, len(pairs) - 1):
-            A, B = pairs[i]
-            r0, r1 = int(offs[i]), int(offs[i + 1])
-            wrp, wci, wv = oracle.spgemm_f32(A, B)
-            lrp = crp[r0:r1 + 1] - crp[r0]
-            ok &= np.array_equal(lrp, wrp) and np.array_equal(cci[crp[r0]:crp[r1]], wci) and \
-                np.array_equal(cv[crp[r0]:crp[r1]].view(np.uint32), wv.view(np.uint32))
-        res["config"] = {"workload": f"batched_{len(dev_pairs)}_uneven", "products": P,
-                         "groups": len(groups), "group0_rows": int(offs[-1]), "group0_nnz_c": n}
-        res["gflops"] = {k: 2 * P / t / 1e9 for k, t in times.items()}
-        res["ms"] = {k: t * 1e3 for k, t in times.items()}
-        res["batched_learned_over_sequential"] = times["sequential_exact"] / times["batched_learned"]
-        res["batched_learned_over_batched_exact"] = times["batched_exact"] / times["batched_learned"]
-        res["spot_check_bit_exact_vs_oracle"] = bool(ok)
+    else:
+        res = run_profile(args, rv, torch)
     if RANK == 0:
         print(json.dumps({"workload": args.workload, **res}), flush=True)
 
@@ -737,23 +1010,35 @@ def run_compare(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="poisson_reuse",
-                    choices=["poisson_reuse", "plain", "batched", "tall_skinny", "rmat", "coo"])
+    ap.add_argument("--workload", default="rmat",
+                    choices=["rmat", "poisson_reuse", "plain", "batched", "tall_skinny", "coo",
+                             "profile"])
     ap.add_argument("--rmat-scale", type=int, default=20)
+    ap.add_argument("--check-rows", type=int, default=100,
+                    help="rmat: rows of two panels checked against the oracle")
+    ap.add_argument("--e2e-steps", type=int, default=2, help="rmat: timed e2e steps (host API)")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="rmat: skip the other configurations' numbers")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--ts-rows", type=int, default=2_000_000)
+    ap.add_argument("--case", default="rmat18", help="profile: rmatS, tall, plain, poisson")
+    ap.add_argument("--rows", default=None, help="profile: row range R0:R1 of A")
+    ap.add_argument("--algo", default="exact", choices=["exact", "learned"])
+    ap.add_argument("--params", default=None, help="profile: tiny,slack,warpmax,cwlog2")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload != "poisson_reuse":
-        run_compare(args)
+    elif args.workload == "rmat":
+        run_headline(args)
+    elif args.workload == "poisson_reuse":
+        run_poisson_line(args)
     else:
-        run_ours(args)
+        run_compare(args)
 
 
 if __name__ == "__main__":

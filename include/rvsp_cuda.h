@@ -4,7 +4,7 @@
  * This is the boundary the reference's host C calls to reach the GPU: plain
  * pointers, sizes and status codes, no CUDA or C++ types. Each entry point
  * names the reference function or struct it replaces when the reference adds
- * RVSP_BACKEND_CUDA (see INTEGRATION.md for the reference-side patch).
+ * RVSP_BACKEND_CUDA.
  *
  * Conventions
  *   - Return values are rvsp_status_t codes (0 = success).
@@ -260,17 +260,25 @@ RVSP_CUDA_API int rvsp_cuda_csr_validate(int32_t rows, int32_t cols, int32_t nnz
                            const int32_t *row_ptr, const int32_t *col_idx);
 
 /*
- * Batched products C_i = A_i * B_i, i < count, in one pipeline (no
- * counterpart in the reference, whose callers loop over rvsp_spgemm_csr).
+ * Batched products C_i = A_i * B_i, i < count, in one call (no counterpart
+ * in the reference, whose callers loop over rvsp_spgemm_csr: each product is
+ * what rv-sparse src/kernels/spgemm/gustavson_core_f32.inc:66-193 computes).
  * Sizes are host arrays [count]; operand arrays are host arrays [count] of
- * device pointers. The operands are packed on the device into block-stacked
- * matrices (A_i's columns shifted, B_i's kept) and multiplied as one
- * product, so every row of every product is binned and launched together.
- * Output: one packed C (device, callee-allocated, release with
- * rvsp_cuda_free) whose rows [row_offsets_out[i], row_offsets_out[i+1]) are
- * C_i, with C_i's own column indices; c_row_ptr is global (subtract
- * c_row_ptr[row_offsets_out[i]] for C_i's local row pointer).
- * row_offsets_out is a host array [count + 1]. algo is
+ * device pointers to whole CSR matrices (row_ptr[0] == 0; a row pointer that
+ * does not start at 0 returns RVSP_ERROR_INVALID_CSR). The operands are
+ * packed on the device into block-stacked matrices (A_i's columns shifted,
+ * B_i's kept); consecutive products are grouped so every group's C fits an
+ * int32 row pointer, and each group is multiplied as one product, so every
+ * row of every product in it is binned and launched together. Each product's
+ * own nnz must fit int32; their sum need not.
+ * Output (device, callee-allocated, release each with rvsp_cuda_free):
+ *   c_row_ptr_out  sum(a_rows[i] + 1) int32: C_i's row pointer (from 0) at
+ *                  c_row_ptr + row_offsets_out[i] + i
+ *   c_col_idx_out / c_values_out  C_i's entries (its own column indices) at
+ *                  offsets [c_offsets_out[i], c_offsets_out[i + 1])
+ *   c_nnz_out      total entries (int64)
+ * row_offsets_out and c_offsets_out are host arrays [count + 1]: the rows
+ * before product i and the entries before product i. algo is
  * RVSP_CUDA_ALGO_EXACT or RVSP_CUDA_ALGO_LEARNED.
  */
 RVSP_CUDA_API int rvsp_cuda_spgemm_batched_f32(
@@ -279,7 +287,8 @@ RVSP_CUDA_API int rvsp_cuda_spgemm_batched_f32(
     const int32_t *const *a_col_idx, const float *const *a_values,
     const int32_t *const *b_row_ptr, const int32_t *const *b_col_idx,
     const float *const *b_values, int32_t **c_row_ptr_out, int32_t **c_col_idx_out,
-    float **c_values_out, int64_t *c_nnz_out, int64_t *row_offsets_out);
+    float **c_values_out, int64_t *c_nnz_out, int64_t *row_offsets_out,
+    int64_t *c_offsets_out);
 
 /* ------------------------------------------------------------------------
  * Learned row-size predictor (no counterpart in the reference).
@@ -354,12 +363,16 @@ RVSP_CUDA_API int rvsp_cuda_plan_learned_stats(rvsp_cuda_plan_t plan, int64_t *o
  * counts (n int32, device) -> row_ptr (n + 1 int32, device), exclusive prefix
  * sum with row_ptr[n] = total; the same values the plan path writes to C's
  * row pointer. n is limited to 8,388,608 rows (RVSP_ERROR_INVALID_ARGUMENT
- * beyond). stream is a cudaStream_t (NULL: legacy default stream). With
+ * beyond). counts must be non-negative (a negative count gives an undefined
+ * row pointer). stream is a cudaStream_t (NULL: legacy default stream). With
  * total_out non-NULL the call synchronises the stream, stores the total and
  * returns RVSP_ERROR_ALLOCATION_FAILED when it exceeds INT32_MAX; with
- * total_out NULL it returns once the work is enqueued.
+ * total_out NULL it returns once the work is enqueued and an overflow is NOT
+ * reported (row_ptr then holds wrapped offsets): pass total_out whenever the
+ * total may pass INT32_MAX.
  * The first call on a device resolves the scratch array's address (once per
- * device, with that device current), so make it before any stream capture.
+ * device, with that device current; again after cudaDeviceReset, in the new
+ * context), so make it before any stream capture.
  * All calls on a device share the scratch: calls that overlap on the GPU race
  * and must be serialised by the caller.
  */
@@ -369,6 +382,23 @@ RVSP_CUDA_API int rvsp_cuda_row_ptr_noalloc(const int32_t *counts, int32_t n, in
 /* Number of kernels this library has launched in this process (graph
  * replays count each kernel node), for launch accounting in benchmarks. */
 RVSP_CUDA_API int64_t rvsp_cuda_launch_count(void);
+
+/*
+ * Device time of this library's kernels by family, for benchmarks and
+ * profiling (no counterpart in the reference, whose bench times whole calls,
+ * rv-sparse bench/bench.c:856-861). rvsp_cuda_kernel_timing(1) resets the
+ * totals and starts timing: every later launch of a family records a CUDA
+ * event pair on its plan's stream (graph replays are not timed);
+ * rvsp_cuda_kernel_timing(0) stops. rvsp_cuda_kernel_times waits for the
+ * recorded pairs and writes each family's total milliseconds (and launch
+ * count, when launches_out is non-NULL); n must be at least
+ * RVSP_CUDA_KERNEL_FAMILIES. rvsp_cuda_kernel_family(i) names family i
+ * (NULL out of range).
+ */
+#define RVSP_CUDA_KERNEL_FAMILIES 13
+RVSP_CUDA_API int rvsp_cuda_kernel_timing(int on);
+RVSP_CUDA_API int rvsp_cuda_kernel_times(double *ms_out, int64_t *launches_out, int32_t n);
+RVSP_CUDA_API const char *rvsp_cuda_kernel_family(int32_t i);
 
 #ifdef __cplusplus
 }

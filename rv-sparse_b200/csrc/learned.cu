@@ -13,11 +13,17 @@
 //                  values into its slot of an over-allocated buffer and record
 //                  its count; a row whose table fills up or whose count passes
 //                  its capacity is flagged (count -1) instead
-//   exact re-run   flagged rows and rows too large for a table (k_need) are
-//                  counted by the exact kernels under a row mask
+//                  heavy rows (a warp per column chunk) are sized by the
+//                  prediction too: each chunk takes its place in the row's
+//                  slot with an atomic add of its count, so the sweep leaves
+//                  every heavy row's exact count and every chunk's count; a
+//                  row whose chunks outgrow the slot is flagged
+//   exact re-run   flagged table rows are counted by the exact kernels under a
+//                  row mask (flagged heavy rows need no count: the sweep
+//                  counted them)
 //   C              scan of all counts -> row pointer; flagged rows are filled
 //                  in place by the exact FILL kernels, the rest are copied from
-//                  their slots (k_compact)
+//                  their slots (k_compact, k_compact_items)
 //
 // Every row is computed by the same order-preserving kernels as the exact
 // path, so the result is bit-identical to it; a misprediction costs time,
@@ -26,6 +32,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "mlp.cuh"
@@ -46,6 +53,7 @@ struct LearnedBinsOut {
     uint8_t* lbin;
     int32_t* lcap;
     uint8_t* predicted;  // 1 where the row is sized by the prediction
+    uint8_t* hmask;      // heavy rows sized by the prediction (null: heavy rows stay exact)
     int32_t* tile_hist;  // [NUM_BINS][tiles]
     int32_t* hist;       // [NUM_BINS]
     int64_t* slot_total;
@@ -86,11 +94,16 @@ __global__ void __launch_bounds__(AN_TILE)
                 cap = ub[row];
             } else {
                 lb = LBIN_EXACT;
+                if (out.hmask) {  // a slot of the predicted size for its chunks
+                    cap = c;
+                    predicted = 1;
+                }
             }
         }
         out.lbin[row] = (uint8_t)lb;
         out.lcap[row] = cap;
         out.predicted[row] = (uint8_t)predicted;
+        if (out.hmask) out.hmask[row] = (uint8_t)(lb == LBIN_EXACT && predicted);
     }
     // warp-aggregated histogram and slot total
     unsigned left = __ballot_sync(FULL, lb >= 0);
@@ -117,20 +130,25 @@ __global__ void __launch_bounds__(AN_TILE)
 // stats: [0] rows sized by the prediction, [1] of those, rows that outgrew
 //        it, [2] rows too large for a table, [3] sum of counts, [4] sum of
 //        capacities and [6] sum of upper bounds of predicted rows that fit
+// Heavy rows sized by the prediction (hmask; null when there are none) were
+// counted by the sweep: only those whose slot overflowed (hovf) need the
+// exact fill, and their counts stand.
 __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
                        const uint8_t* __restrict__ predicted, const int32_t* __restrict__ lcap,
                        const int32_t* __restrict__ ub, int32_t* __restrict__ cnt,
-                       uint8_t* __restrict__ need,
+                       uint8_t* __restrict__ need, const uint8_t* __restrict__ hmask,
+                       const uint8_t* __restrict__ hovf,
                        int32_t* __restrict__ n_need, int64_t* __restrict__ stats) {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
     bool nd = false, ovf = false, big = false, pr = false, under = false;
     int64_t fitc = 0, fitcap = 0, fitub = 0;
     if (row < rows) {
         const int lb = lbin[row];
+        const bool hslot = hmask && hmask[row];
         pr = predicted[row] != 0;
         big = lb == LBIN_EXACT;
-        ovf = lb >= BIN_WARP0 && lb < LBIN_EXACT && cnt[row] < 0;
-        nd = big || ovf;
+        ovf = hslot ? hovf[row] != 0 : (lb >= BIN_WARP0 && lb < LBIN_EXACT && cnt[row] < 0);
+        nd = (big && !hslot) || ovf;
         under = pr && (ovf || cnt[row] > lcap[row]);
         if (pr && !ovf) {
             fitc = cnt[row];
@@ -138,7 +156,7 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
             fitub = ub[row];
         }
         need[row] = nd ? 1 : 0;
-        if (nd) cnt[row] = 0;
+        if (nd && !hslot) cnt[row] = 0;
     }
     const unsigned mn = __ballot_sync(FULL, nd), mo = __ballot_sync(FULL, ovf && pr),
                    mb = __ballot_sync(FULL, big), mp = __ballot_sync(FULL, pr),
@@ -240,6 +258,32 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Copy the chunks of heavy rows finished in their slots into C: one warp per
+// work item (grid-stride), the chunk's entries from its slot offset to its
+// place in C (its row's start plus the counts of the row's earlier chunks).
+__global__ void __launch_bounds__(256)
+    k_compact_items(const HeavyItem* __restrict__ items, int32_t n,
+                    const uint8_t* __restrict__ hmask, const uint8_t* __restrict__ need,
+                    const int32_t* __restrict__ item_cnt, const int32_t* __restrict__ item_off,
+                    const int64_t* __restrict__ item_scan, const int64_t* __restrict__ slot_off,
+                    const int32_t* __restrict__ c_rp, const int32_t* __restrict__ tmp_ci,
+                    const float* __restrict__ tmp_v, int32_t* __restrict__ c_ci,
+                    float* __restrict__ c_v) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += nwarps) {
+        const HeavyItem it = items[w];
+        if (it.chunk < 0 || !hmask[it.row] || need[it.row]) continue;
+        const int k = item_cnt[w];
+        const int64_t src = slot_off[it.row] + item_off[w];
+        const int64_t dst = (int64_t)c_rp[it.row] + (item_scan[w] - item_scan[it.first]);
+        for (int x = lane; x < k; x += 32) {
+            c_ci[dst + x] = tmp_ci[src + x];
+            c_v[dst + x] = tmp_v[src + x];
+        }
+    }
+}
+
 // Enqueued by analyze() before its host synchronisation: prediction and
 // predicted-capacity bins, so one round trip returns both histograms.
 static int learned_pre_sync(rvsp_cuda_plan* plan) {
@@ -262,18 +306,26 @@ static int learned_pre_sync(rvsp_cuda_plan* plan) {
     ENS(plan->need, M);
     ENS(plan->row_flag, M);
     ENS(plan->pflag, M);
+    ENS(plan->hmask, M);
+    ENS(plan->hovf, M);
 #undef ENS
     Misc* misc = plan->misc.as<Misc>();
-    launch_mlp_infer(model, plan->feat.as<float4>(), plan->ub.as<int32_t>(), plan->bin.as<uint8_t>(),
-                     (int32_t)M, plan->pred_cap.as<int32_t>(), plan->stream);
-    note_launch(plan, 1);
-    LearnedBinsOut lo{plan->lbin.as<uint8_t>(), plan->lcap.as<int32_t>(),
-                      plan->pflag.as<uint8_t>(), plan->ltile_hist.as<int32_t>(), misc->lhist,
-                      &misc->slot_total};
-    k_learned_bins<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(
-        (int32_t)M, plan->bin.as<uint8_t>(), plan->ops.as<int64_t>(), plan->ub.as<int32_t>(),
-        plan->pred_cap.as<int32_t>(), lo, plan->params);
-    note_launch(plan, 1);
+    {
+        KTime kt(plan->stream, plan->capturing, KF_LEARNED);
+        launch_mlp_infer(model, plan->feat.as<float4>(), plan->ub.as<int32_t>(),
+                         plan->bin.as<uint8_t>(), (int32_t)M, plan->pred_cap.as<int32_t>(),
+                         plan->stream);
+        // heavy rows take predicted slots only in the fused sweep (the
+        // one-shot product); the descriptor's count keeps them exact
+        LearnedBinsOut lo{plan->lbin.as<uint8_t>(), plan->lcap.as<int32_t>(),
+                          plan->pflag.as<uint8_t>(),
+                          plan->heavy_slots ? plan->hmask.as<uint8_t>() : nullptr,
+                          plan->ltile_hist.as<int32_t>(), misc->lhist, &misc->slot_total};
+        k_learned_bins<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(
+            (int32_t)M, plan->bin.as<uint8_t>(), plan->ops.as<int64_t>(), plan->ub.as<int32_t>(),
+            plan->pred_cap.as<int32_t>(), lo, plan->params);
+    }
+    note_launch(plan, 2);
     return scan_counts(plan, plan->ltile_hist.as<int32_t>(), NUM_BINS * tiles, nullptr,
                        plan->ltile_off.as<int32_t>(), &misc->ltile_total);
 }
@@ -286,6 +338,7 @@ static int learned_pre_sync(rvsp_cuda_plan* plan) {
 // slot_off) for learned_finish; without, the sweep is the COUNT kernels with
 // tables sized by the prediction (the descriptor's structure analysis).
 int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool fused) {
+    plan->heavy_slots = fused;
     int st = analyze(plan, A, B, true, learned_pre_sync);
     if (st) return st;
     trace_point("learned: analysis + bins");
@@ -327,26 +380,40 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
         (e = cudaMemsetAsync(plan->item_cnt.p, 0, (size_t)plan->n_items * 4, plan->stream)) !=
             cudaSuccess)
         return fail(e, "memset");
+    const bool hslots = fused && plan->n_items > 0;
+    if (hslots && ((e = plan->item_off.ensure((size_t)plan->n_items * 4)) != cudaSuccess ||
+                   (e = cudaMemsetAsync(plan->hovf.p, 0, M, plan->stream)) != cudaSuccess))
+        return fail(e, "heavy slots");
     // one sweep over the predicted-capacity bins
     RowOut fo{plan->cnt.as<int32_t>(), nullptr, plan->tmp_ci.as<int32_t>(), plan->tmp_v.as<float>(),
               &misc->err, false};
     fo.ctl.slot_off = fused ? plan->slot_off.as<int64_t>() : nullptr;
     fo.ctl.learned = 1;
+    if (hslots) {
+        fo.ctl.item_off = plan->item_off.as<int32_t>();
+        fo.ctl.ovf = plan->hovf.as<uint8_t>();
+    }
     fo.learned_bins = true;
     run_rows(plan, fused ? FILL : COUNT, A, B, fo);
-    k_need<<<(unsigned)((M + 255) / 256), 256, 0, plan->stream>>>(
-        (int32_t)M, plan->lbin.as<uint8_t>(), plan->pflag.as<uint8_t>(),
-        plan->lcap.as<int32_t>(), plan->ub.as<int32_t>(), plan->cnt.as<int32_t>(),
-        plan->need.as<uint8_t>(),
-        &misc->n_need, misc->lstats);
+    {
+        KTime ktn(plan->stream, plan->capturing, KF_LEARNED);
+        k_need<<<(unsigned)((M + 255) / 256), 256, 0, plan->stream>>>(
+            (int32_t)M, plan->lbin.as<uint8_t>(), plan->pflag.as<uint8_t>(),
+            plan->lcap.as<int32_t>(), plan->ub.as<int32_t>(), plan->cnt.as<int32_t>(),
+            plan->need.as<uint8_t>(), hslots ? plan->hmask.as<uint8_t>() : nullptr,
+            hslots ? plan->hovf.as<uint8_t>() : nullptr, &misc->n_need, misc->lstats);
+    }
     note_launch(plan, 1);
     // exact counts of the rows the sweep could not finish (tiny rows never overflow)
     RowOut co{plan->cnt.as<int32_t>(), nullptr, nullptr, nullptr, &misc->err, false};
     co.ctl.only = plan->need.as<uint8_t>();
     const int32_t tiny = plan->bin_count[BIN_TINY];
+    const int32_t items = plan->n_items;
     plan->bin_count[BIN_TINY] = 0;
+    if (hslots) plan->n_items = 0;  // the sweep counted the heavy rows
     run_rows(plan, COUNT, A, B, co);
     plan->bin_count[BIN_TINY] = tiny;
+    plan->n_items = items;
     if ((st = scan_counts(plan, plan->cnt.as<int32_t>(), M, nullptr, plan->c_rp.as<int32_t>(),
                           &misc->scan_total)))
         return st;
@@ -391,6 +458,7 @@ int learned_finish(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, int
     }
     const int32_t* lrows = plan->lbin_rows.as<int32_t>();
     const int32_t nt = plan->lcount[BIN_TINY];
+    KTime kt(plan->stream, plan->capturing, KF_COMPACT);
     if (nt > 0) {
         k_compact<<<(unsigned)(((int64_t)nt + 255) / 256), 256, 0, plan->stream>>>(
             lrows + plan->loffs.off[BIN_TINY], nt, plan->need.as<uint8_t>(), plan->cnt.as<int32_t>(),
@@ -404,6 +472,15 @@ int learned_finish(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, int
         k_compact<<<(unsigned)(((int64_t)nw + 255) / 256), 256, 0, plan->stream>>>(
             lrows + plan->loffs.off[BIN_WARP0], nw, plan->need.as<uint8_t>(),
             plan->cnt.as<int32_t>(), plan->slot_off.as<int64_t>(), plan->c_rp.as<int32_t>(),
+            plan->tmp_ci.as<int32_t>(), plan->tmp_v.as<float>(), c_ci, c_v);
+        note_launch(plan, 1);
+    }
+    if (plan->heavy_slots && plan->n_items > 0) {
+        const int64_t grid = std::min<int64_t>(((int64_t)plan->n_items + 7) / 8, 148 * 64);
+        k_compact_items<<<(unsigned)grid, 256, 0, plan->stream>>>(
+            plan->items.as<HeavyItem>(), plan->n_items, plan->hmask.as<uint8_t>(),
+            plan->need.as<uint8_t>(), plan->item_cnt.as<int32_t>(), plan->item_off.as<int32_t>(),
+            plan->item_scan.as<int64_t>(), plan->slot_off.as<int64_t>(), plan->c_rp.as<int32_t>(),
             plan->tmp_ci.as<int32_t>(), plan->tmp_v.as<float>(), c_ci, c_v);
         note_launch(plan, 1);
     }

@@ -7,7 +7,7 @@
 // gradient, back-propagates, and reduces the weight gradients over its
 // samples in shared memory before adding them to the global gradient; a
 // second kernel applies Adam. The gradient of the mean batch loss is what the
-// FP64 oracle (oracle/oracle.py, mlp_forward_backward_f64) checks.
+// tests check against an FP64 restatement of the same network.
 
 #include <cuda_runtime.h>
 #include <dlfcn.h>

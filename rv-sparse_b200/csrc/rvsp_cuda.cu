@@ -59,6 +59,63 @@ bool is_dev(const void* p) {
     return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
+// ---------------------------------------------------------------------------
+// kernel-family timing (rvsp_cuda_kernel_timing / rvsp_cuda_kernel_times)
+// ---------------------------------------------------------------------------
+static std::atomic<bool> g_ktime_on{false};
+static std::mutex g_ktime_mu;
+struct KPending {
+    int fam;
+    cudaEvent_t e0, e1;
+};
+static std::vector<KPending> g_ktime_pending;
+static double g_ktime_ms[KF_NUM];
+static int64_t g_ktime_n[KF_NUM];
+
+bool ktime_enabled() { return g_ktime_on.load(std::memory_order_relaxed); }
+
+// Reads every queued pair (waiting for its end event) into the totals.
+static void ktime_drain_locked() {
+    for (const KPending& k : g_ktime_pending) {
+        float ms = 0.0f;
+        if (cudaEventSynchronize(k.e1) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, k.e0, k.e1) == cudaSuccess) {
+            g_ktime_ms[k.fam] += ms;
+            g_ktime_n[k.fam] += 1;
+        }
+        cudaEventDestroy(k.e0);
+        cudaEventDestroy(k.e1);
+    }
+    g_ktime_pending.clear();
+    cudaGetLastError();
+}
+
+KTime::KTime(cudaStream_t stream, bool capturing, int family) {
+    if (!ktime_enabled() || capturing) return;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventRecord(e0, stream) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        e0 = nullptr;
+        cudaGetLastError();
+        return;
+    }
+    st = stream;
+    fam = family;
+}
+
+KTime::~KTime() {
+    if (!e0) return;
+    cudaEvent_t e1 = nullptr;
+    if (cudaEventCreate(&e1) != cudaSuccess || cudaEventRecord(e1, st) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        cudaGetLastError();
+        return;
+    }
+    std::lock_guard<std::mutex> lk(g_ktime_mu);
+    g_ktime_pending.push_back({fam, e0, e1});
+    if (g_ktime_pending.size() >= 4096) ktime_drain_locked();
+}
+
 cudaError_t DevBuf::ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
     if (p) cudaFree(p);
@@ -130,11 +187,18 @@ static void set_mode_attrs() {
                          HEAVY_SMEM_MAX);
 }
 
-// Heavy kernel shape for every mode and chunk width: warps per CTA chosen to
-// keep the most warps resident per SM (each warp holds its own accumulator
-// and bitmap in shared memory), and the resident CTAs per SM; the launches
-// fill the GPU once and the warps pull work items from a counter.
-static int g_heavy_w[3][HEAVY_CW_LOG2_MAX + 1];
+// Heavy kernel shape for every chunk width: chunks (warps) per CTA, the
+// largest group up to HEAVY_GROUP_MAX whose FILL accumulators, bitmaps and
+// staging fit one CTA's shared memory (every mode of a plan shares the
+// padded work items, hence one group size per chunk width), and the resident
+// CTAs per SM of each mode; the launches fill the GPU once and the CTAs pull
+// groups from a counter.
+int heavy_group(int cw_log2) {
+    int g = HEAVY_GROUP_MAX;
+    // (1 KB left for the kernel's static shared memory)
+    while (g > 1 && heavy_grp_smem_bytes(FILL, 1 << cw_log2, g) > HEAVY_SMEM_MAX - 1024) --g;
+    return g;
+}
 static int g_heavy_ctas[3][HEAVY_CW_LOG2_MAX + 1];
 static int g_sms = 148;
 
@@ -150,25 +214,15 @@ void init_kernel_attributes() {
         for (int cl = HEAVY_CW_LOG2_MIN; cl <= HEAVY_CW_LOG2_MAX; ++cl) {
             const void* fns[3] = {(const void*)k_heavy<COUNT>, (const void*)k_heavy<FILL>,
                                   (const void*)k_heavy<REUSE>};
+            const int G = heavy_group(cl);
             for (int m = 0; m < 3; ++m) {
-                const size_t per = (size_t)heavy_smem_bytes(m, 1 << cl);
-                int best_w = 1, best_n = 1, best = 0;
-                for (int W = 1; W <= HEAVY_MAX_WARPS; ++W) {
-                    if (W * per > (size_t)HEAVY_SMEM_MAX) break;
-                    int n = 0;
-                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fns[m], W * 32, W * per) !=
-                        cudaSuccess) {
-                        cudaGetLastError();
-                        continue;
-                    }
-                    if (n * W > best) {
-                        best = n * W;
-                        best_w = W;
-                        best_n = n;
-                    }
+                int n = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                        &n, fns[m], G * 32, heavy_grp_smem_bytes(m, 1 << cl, G)) != cudaSuccess) {
+                    cudaGetLastError();
+                    n = 1;
                 }
-                g_heavy_w[m][cl] = best_w;
-                g_heavy_ctas[m][cl] = best_n;
+                g_heavy_ctas[m][cl] = n > 0 ? n : 1;
             }
         }
         cudaGetLastError();
@@ -212,6 +266,7 @@ static void launch_warp(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
                                          : plan->bin_rows.as<int32_t>() + plan->offs.off[b];
     const int32_t* lo = plan->list_off.as<int32_t>() + plan->offs.off[b];
     uint16_t* pm = plan->pm16.as<uint16_t>() + plan->pm16_base[b];
+    KTime kt(plan->stream, plan->capturing, KF_WARP_COUNT + MODE);
     if (MODE == REUSE && o.maps) {
         constexpr int WM = map_warps<CAP>();
         k_warp_reuse_map<CAP, WM><<<(n + WM - 1) / WM, WM * 32, WM * 4 * CAP, plan->stream>>>(
@@ -236,9 +291,12 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
     for (int b = BIN_TINY; b < NUM_BINS; ++b) {
         const int n = o.learned_bins ? plan->lcount[b] : plan->bin_count[b];
         if (n == 0) continue;
-        if (o.learned_bins && b == BIN_HEAVY) continue;  // left to the exact path
+        // heavy rows in the learned sweep: into their predicted slots when
+        // the sweep fills (ctl.item_off), else left to the exact path
+        if (o.learned_bins && b == BIN_HEAVY && !o.ctl.item_off) continue;
         const int32_t* r = rows + (o.learned_bins ? plan->loffs.off[b] : plan->offs.off[b]);
         if (b == BIN_TINY) {
+            KTime kt(plan->stream, plan->capturing, KF_TINY_COUNT + MODE);
             const int32_t* lo = plan->list_off.as<int32_t>() + plan->offs.off[b];
             const int grid = (n + TINY_TPB - 1) / TINY_TPB;
             if (MODE == REUSE && o.maps)
@@ -261,19 +319,23 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
                 default: launch_warp<4096, MODE>(plan, A, B, b, o); break;
             }
         } else if (plan->n_items > 0) {
+            KTime kt(plan->stream, plan->capturing, KF_HEAVY_COUNT + MODE);
             const int cl = plan->params.heavy_cw_log2;
-            const int W = g_heavy_w[MODE][cl];
+            const int G = heavy_group(cl);
+            const int ngroups = plan->n_items / G;
             const int64_t fill = (int64_t)g_sms * g_heavy_ctas[MODE][cl];
-            const int grid = (int)std::min<int64_t>((plan->n_items + W - 1) / W, fill);
+            const int grid = (int)std::min<int64_t>(ngroups, fill);
             const HeavyAux aux{plan->bmeta.as<int4>(), plan->bdoff.as<int64_t>(),
                                plan->dir_ok ? plan->bdir.as<int32_t>() : nullptr,
                                plan->ameta_ok ? plan->ameta.as<int4>() : nullptr,
                                plan->ameta_ok ? plan->adoff.as<int32_t>() : nullptr};
             int32_t* queue = &plan->misc.as<Misc>()->heavy_queue;
             cudaMemsetAsync(queue, 0, sizeof(int32_t), plan->stream);
-            k_heavy<MODE><<<grid, W * 32, W * heavy_smem_bytes(MODE, 1 << cl), plan->stream>>>(
-                A, B, plan->items.as<HeavyItem>(), plan->n_items, plan->item_cnt.as<int32_t>(),
-                o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, o.ctl, cl,
+            RowCtl ctl = o.ctl;
+            if (o.learned_bins) ctl.only = plan->hmask.as<uint8_t>();  // rows kept heavy
+            k_heavy<MODE><<<grid, G * 32, heavy_grp_smem_bytes(MODE, 1 << cl, G), plan->stream>>>(
+                A, B, plan->items.as<HeavyItem>(), ngroups, G, plan->item_cnt.as<int32_t>(),
+                o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, ctl, cl,
                 aux, queue);
             note_launch(plan, 1);
         }
@@ -295,6 +357,7 @@ int scan_counts(rvsp_cuda_plan* plan, const int32_t* in, int64_t n, int64_t* out
     cudaError_t e = plan->scan_tmp.ensure((size_t)ntiles * sizeof(int64_t));
     if (e != cudaSuccess) return fail(e, "scan workspace");
     int64_t* tmp = plan->scan_tmp.as<int64_t>();
+    KTime kt(plan->stream, plan->capturing, KF_SCAN);
     k_scan_reduce<<<(unsigned)ntiles, SCAN_TPB, 0, plan->stream>>>(in, n, tmp);
     k_scan_tiles<<<1, SCAN_TPB, 0, plan->stream>>>(tmp, ntiles, total_dev);
     k_scan_apply<<<(unsigned)ntiles, SCAN_TPB, 0, plan->stream>>>(
@@ -390,7 +453,11 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
                    plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
                    features ? plan->feat.as<float4>() : nullptr, misc->hist,
                    plan->tile_hist.as<int32_t>(), misc->totals, misc->bin_prod, &misc->err};
-    k_analyze<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(A, B, out, plan->params);
+    {
+        KTime kt(plan->stream, plan->capturing, KF_ANALYSIS);
+        k_analyze<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(
+            A, B, out, plan->params, heavy_group(plan->params.heavy_cw_log2));
+    }
     note_launch(plan, 1);
     int st = scan_counts(plan, plan->tile_hist.as<int32_t>(), NUM_BINS * tiles, nullptr,
                          plan->tile_off.as<int32_t>(), &misc->tile_total);
@@ -439,8 +506,11 @@ int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
         (e = plan->bdoff.ensure(K * 8)) != cudaSuccess)
         return fail(e, "heavy lookups");
     Misc* misc = plan->misc.as<Misc>();
-    k_bmeta<<<(unsigned)((K + 255) / 256), 256, 0, plan->stream>>>(
-        B, cl, plan->bmeta.as<int4>(), plan->bdcount.as<int32_t>(), &misc->err);
+    {
+        KTime kt(plan->stream, plan->capturing, KF_ANALYSIS);
+        k_bmeta<<<(unsigned)((K + 255) / 256), 256, 0, plan->stream>>>(
+            B, cl, plan->bmeta.as<int4>(), plan->bdcount.as<int32_t>(), &misc->err);
+    }
     note_launch(plan, 1);
     int st = scan_counts(plan, plan->bdcount.as<int32_t>(), K, plan->bdscan.as<int64_t>(), nullptr,
                          &misc->dir_total);
@@ -453,6 +523,7 @@ int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
     plan->dir_ok = total > 0 && total <= (int64_t(1) << 28) &&
                    plan->bdir.ensure((size_t)total * 4) == cudaSuccess;
     cudaGetLastError();  // a refused directory allocation only costs the searches
+    KTime kt(plan->stream, plan->capturing, KF_ANALYSIS);
     if (plan->dir_ok) {
         k_bdir<<<(unsigned)((K * 32 + 255) / 256), 256, 0, plan->stream>>>(
             B, cl, plan->bmeta.as<int4>(), plan->bdcount.as<int32_t>(),
@@ -489,9 +560,11 @@ void launch_bin_scatter(rvsp_cuda_plan* plan, const uint8_t* bin, const int32_t*
                         int32_t* bin_rows, bool heavy_items) {
     const int64_t M = plan->a_rows;
     Misc* misc = plan->misc.as<Misc>();
+    KTime kt(plan->stream, plan->capturing, KF_ANALYSIS);
     k_bin_scatter<<<(unsigned)((M + AN_TILE - 1) / AN_TILE), AN_TILE, 0, plan->stream>>>(
         (int32_t)M, bin, tile_off, plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
-        bin_rows, &misc->item_cursor, heavy_items ? plan->items.as<HeavyItem>() : nullptr);
+        bin_rows, &misc->item_cursor, heavy_items ? plan->items.as<HeavyItem>() : nullptr,
+        heavy_group(plan->params.heavy_cw_log2));
     note_launch(plan, 1);
 }
 
@@ -635,6 +708,37 @@ void rvsp_cuda_free(void* p) {
 
 int64_t rvsp_cuda_launch_count(void) { return (int64_t)g_launches.load(); }
 
+int rvsp_cuda_kernel_timing(int on) {
+    std::lock_guard<std::mutex> lk(g_ktime_mu);
+    ktime_drain_locked();
+    for (int i = 0; i < KF_NUM; ++i) {
+        g_ktime_ms[i] = 0.0;
+        g_ktime_n[i] = 0;
+    }
+    g_ktime_on.store(on != 0);
+    return RVSP_SUCCESS;
+}
+
+int rvsp_cuda_kernel_times(double* ms_out, int64_t* launches_out, int32_t n) {
+    if (!ms_out) return RVSP_ERROR_NULL_POINTER;
+    if (n < KF_NUM) return RVSP_ERROR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(g_ktime_mu);
+    ktime_drain_locked();
+    for (int i = 0; i < KF_NUM; ++i) {
+        ms_out[i] = g_ktime_ms[i];
+        if (launches_out) launches_out[i] = g_ktime_n[i];
+    }
+    return RVSP_SUCCESS;
+}
+
+const char* rvsp_cuda_kernel_family(int32_t i) {
+    static const char* names[KF_NUM] = {
+        "k_tiny<COUNT>", "k_tiny<FILL>", "k_tiny_reuse", "k_warp<COUNT>", "k_warp<FILL>",
+        "k_warp_reuse", "k_heavy<COUNT>", "k_heavy<FILL>", "k_heavy<REUSE>", "analysis",
+        "scan", "learned_sizing", "k_compact"};
+    return i >= 0 && i < KF_NUM ? names[i] : nullptr;
+}
+
 int rvsp_cuda_plan_create(rvsp_cuda_plan_t* out, int algo) {
     if (!out) return RVSP_ERROR_NULL_POINTER;
     *out = nullptr;
@@ -672,7 +776,7 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
                       &p->pred_cap, &p->slot_off, &p->tmp_ci, &p->tmp_v, &p->row_flag,
                       &p->tile_hist, &p->tile_off, &p->pm8, &p->pm16, &p->list_ops,
                       &p->list_off, &p->lbin, &p->lcap, &p->ltile_hist, &p->ltile_off,
-                      &p->lbin_rows, &p->need, &p->pflag, &p->bmeta, &p->bdcount,
+                      &p->lbin_rows, &p->need, &p->pflag, &p->hmask, &p->hovf, &p->item_off, &p->bmeta, &p->bdcount,
                       &p->bdscan, &p->bdoff, &p->bdir, &p->ameta, &p->adoff};
     for (DevBuf* b : bufs) b->release();
     if (p->side) {
@@ -1088,7 +1192,42 @@ static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
-NoAllocScratch* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+// the scratch array's device address per device, and the context it was
+// resolved in (a cudaDeviceReset makes a new context, in which the module,
+// and with it the array, may load at another address)
+struct NoAllocAddr {
+    unsigned long long ctx_id;
+    NoAllocScratch* addr;
+};
+NoAllocAddr g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+
+// Unique id of the calling thread's current CUDA context (cuCtxGetId: never
+// reused within the process), or 0 when the driver cannot tell, in which case
+// the caller resolves the address again.
+unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return 0;
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
 
 }  // namespace
 
@@ -1115,17 +1254,23 @@ int rvsp_cuda_row_ptr_noalloc(const int32_t* counts, int32_t n, int32_t* row_ptr
     }
     NoAllocScratch* scratch = nullptr;
     {
-        // once per device, with that device current: the host-side name of a
-        // __device__ array is not a device address, so resolve it here
+        // once per device (and context), with that device current: the
+        // host-side name of a __device__ array is not a device address, so
+        // resolve it here
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
+        NoAllocAddr& slot = g_noalloc_addr[dev];
+        const unsigned long long ctx = current_context_id();
+        if (!slot.addr || ctx == 0 || slot.ctx_id != ctx) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess)
+            if (e != cudaSuccess) {
+                slot.addr = nullptr;
                 return fail(e, "rvsp_cuda_row_ptr_noalloc: cudaGetSymbolAddress");
-            g_noalloc_addr[dev] = static_cast<NoAllocScratch*>(p);
+            }
+            slot.addr = static_cast<NoAllocScratch*>(p);
+            slot.ctx_id = current_context_id();
         }
-        scratch = g_noalloc_addr[dev];
+        scratch = slot.addr;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int64_t ntiles = ((int64_t)n + SCAN_TILE - 1) / SCAN_TILE;

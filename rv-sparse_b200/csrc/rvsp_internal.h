@@ -61,7 +61,7 @@ struct RowOut {
     float* c_v;
     int32_t* err;
     bool maps;           // FILL: record position maps; REUSE: replay them
-    RowCtl ctl = {nullptr, nullptr, 0};
+    RowCtl ctl = {nullptr, nullptr, 0, nullptr, nullptr};
     bool learned_bins = false;  // iterate the predicted-capacity bins instead
     // REUSE, every row a tiny row: the map-replay kernel also writes the
     // caller's row pointer (the copy of the analysed one is skipped)
@@ -85,6 +85,30 @@ inline void trace_point(const char* what) {
     last = now;
 }
 bool is_dev(const void* p);
+
+// Opt-in device timing of the kernels by family (rvsp_cuda_kernel_timing):
+// a KTime scope records a CUDA event pair around the launches it covers on
+// the plan's stream (none while the plan records a graph); the pairs are
+// read when the totals are queried.
+enum KernelFamily : int {
+    KF_TINY_COUNT = 0, KF_TINY_FILL, KF_TINY_REUSE,
+    KF_WARP_COUNT, KF_WARP_FILL, KF_WARP_REUSE,
+    KF_HEAVY_COUNT, KF_HEAVY_FILL, KF_HEAVY_REUSE,
+    KF_ANALYSIS,  // row analysis, binning, heavy-row lookups
+    KF_SCAN,      // prefix sums
+    KF_LEARNED,   // inference, predicted bins, re-run masks
+    KF_COMPACT,   // slot -> C copies of the learned path
+    KF_NUM
+};
+bool ktime_enabled();
+struct KTime {
+    cudaEvent_t e0 = nullptr;
+    cudaStream_t st = nullptr;
+    int fam = 0;
+    KTime(cudaStream_t stream, bool capturing, int family);
+    ~KTime();
+};
+
 void init_kernel_attributes();
 BinParams default_params();  // the process-wide default of new and internal plans
 void keep_pool_memory();     // the device pool keeps freed blocks (one-shot entry points)
@@ -153,6 +177,10 @@ struct rvsp_cuda_plan {
     int64_t slot_total = 0;
     int64_t lstats[8] = {};   // see rvsp_cuda_plan_learned_stats
     rvsp::DevBuf pred_cap, slot_off, tmp_ci, tmp_v, row_flag;
+    // heavy rows of the learned sweep: rows kept heavy (hmask), rows whose
+    // slot overflowed (hovf), each chunk's offset in its row's slot (item_off)
+    rvsp::DevBuf hmask, hovf, item_off;
+    bool heavy_slots = false;  // the last learned analysis sized heavy rows by prediction
 
     // numeric-only CUDA graph
     cudaGraphExec_t gexec = nullptr;

@@ -11,8 +11,9 @@
 //                  (row, column-chunk) work items
 //   k_tiny<MODE>   thread per row, rows with <= 32 products
 //   k_warp<CAP,..> warp per row, shared-memory hash table of CAP slots
-//   k_heavy<..>    warp per (row, column chunk), dense shared-memory
-//                  accumulator + occupancy bitmap over CW columns
+//   k_heavy<..>    CTA per (row, group of column chunks), a warp per chunk:
+//                  dense shared-memory accumulator + occupancy bitmap over
+//                  CW columns, B-row lookups shared by the group
 //   k_scan_*       exclusive scan of row counts into C's row pointer
 //
 // Each row kernel runs in one of three modes:
@@ -177,7 +178,7 @@ __device__ __forceinline__ void warp_bin_add(int key, int nkeys, unsigned long l
 constexpr int AN_SHORT = 32;
 
 __global__ void __launch_bounds__(AN_TILE)
-    k_analyze(CsrView A, CsrView B, AnalyzeOut out, BinParams P) {
+    k_analyze(CsrView A, CsrView B, AnalyzeOut out, BinParams P, int heavy_group) {
     __shared__ int32_t s_rp[AN_TILE + 1];
     __shared__ unsigned long long s_ops[AN_TILE];
     __shared__ int32_t s_maxlen[AN_TILE];
@@ -288,7 +289,9 @@ __global__ void __launch_bounds__(AN_TILE)
     }
     warp_bin_add(b, NUM_BINS, (unsigned long long)ops, s_hist, s_bprod);
     const unsigned long long wprod = warp_sum64((unsigned long long)ops);
-    const unsigned long long witems = warp_sum64((unsigned long long)nch);
+    // a heavy row's items are padded to whole groups of the heavy kernel
+    const int nitems = (nch + heavy_group - 1) / heavy_group * heavy_group;
+    const unsigned long long witems = warp_sum64((unsigned long long)nitems);
     if (lane_id() == 0) {
         if (wprod) atomicAdd(&s_prod, wprod);
         if (witems) atomicAdd(&s_items, witems);
@@ -313,7 +316,8 @@ __global__ void __launch_bounds__(AN_TILE)
     k_bin_scatter(int32_t rows, const uint8_t* __restrict__ bin,
                   const int32_t* __restrict__ tile_off, const int32_t* __restrict__ chunk_lo,
                   const int32_t* __restrict__ nchunks, int32_t* __restrict__ bin_rows,
-                  int32_t* __restrict__ item_cursor, HeavyItem* __restrict__ items) {
+                  int32_t* __restrict__ item_cursor, HeavyItem* __restrict__ items,
+                  int heavy_group) {
     __shared__ int32_t s_wc[AN_TILE / 32][NUM_BINS];
     const int t = threadIdx.x, lane = lane_id(), warp = t >> 5;
     const int row = blockIdx.x * AN_TILE + t;
@@ -330,10 +334,14 @@ __global__ void __launch_bounds__(AN_TILE)
                     __popc(peers & ((1u << lane) - 1));
     bin_rows[pos] = row;
     if (b == BIN_HEAVY && items) {
+        // whole groups of heavy_group items (the cursor stays a multiple of
+        // it), the padding items marked by chunk -1
         const int n = nchunks[row];
-        const int first = atomicAdd(item_cursor, n);
+        const int padded = (n + heavy_group - 1) / heavy_group * heavy_group;
+        const int first = atomicAdd(item_cursor, padded);
         const int lo = chunk_lo[row];
-        for (int c = 0; c < n; ++c) items[first + c] = HeavyItem{row, lo + c, first, 0};
+        for (int c = 0; c < padded; ++c)
+            items[first + c] = HeavyItem{row, c < n ? lo + c : -1, first, 0};
     }
 }
 
@@ -1331,20 +1339,135 @@ __global__ void k_ameta(CsrView A, CsrView B, const int32_t* __restrict__ rows, 
     }
 }
 
-constexpr int HEAVY_MAX_WARPS = 32;
+// Accumulates, for the calling warp, the in-chunk B segments of 32 A entries
+// (lane l: positions [s, s + len) of its entry's B row, A value av) into the
+// chunk [lo, lo + cw) in A-row order. A run of short segments is walked
+// flattened (products spread over the lanes, two steps of 32 in flight,
+// same-column products of a step combined in lane order by ordered_add); a
+// segment of HEAVY_SEG or more products is walked with the lanes over its own
+// columns, which are distinct, so it needs neither the product search nor
+// the ordered combine. COUNT and FILL set bits of the presence bitmap; FILL
+// and REUSE add into the accumulator.
+template <int MODE>
+__device__ __forceinline__ void heavy_segments(const CsrView& B, int s, int len, float av, int lo,
+                                               int cw, float* acc, unsigned* bits,
+                                               int32_t* err) {
+    const int lane = lane_id();
+    const int incl = warp_incl_scan(len);
+    const unsigned longm = __ballot_sync(FULL, len >= HEAVY_SEG);
+    int e = 0;
+    while (e < 32) {
+        const unsigned rest = (longm >> e) << e;
+        const int nl = rest ? __ffs(rest) - 1 : 32;
+        if (nl > e) {
+            const int pstart = e > 0 ? __shfl_sync(FULL, incl, (e - 1) & 31) : 0;
+            const int pend = __shfl_sync(FULL, incl, nl - 1);
+            for (int f0 = pstart; f0 < pend; f0 += 64) {
+                // two steps located and loaded before either is accumulated
+                const int p0 = f0 + lane, p1 = f0 + 32 + lane;
+                const ProductRef r0 = locate_product(p0, incl, len, s, av);
+                const ProductRef r1 = locate_product(p1, incl, len, s, av);
+                int c0 = 0, c1 = 0;
+                float b0 = 0.0f, b1 = 0.0f;
+                if (p0 < pend) {
+                    c0 = __ldg(B.ci + r0.q) - lo;
+                    if (MODE != COUNT) b0 = __ldg(B.v + r0.q);
+                }
+                if (p1 < pend) {
+                    c1 = __ldg(B.ci + r1.q) - lo;
+                    if (MODE != COUNT) b1 = __ldg(B.v + r1.q);
+                }
+                const bool ok0 = p0 < pend && (unsigned)c0 < (unsigned)cw;
+                const bool ok1 = p1 < pend && (unsigned)c1 < (unsigned)cw;
+                if ((p0 < pend && !ok0) || (p1 < pend && !ok1))
+                    atomicOr(err, ERR_STRUCTURE);  // B row not sorted
+                if (MODE != REUSE) {
+                    if (ok0) atomicOr(&bits[c0 >> 5], 1u << (c0 & 31));
+                    if (ok1) atomicOr(&bits[c1 >> 5], 1u << (c1 & 31));
+                }
+                if (MODE != COUNT) {
+                    ordered_add(acc, ok0 ? c0 : 0, ok0, __fmul_rn(r0.a, b0));
+                    __syncwarp();
+                    if (f0 + 32 < pend) ordered_add(acc, ok1 ? c1 : 0, ok1, __fmul_rn(r1.a, b1));
+                }
+                __syncwarp();
+            }
+            e = nl;
+        }
+        if (e < 32) {
+            const int se = __shfl_sync(FULL, s, e);
+            const int qe = se + __shfl_sync(FULL, len, e);
+            const float ae = __shfl_sync(FULL, av, e);
+            for (int q0 = se; q0 < qe; q0 += 64) {
+                const int qa = q0 + lane, qb = q0 + 32 + lane;
+                const bool two = q0 + 32 < qe;  // warp-uniform
+                int ca = 0, cb = 0;
+                float va = 0.0f, vb = 0.0f;
+                if (qa < qe) {
+                    ca = __ldg(B.ci + qa) - lo;
+                    if (MODE != COUNT) va = __ldg(B.v + qa);
+                }
+                if (two && qb < qe) {
+                    cb = __ldg(B.ci + qb) - lo;
+                    if (MODE != COUNT) vb = __ldg(B.v + qb);
+                }
+                const bool oka = qa < qe && (unsigned)ca < (unsigned)cw;
+                const bool okb = two && qb < qe && (unsigned)cb < (unsigned)cw;
+                if ((qa < qe && !oka) || (two && qb < qe && !okb)) atomicOr(err, ERR_STRUCTURE);
+                if (MODE != REUSE) {
+                    if (oka) atomicOr(&bits[ca >> 5], 1u << (ca & 31));
+                    if (okb) atomicOr(&bits[cb >> 5], 1u << (cb & 31));
+                }
+                if (MODE != COUNT) {
+                    if (oka) acc[ca] = __fadd_rn(acc[ca], __fmul_rn(ae, va));
+                    if (okb) acc[cb] = __fadd_rn(acc[cb], __fmul_rn(ae, vb));
+                }
+            }
+            __syncwarp();
+            ++e;
+        }
+    }
+}
+
+// Heavy rows, grouped. The work items are (row, column chunk) pairs, each
+// row's items padded to a multiple of the group size G (padding items have
+// chunk -1), so G consecutive items never cross rows. One CTA of G warps
+// takes a group at a time from a counter; warp w owns the group's chunk w
+// (its accumulator and bitmap), so every column is still added by one warp
+// in A-row order. The A row is walked 32 * G entries at a time: first each
+// thread looks up one entry's B row once for the whole group and stages the
+// G + 1 positions where its B row crosses the group's chunk boundaries
+// (from the B row's chunk directory, a short scan of a short row, or a
+// binary search), then each warp walks its own chunk's segments from that
+// staging in shared memory. The expensive lookup is paid once per (A entry,
+// group) instead of once per (A entry, chunk).
+constexpr int HEAVY_GROUP_MAX = 8;
+
+// Shared memory of the staging: per entry of a batch (32 * G entries) its
+// G + 1 boundary positions and its A value.
+__host__ __device__ constexpr int heavy_stage_bytes(int g) {
+    return 32 * g * (g + 1) * 4 + 32 * g * 4;
+}
+__host__ __device__ constexpr int heavy_grp_smem_bytes(int mode, int cw, int g) {
+    return heavy_stage_bytes(g) + g * heavy_smem_bytes(mode, cw);
+}
 
 template <int MODE>
-__global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
-    k_heavy(CsrView A, CsrView B, const HeavyItem* __restrict__ items, int nitems,
+__global__ void __launch_bounds__(HEAVY_GROUP_MAX * 32)
+    k_heavy(CsrView A, CsrView B, const HeavyItem* __restrict__ items, int ngroups, int G,
             int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
             const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
             int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err,
             RowCtl ctl, int cw_log2, HeavyAux aux, int32_t* __restrict__ queue) {
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_group;
     const int cw = 1 << cw_log2;
     const int nw = cw >> 5;  // bitmap words
-    const int warp = threadIdx.x >> 5, lane = lane_id();
-    unsigned char* mine = smem + warp * heavy_smem_bytes(MODE, cw);
+    const int warp = threadIdx.x >> 5, lane = lane_id(), t = threadIdx.x;
+    const int E = 32 * G, SP = G + 1;
+    int32_t* split = reinterpret_cast<int32_t*>(smem);             // [E][G + 1]
+    float* s_av = reinterpret_cast<float*>(smem + 4 * E * SP);     // [E]
+    unsigned char* mine = smem + heavy_stage_bytes(G) + warp * heavy_smem_bytes(MODE, cw);
     float* acc = reinterpret_cast<float*>(mine);
     unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * cw));
 
@@ -1357,141 +1480,96 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
     }
     if (MODE != REUSE)
         for (int x = lane; x < nw; x += 32) bits[x] = 0u;
-    __syncwarp();
     for (;;) {
-        // items are pulled one at a time, so a warp that drew a light item
-        // takes the next one instead of idling beside a heavy one
-        int w = 0;
-        if (lane == 0) w = atomicAdd(queue, 1);
-        w = __shfl_sync(FULL, w, 0);
-        if (w >= nitems) break;
+        __syncthreads();  // the previous group's staging is no longer read
+        if (t == 0) s_group = atomicAdd(queue, 1);
+        __syncthreads();
+        const int gi = s_group;
+        if (gi >= ngroups) break;
+        const int i0 = gi * G;
+        const HeavyItem head = items[i0];
+        const int row = head.row;
+        if (head.chunk < 0 || (ctl.only && !ctl.only[row])) continue;  // CTA-uniform
+        const int w = i0 + warp;  // this warp's item
         const HeavyItem it = items[w];
-        const int row = it.row;
-        if (ctl.only && !ctl.only[row]) continue;
-        const int lo = it.chunk << cw_log2;
-        const int hi = (int)min((int64_t)lo + cw, (int64_t)B.cols);
-        if (MODE == REUSE) {
+        const bool active = it.chunk >= 0;  // warp-uniform
+        const int lo = active ? it.chunk << cw_log2 : 0;
+        if (MODE == REUSE && active) {
             float4* a4 = reinterpret_cast<float4*>(acc);
             for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
             __syncwarp();
         }
         int a0, a1;
         row_range(A, row, &a0, &a1, err);
-        for (int base = a0; base < a1; base += 32) {
-            const int j = base + lane;
-            int s = 0, len = 0;
-            float av = 0.0f;
-            if (j < a1) {
-                // {start, end, first column, last column} of B row A.ci[j],
-                // and its directory offset
+        for (int base = a0; base < a1; base += E) {
+            // stage: thread t looks up entry base + t for the whole group
+            {
+                const int j = base + t;
+                int32_t* sp = split + t * SP;
                 int4 m = make_int4(0, 0, 0, -1);
                 int64_t d = -1;
-                if (aux.ameta) {
-                    m = aux.ameta[j];
-                    if (aux.dir) d = aux.adoff[j];
-                } else {
-                    const int k = A.ci[j];
-                    if ((unsigned)k >= (unsigned)B.rows) {
-                        atomicOr(err, ERR_STRUCTURE);
+                float av = 0.0f;
+                if (j < a1) {
+                    if (aux.ameta) {
+                        m = aux.ameta[j];
+                        if (aux.dir) d = aux.adoff[j];
                     } else {
-                        m = aux.meta[k];
-                        if (aux.dir) d = aux.doff[k];
+                        const int k = A.ci[j];
+                        if ((unsigned)k >= (unsigned)B.rows) {
+                            atomicOr(err, ERR_STRUCTURE);
+                        } else {
+                            m = aux.meta[k];
+                            if (aux.dir) d = aux.doff[k];
+                        }
                     }
-                }
-                if (m.y > m.x && m.w >= lo && m.z < hi) {
-                    int t;
-                    if (d >= 0) {
-                        const int c = it.chunk - (m.z >> cw_log2);
-                        s = m.z >= lo ? m.x : aux.dir[d + c];
-                        t = m.w < hi ? m.y : aux.dir[d + c + 1];
-                        // only an unsorted row (a broken operand) leaves a
-                        // directory entry unwritten: stay inside the row
-                        s = min(max(s, m.x), m.y);
-                        t = min(max(t, s), m.y);
-                    } else {
-                        s = m.z >= lo ? m.x : seq_lower_bound(B.ci, m.x, m.y, lo);
-                        t = m.w < hi ? m.y : seq_lower_bound(B.ci, s, m.y, hi);
-                    }
-                    len = t - s;
                     if (MODE != COUNT) av = A.v[j];
                 }
-            }
-            const int incl = warp_incl_scan(len);
-            const unsigned longm = __ballot_sync(FULL, len >= HEAVY_SEG);
-            int e = 0;
-            while (e < 32) {
-                const unsigned rest = (longm >> e) << e;
-                const int nl = rest ? __ffs(rest) - 1 : 32;
-                if (nl > e) {
-                    const int pstart = e > 0 ? __shfl_sync(FULL, incl, (e - 1) & 31) : 0;
-                    const int pend = __shfl_sync(FULL, incl, nl - 1);
-                    for (int f0 = pstart; f0 < pend; f0 += 64) {
-                        // two steps located and loaded before either is accumulated
-                        const int p0 = f0 + lane, p1 = f0 + 32 + lane;
-                        const ProductRef r0 = locate_product(p0, incl, len, s, av);
-                        const ProductRef r1 = locate_product(p1, incl, len, s, av);
-                        int c0 = 0, c1 = 0;
-                        float b0 = 0.0f, b1 = 0.0f;
-                        if (p0 < pend) {
-                            c0 = __ldg(B.ci + r0.q) - lo;
-                            if (MODE != COUNT) b0 = __ldg(B.v + r0.q);
-                        }
-                        if (p1 < pend) {
-                            c1 = __ldg(B.ci + r1.q) - lo;
-                            if (MODE != COUNT) b1 = __ldg(B.v + r1.q);
-                        }
-                        const bool ok0 = p0 < pend && (unsigned)c0 < (unsigned)cw;
-                        const bool ok1 = p1 < pend && (unsigned)c1 < (unsigned)cw;
-                        if ((p0 < pend && !ok0) || (p1 < pend && !ok1))
-                            atomicOr(err, ERR_STRUCTURE);  // B row not sorted
-                        if (MODE != REUSE) {
-                            if (ok0) atomicOr(&bits[c0 >> 5], 1u << (c0 & 31));
-                            if (ok1) atomicOr(&bits[c1 >> 5], 1u << (c1 & 31));
-                        }
-                        if (MODE != COUNT) {
-                            ordered_add(acc, ok0 ? c0 : 0, ok0, __fmul_rn(r0.a, b0));
-                            __syncwarp();
-                            if (f0 + 32 < pend)
-                                ordered_add(acc, ok1 ? c1 : 0, ok1, __fmul_rn(r1.a, b1));
-                        }
-                        __syncwarp();
+                s_av[t] = av;
+                const int fc = m.z >> cw_log2;
+                int q = m.x;  // monotone cursor of the scan / search
+                for (int b = 0; b <= G; ++b) {
+                    const int64_t X = (int64_t)(head.chunk + b) << cw_log2;  // boundary column
+                    int pos;
+                    if (m.y <= m.x || X <= m.z) {
+                        pos = m.x;
+                    } else if (X > m.w) {
+                        pos = m.y;
+                    } else if (d >= 0) {
+                        // the chunk directory: first position at or past the
+                        // start of chunk head.chunk + b (inside the row's chunks)
+                        pos = aux.dir[d + (head.chunk + b - fc)];
+                        pos = min(max(pos, m.x), m.y);  // only a broken operand is outside
+                    } else if (m.y - m.x <= 32) {
+                        while (q < m.y && __ldg(B.ci + q) < X) ++q;
+                        pos = q;
+                    } else {
+                        q = seq_lower_bound(B.ci, q, m.y, (int)X);
+                        pos = q;
                     }
-                    e = nl;
-                }
-                if (e < 32) {
-                    const int se = __shfl_sync(FULL, s, e);
-                    const int qe = se + __shfl_sync(FULL, len, e);
-                    const float ae = __shfl_sync(FULL, av, e);
-                    for (int q0 = se; q0 < qe; q0 += 64) {
-                        const int qa = q0 + lane, qb = q0 + 32 + lane;
-                        const bool two = q0 + 32 < qe;  // warp-uniform
-                        int ca = 0, cb = 0;
-                        float va = 0.0f, vb = 0.0f;
-                        if (qa < qe) {
-                            ca = __ldg(B.ci + qa) - lo;
-                            if (MODE != COUNT) va = __ldg(B.v + qa);
-                        }
-                        if (two && qb < qe) {
-                            cb = __ldg(B.ci + qb) - lo;
-                            if (MODE != COUNT) vb = __ldg(B.v + qb);
-                        }
-                        const bool oka = qa < qe && (unsigned)ca < (unsigned)cw;
-                        const bool okb = two && qb < qe && (unsigned)cb < (unsigned)cw;
-                        if ((qa < qe && !oka) || (two && qb < qe && !okb))
-                            atomicOr(err, ERR_STRUCTURE);
-                        if (MODE != REUSE) {
-                            if (oka) atomicOr(&bits[ca >> 5], 1u << (ca & 31));
-                            if (okb) atomicOr(&bits[cb >> 5], 1u << (cb & 31));
-                        }
-                        if (MODE != COUNT) {
-                            if (oka) acc[ca] = __fadd_rn(acc[ca], __fmul_rn(ae, va));
-                            if (okb) acc[cb] = __fadd_rn(acc[cb], __fmul_rn(ae, vb));
-                        }
-                    }
-                    __syncwarp();
-                    ++e;
+                    sp[b] = pos;
                 }
             }
+            __syncthreads();
+            if (active) {
+                const int ne = min(E, a1 - base);
+                for (int sub = 0; sub < ne; sub += 32) {
+                    const int e = sub + lane;
+                    int s = 0, len = 0;
+                    float av = 0.0f;
+                    if (e < ne) {
+                        s = split[e * SP + warp];
+                        len = max(split[e * SP + warp + 1] - s, 0);
+                        av = s_av[e];
+                    }
+                    if (__any_sync(FULL, len > 0))
+                        heavy_segments<MODE>(B, s, len, av, lo, cw, acc, bits, err);
+                }
+            }
+            __syncthreads();
+        }
+        if (!active) {
+            if (MODE == COUNT && lane == 0) item_cnt[w] = 0;  // padding item
+            continue;
         }
         __syncwarp();
         if (MODE == COUNT) {
@@ -1509,7 +1587,32 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
         } else if (MODE == FILL) {
             // lane l writes the present columns of bitmap word x0 + l; the
             // words' popcounts give each lane its first output position
-            int64_t out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
+            int64_t out;
+            bool keep = true;
+            if (ctl.item_off) {
+                // learned sweep: the chunk takes the next place in its row's
+                // slot (c_ci / c_v are the slot buffers); a chunk that does
+                // not fit only clears its bitmap and accumulator
+                int c = 0;
+                for (int x = lane; x < nw; x += 32) c += __popc(bits[x]);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+                int off = 0;
+                if (lane == 0) {
+                    item_cnt[w] = c;
+                    off = atomicAdd(&row_cnt[row], c);
+                }
+                off = __shfl_sync(FULL, off, 0);
+                const int64_t s0 = ctl.slot_off[row], cap = ctl.slot_off[row + 1] - s0;
+                keep = (int64_t)off + c <= cap;
+                if (lane == 0) {
+                    ctl.item_off[w] = keep ? off : -1;
+                    if (!keep) ctl.ovf[row] = 1;
+                }
+                out = s0 + off;
+            } else {
+                out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
+            }
             for (int x0 = 0; x0 < nw; x0 += 32) {
                 unsigned word = 0u;
                 if (x0 + lane < nw) {
@@ -1523,18 +1626,21 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
                     const int b = __ffs(word) - 1;
                     word &= word - 1;
                     const int col = (x0 + lane) * 32 + b;
-                    c_ci[pos] = lo + col;
-                    c_v[pos] = acc[col];
+                    if (keep) {
+                        c_ci[pos] = lo + col;
+                        c_v[pos] = acc[col];
+                    }
                     acc[col] = 0.0f;
                     ++pos;
                 }
                 out += __shfl_sync(FULL, incl, 31);
             }
         } else {
+            const int hi = (int)min((int64_t)lo + cw, (int64_t)B.cols);
             const int r0 = c_rp[row], r1 = c_rp[row + 1];
             const int s = warp_lower_bound(c_ci, r0, r1, lo);
-            const int t = warp_lower_bound(c_ci, s, r1, hi);
-            for (int q = s + lane; q < t; q += 32) {
+            const int t2 = warp_lower_bound(c_ci, s, r1, hi);
+            for (int q = s + lane; q < t2; q += 32) {
                 const int col = c_ci[q] - lo;
                 c_v[q] = (unsigned)col < (unsigned)cw ? acc[col] : 0.0f;
             }

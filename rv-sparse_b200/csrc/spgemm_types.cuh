@@ -70,6 +70,8 @@ __host__ __device__ inline bool bin_params_valid(const BinParams& p) {
            p.heavy_cw_log2 >= HEAVY_CW_LOG2_MIN && p.heavy_cw_log2 <= HEAVY_CW_LOG2_MAX;
 }
 
+// Work item of the heavy kernel: a column chunk of a heavy row (chunk -1:
+// padding that completes the row's last group of chunks).
 struct HeavyItem {
     int32_t row;
     int32_t chunk;
@@ -106,10 +108,18 @@ struct BinOffsets {
 //   learned   tables are sized by a prediction: a row whose table fills up
 //             (or, with slot_off, whose count passes its slot) gets cnt[r] = -1
 //             and is left for the exact path instead of raising an error
+//   item_off  heavy FILL into slots: every chunk takes its place in the row's
+//             slot with an atomic add of its count to cnt[r] (so cnt[r] ends
+//             as the row's exact count and item_cnt holds every chunk's);
+//             item_off[w] is the chunk's offset in the slot, or -1 when the
+//             slot was full, in which case ovf[r] is set and the row is left
+//             for the exact fill
 struct RowCtl {
     const int64_t* slot_off;
     const uint8_t* only;
     int learned;
+    int32_t* item_off;
+    uint8_t* ovf;
 };
 
 // Table bin of a warp row holding up to ub distinct columns: the smallest

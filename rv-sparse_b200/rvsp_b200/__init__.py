@@ -120,6 +120,9 @@ _PROTOS = {
     "rvsp_cuda_csr_check": (C.c_int, [_I32, _I32, _I32, _VP, _VP, C.POINTER(_I32)]),
     "rvsp_cuda_csr_validate": (C.c_int, [_I32, _I32, _I32, _VP, _VP]),
     "rvsp_cuda_launch_count": (_I64, []),
+    "rvsp_cuda_kernel_timing": (C.c_int, [C.c_int]),
+    "rvsp_cuda_kernel_times": (C.c_int, [_VP, _VP, _I32]),
+    "rvsp_cuda_kernel_family": (C.c_char_p, [_I32]),
     "rvsp_cuda_learned_available": (C.c_int, []),
     "rvsp_cuda_mlp_load": (C.c_int, [C.c_char_p]),
     "rvsp_cuda_mlp_set": (C.c_int, [_VP, _I32]),
@@ -144,7 +147,7 @@ _PROTOS = {
     "rvsp_cuda_spgemm_batched_f32": (C.c_int, [C.c_int, _I32, _VP, _VP, _VP, _VP, _VP,
                                                _VP, _VP, _VP, _VP, _VP, _VP,
                                                C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
-                                               C.POINTER(_I64), _VP]),
+                                               C.POINTER(_I64), _VP, _VP]),
 }
 
 BIN_PARAMS = 4  # tiny_ops, slack_shift, warp_cap_max, heavy_cw_log2
@@ -188,6 +191,24 @@ def device_count() -> int:
 
 def launch_count() -> int:
     return lib().rvsp_cuda_launch_count()
+
+
+KERNEL_FAMILIES = 13
+
+
+def kernel_timing(on: bool) -> None:
+    """Start (resetting the totals) or stop per-family device timing."""
+    check(lib().rvsp_cuda_kernel_timing(1 if on else 0), "kernel_timing")
+
+
+def kernel_times() -> dict:
+    """{family: (total ms, launches)} of the timed launches so far."""
+    L = lib()
+    ms = np.zeros(KERNEL_FAMILIES, np.float64)
+    n = np.zeros(KERNEL_FAMILIES, np.int64)
+    check(L.rvsp_cuda_kernel_times(ms.ctypes.data, n.ctypes.data, KERNEL_FAMILIES), "kernel_times")
+    return {L.rvsp_cuda_kernel_family(i).decode(): (float(ms[i]), int(n[i]))
+            for i in range(KERNEL_FAMILIES)}
 
 
 def ptr(a) -> int | None:
@@ -421,9 +442,11 @@ def pack_params(d):
 
 def spgemm_batched(pairs_dev, algo=RVSP_CUDA_ALGO_EXACT):
     """Batched product of device operand pairs (objects with rows, cols, nnz,
-    row_ptr, col_idx, values as device tensors). Returns the library-owned
-    packed C device pointers (rp, ci, v), nnz and the row offsets; release the
-    pointers with free_device()."""
+    row_ptr, col_idx, values as device tensors). Returns the library-owned C
+    device pointers (rp, ci, v), the total nnz, the row offsets and the entry
+    offsets: product i's row pointer (from 0) starts at rp + row_offs[i] + i,
+    its entries at ci / v + c_offs[i]. Release the pointers with
+    free_device()."""
     L = lib()
     n = len(pairs_dev)
     i32 = lambda xs: np.ascontiguousarray(xs, np.int32)  # noqa: E731
@@ -439,12 +462,14 @@ def spgemm_batched(pairs_dev, algo=RVSP_CUDA_ALGO_EXACT):
     prp, pci, pv = C.c_void_p(), C.c_void_p(), C.c_void_p()
     nnz = C.c_int64()
     offs = np.zeros(n + 1, np.int64)
+    c_offs = np.zeros(n + 1, np.int64)
     st = L.rvsp_cuda_spgemm_batched_f32(algo, n, a_rows.ctypes.data, a_cols.ctypes.data,
                                         b_cols.ctypes.data, a_nnz.ctypes.data, b_nnz.ctypes.data,
                                         *[C.cast(x, C.c_void_p) for x in arrs], C.byref(prp),
-                                        C.byref(pci), C.byref(pv), C.byref(nnz), offs.ctypes.data)
+                                        C.byref(pci), C.byref(pv), C.byref(nnz), offs.ctypes.data,
+                                        c_offs.ctypes.data)
     check(st, "rvsp_cuda_spgemm_batched_f32")
-    return (prp.value, pci.value, pv.value), nnz.value, offs
+    return (prp.value, pci.value, pv.value), nnz.value, offs, c_offs
 
 
 _libc = None

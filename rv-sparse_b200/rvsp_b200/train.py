@@ -53,8 +53,12 @@ def corpus(seed: int, scale: float = 1.0):
             A = gen.poisson_rows(s(n), s(n), lam, rng)
             B = gen.poisson_rows(s(n), s(n), lam, rng)
             out.append((f"poisson_n{n}_l{lam:g}", A, B))
+    # power-law graphs up to 2^18 vertices: their heavy rows (a warp per
+    # column chunk) are sized by the prediction too
     for sc, (a, b, c) in ((12, (0.57, 0.19, 0.19)), (13, (0.45, 0.22, 0.22)),
-                          (14, (0.57, 0.19, 0.19)), (13, (0.65, 0.15, 0.15))):
+                          (14, (0.57, 0.19, 0.19)), (13, (0.65, 0.15, 0.15)),
+                          (16, (0.57, 0.19, 0.19)), (17, (0.57, 0.19, 0.19)),
+                          (18, (0.57, 0.19, 0.19)), (16, (0.45, 0.22, 0.22))):
         R = gen.rmat(scale=sc, edge_factor=16, a=a, b=b, c=c, seed=int(rng.integers(1 << 30)))
         out.append((f"rmat_s{sc}_a{a}", R, R))
     for bmax in (500, 4000):

@@ -1,7 +1,8 @@
-"""The benchmark's roofline arithmetic on CPU: the algorithmic bytes of the
-headline product (the per-unit byte formula of the hot path, every operand
-array read once and C written once) and the exact sizes of the Poisson 1024^2
-product it is quoted on."""
+"""The benchmark's host logic on CPU: the algorithmic bytes of a product
+(the per-unit byte formula of the hot path, every operand array read once and
+C written once) on the Poisson 1024^2 product, the heavy-row rule behind the
+roofline's byte count, the row sample of the CPU baselines, and the reference
+arm's JSON line on the R-MAT 2^20 headline product."""
 
 import importlib.util
 import os
@@ -66,4 +67,32 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
-    assert d["config"]["workload"].startswith("poisson2d_1024")
+    assert d["config"]["workload"] == "rmat_scale20_ef16_c_eq_a_times_a"
+    assert d["config"]["products"] == 20_936_185_642
+
+
+def test_heavy_row_rule_matches_the_bins():
+    """bench.heavy_rows restates the library's bin rule (spgemm_types.cuh
+    table_bin / bin_of) for the roofline's byte count: a row is heavy when it
+    has more products than the tiny bin and its table ub + (ub >> 2) passes
+    the 2048-slot warp table."""
+    bench = _bench()
+    ops = np.array([0, 32, 33, 1638, 1639, 2000, 10**9])
+    # ub = min(ops, cols); 1638 + 409 = 2047 fits, 1639 + 409 = 2048 fits,
+    # 2000 + 500 > 2048 does not
+    assert bench.heavy_rows(ops, 1 << 20).tolist() == [False, False, False, False, False,
+                                                       True, True]
+    assert bench.heavy_rows(ops, 1000).tolist() == [False] * 7
+
+
+def test_row_sample_is_a_csr_of_the_sampled_rows():
+    bench = _bench()
+    A = gen.rmat(scale=10, edge_factor=16, seed=0)
+    ops = gen.row_products(A, A)
+    S, Ps, rows = bench.row_sample(A, ops, 0.2, 5)
+    assert S.rows == rows.size and np.all(np.diff(rows) > 0)
+    for i, r in enumerate(rows[:50]):
+        a, b = A.row_ptr[r], A.row_ptr[r + 1]
+        assert np.array_equal(S.col_idx[S.row_ptr[i]:S.row_ptr[i + 1]], A.col_idx[a:b])
+        assert np.array_equal(S.values[S.row_ptr[i]:S.row_ptr[i + 1]], A.values[a:b])
+    assert Ps == int(ops[rows].sum())

@@ -418,17 +418,34 @@ def test_batched_products_match_oracle(gpu_lib, algo):
     pairs = gen.batched_uneven(count=24, lo=8, hi=4000, seed=13)
     pairs.append((gen.uniform_fixed(50, 3, 2, seed=1), gen.uniform_fixed(3, 9000, 3, seed=2)))
     dev_pairs = [(DevCSR(A), DevCSR(B)) for A, B in pairs]
-    (prp, pci, pv), nnz, offs = rv.spgemm_batched(dev_pairs, algo)
+    (prp, pci, pv), nnz, offs, coffs = rv.spgemm_batched(dev_pairs, algo)
     try:
-        crp = d2h(prp, int(offs[-1]) + 1, np.int32)
+        crp = d2h(prp, int(offs[-1]) + len(pairs), np.int32)
         cci = d2h(pci, nnz, np.int32)
         cv = d2h(pv, nnz, np.float32)
     finally:
         rv.free_device(prp, pci, pv)
-    assert offs[-1] == sum(A.rows for A, _ in pairs)
+    assert offs[-1] == sum(A.rows for A, _ in pairs) and coffs[-1] == nnz
     for i, (A, B) in enumerate(pairs):
-        r0, r1 = int(offs[i]), int(offs[i + 1])
+        r0 = int(offs[i]) + i
+        lrp = crp[r0:r0 + A.rows + 1]
+        e0, e1 = int(coffs[i]), int(coffs[i + 1])
         wrp, wci, wv = oracle.spgemm_f32(A, B)
-        assert np.array_equal(crp[r0:r1 + 1] - crp[r0], wrp), i
-        assert np.array_equal(cci[crp[r0]:crp[r1]], wci), i
-        assert np.array_equal(bits(cv[crp[r0]:crp[r1]]), bits(wv)), i
+        assert np.array_equal(lrp, wrp), i
+        assert e1 - e0 == lrp[-1], i
+        assert np.array_equal(cci[e0:e1], wci), i
+        assert np.array_equal(bits(cv[e0:e1]), bits(wv)), i
+
+
+def test_batched_rejects_a_row_panel(gpu_lib):
+    """Batched operands are whole matrices: an A whose row pointer does not
+    start at 0 is refused instead of being packed with wrong offsets."""
+    A = gen.uniform_fixed(40, 40, 4, seed=2)
+    dA = DevCSR(A)
+    panel = DevCSR(A)
+    panel.rows = 20
+    panel.row_ptr = dA.row_ptr[10:31]
+    panel.nnz = int(A.row_ptr[30] - A.row_ptr[10])
+    with pytest.raises(rv.RvspError) as e:
+        rv.spgemm_batched([(dA, dA), (panel, dA)], rv.RVSP_CUDA_ALGO_EXACT)
+    assert e.value.status == rv.RVSP_ERROR_INVALID_CSR
