@@ -438,7 +438,7 @@ def run_headline(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
                      "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4) if achieved else None,
-                     "traffic": None, "traffic_source": "not measured in this run",
+                     **committed_traffic(fam, bytes_heavy),
                      "peak_source": f"{peak_kind} hbm_gbs", "kernel": fam,
                      "bytes_per_launch": int(bytes_heavy), "launch_ms": round(fam_launch_ms, 3),
                      "whole_product_frac_learned": round(
@@ -458,6 +458,21 @@ def run_headline(args):
     ranks.barrier(dist)
     if dist:
         dist.destroy_process_group()
+
+
+def committed_traffic(kernel, bytes_per_launch):
+    """DRAM traffic of the dominant kernel from the committed ncu summary
+    (profiles/traffic.json: read + write bytes of one captured launch per
+    algorithmic byte of that launch, scaled here to this launch's algorithmic
+    bytes), labelled as such; None when no capture covers the kernel."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        ratio = json.load(open(path))["rmat"][kernel]["dram_bytes_per_algorithmic_byte"]
+    except Exception:
+        return {"traffic": None, "traffic_source": "no ncu capture of this kernel committed"}
+    return {"traffic": int(ratio * bytes_per_launch),
+            "traffic_source": "committed ncu figure (profiles/traffic.json), DRAM bytes per "
+                              "algorithmic byte of a captured launch scaled to this launch"}
 
 
 def run_rmat_e2e(rv, A, ops, panels, args, torch):

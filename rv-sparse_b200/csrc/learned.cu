@@ -258,13 +258,14 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// Copy the chunks of heavy rows finished in their slots into C: one warp per
-// work item (grid-stride), the chunk's entries from its slot offset to its
-// place in C (its row's start plus the counts of the row's earlier chunks).
+// Copy the chunks of heavy rows finished in their slots (or the overflow
+// pool) into C: one warp per work item (grid-stride), the chunk's entries from
+// where the sweep put them to their place in C (its row's start plus the
+// counts of the row's earlier chunks).
 __global__ void __launch_bounds__(256)
     k_compact_items(const HeavyItem* __restrict__ items, int32_t n,
                     const uint8_t* __restrict__ hmask, const uint8_t* __restrict__ need,
-                    const int32_t* __restrict__ item_cnt, const int32_t* __restrict__ item_off,
+                    const int32_t* __restrict__ item_cnt, const int64_t* __restrict__ item_off,
                     const int64_t* __restrict__ item_scan, const int64_t* __restrict__ slot_off,
                     const int32_t* __restrict__ c_rp, const int32_t* __restrict__ tmp_ci,
                     const float* __restrict__ tmp_v, int32_t* __restrict__ c_ci,
@@ -275,7 +276,7 @@ __global__ void __launch_bounds__(256)
         const HeavyItem it = items[w];
         if (it.chunk < 0 || !hmask[it.row] || need[it.row]) continue;
         const int k = item_cnt[w];
-        const int64_t src = slot_off[it.row] + item_off[w];
+        const int64_t src = item_off[w];
         const int64_t dst = (int64_t)c_rp[it.row] + (item_scan[w] - item_scan[it.first]);
         for (int x = lane; x < k; x += 32) {
             c_ci[dst + x] = tmp_ci[src + x];
@@ -354,19 +355,23 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
     cudaError_t e;
     size_t free_b = SIZE_MAX, total_b = 0;
     // slots past 1 GiB must fit in half the free memory
-    if (fused && (size_t)plan->slot_total * 8 > (1ull << 30) &&
+    if (fused && (size_t)plan->slot_total * 10 > (1ull << 30) &&
         (e = cudaMemGetInfo(&free_b, &total_b)) != cudaSuccess)
         return fail(e, "mem info");
+    // heavy rows' chunks that outgrow their predicted slot share an overflow
+    // pool of a quarter of the slots, after them in the same buffers
+    plan->pool_cap = fused && plan->n_items > 0 ? plan->slot_total / 4 : 0;
+    const int64_t tmp_total = plan->slot_total + plan->pool_cap;
     if (fused) {
-        if ((size_t)plan->slot_total * 8 > free_b / 2) {
+        if ((size_t)tmp_total * 8 > free_b / 2) {
             g_err = "predicted capacity exceeds the memory budget";
             return RVSP_ERROR_ALLOCATION_FAILED;
         }
         if ((e = plan->slot_off.ensure(((size_t)M + 1) * 8)) != cudaSuccess)
             return fail(e, "slots");
-        if ((e = plan->tmp_ci.ensure((size_t)plan->slot_total * 4)) != cudaSuccess)
+        if ((e = plan->tmp_ci.ensure((size_t)tmp_total * 4)) != cudaSuccess)
             return fail(e, "slots");
-        if ((e = plan->tmp_v.ensure((size_t)plan->slot_total * 4)) != cudaSuccess)
+        if ((e = plan->tmp_v.ensure((size_t)tmp_total * 4)) != cudaSuccess)
             return fail(e, "slots");
     }
     launch_bin_scatter(plan, plan->lbin.as<uint8_t>(), plan->ltile_off.as<int32_t>(),
@@ -381,7 +386,7 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
             cudaSuccess)
         return fail(e, "memset");
     const bool hslots = fused && plan->n_items > 0;
-    if (hslots && ((e = plan->item_off.ensure((size_t)plan->n_items * 4)) != cudaSuccess ||
+    if (hslots && ((e = plan->item_off.ensure((size_t)plan->n_items * 8)) != cudaSuccess ||
                    (e = cudaMemsetAsync(plan->hovf.p, 0, M, plan->stream)) != cudaSuccess))
         return fail(e, "heavy slots");
     // one sweep over the predicted-capacity bins
@@ -390,8 +395,11 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
     fo.ctl.slot_off = fused ? plan->slot_off.as<int64_t>() : nullptr;
     fo.ctl.learned = 1;
     if (hslots) {
-        fo.ctl.item_off = plan->item_off.as<int32_t>();
+        fo.ctl.item_off = plan->item_off.as<int64_t>();
         fo.ctl.ovf = plan->hovf.as<uint8_t>();
+        fo.ctl.pool_fill = &misc->pool_fill;  // zeroed with the rest of Misc by the analysis
+        fo.ctl.pool_base = plan->slot_total;
+        fo.ctl.pool_cap = plan->pool_cap;
     }
     fo.learned_bins = true;
     run_rows(plan, fused ? FILL : COUNT, A, B, fo);
@@ -479,7 +487,7 @@ int learned_finish(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, int
         const int64_t grid = std::min<int64_t>(((int64_t)plan->n_items + 7) / 8, 148 * 64);
         k_compact_items<<<(unsigned)grid, 256, 0, plan->stream>>>(
             plan->items.as<HeavyItem>(), plan->n_items, plan->hmask.as<uint8_t>(),
-            plan->need.as<uint8_t>(), plan->item_cnt.as<int32_t>(), plan->item_off.as<int32_t>(),
+            plan->need.as<uint8_t>(), plan->item_cnt.as<int32_t>(), plan->item_off.as<int64_t>(),
             plan->item_scan.as<int64_t>(), plan->slot_off.as<int64_t>(), plan->c_rp.as<int32_t>(),
             plan->tmp_ci.as<int32_t>(), plan->tmp_v.as<float>(), c_ci, c_v);
         note_launch(plan, 1);

@@ -776,8 +776,9 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
                       &p->pred_cap, &p->slot_off, &p->tmp_ci, &p->tmp_v, &p->row_flag,
                       &p->tile_hist, &p->tile_off, &p->pm8, &p->pm16, &p->list_ops,
                       &p->list_off, &p->lbin, &p->lcap, &p->ltile_hist, &p->ltile_off,
-                      &p->lbin_rows, &p->need, &p->pflag, &p->hmask, &p->hovf, &p->item_off, &p->bmeta, &p->bdcount,
-                      &p->bdscan, &p->bdoff, &p->bdir, &p->ameta, &p->adoff};
+                      &p->lbin_rows, &p->need, &p->pflag, &p->hmask, &p->hovf,
+                      &p->item_off, &p->bmeta, &p->bdcount, &p->bdscan, &p->bdoff, &p->bdir,
+                      &p->ameta, &p->adoff};
     for (DevBuf* b : bufs) b->release();
     if (p->side) {
         cudaStreamSynchronize(p->side);

@@ -51,6 +51,7 @@ struct Misc {
     int64_t dir_total;         // heavy-row B directory entries
     int32_t heavy_queue;       // next heavy work item of the running launch
     int32_t row_queue;         // next row of the running warp-bin launch
+    unsigned long long pool_fill;  // learned path: entries placed in the overflow pool
 };
 
 // Output pointers of a row-kernel launch.
@@ -61,7 +62,7 @@ struct RowOut {
     float* c_v;
     int32_t* err;
     bool maps;           // FILL: record position maps; REUSE: replay them
-    RowCtl ctl = {nullptr, nullptr, 0, nullptr, nullptr};
+    RowCtl ctl = {nullptr, nullptr, 0, nullptr, nullptr, nullptr, 0, 0};
     bool learned_bins = false;  // iterate the predicted-capacity bins instead
     // REUSE, every row a tiny row: the map-replay kernel also writes the
     // caller's row pointer (the copy of the analysed one is skipped)
@@ -178,8 +179,10 @@ struct rvsp_cuda_plan {
     int64_t lstats[8] = {};   // see rvsp_cuda_plan_learned_stats
     rvsp::DevBuf pred_cap, slot_off, tmp_ci, tmp_v, row_flag;
     // heavy rows of the learned sweep: rows kept heavy (hmask), rows whose
-    // slot overflowed (hovf), each chunk's offset in its row's slot (item_off)
+    // chunks found no room (hovf), where each chunk went in the slot buffer
+    // (item_off), the size of the shared overflow pool after the slots
     rvsp::DevBuf hmask, hovf, item_off;
+    int64_t pool_cap = 0;
     bool heavy_slots = false;  // the last learned analysis sized heavy rows by prediction
 
     // numeric-only CUDA graph

@@ -1591,25 +1591,33 @@ __global__ void __launch_bounds__(HEAVY_GROUP_MAX * 32)
             bool keep = true;
             if (ctl.item_off) {
                 // learned sweep: the chunk takes the next place in its row's
-                // slot (c_ci / c_v are the slot buffers); a chunk that does
-                // not fit only clears its bitmap and accumulator
+                // slot (c_ci / c_v are the slot buffers), else in the shared
+                // overflow pool; a chunk that finds no room only clears its
+                // bitmap and accumulator
                 int c = 0;
                 for (int x = lane; x < nw; x += 32) c += __popc(bits[x]);
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
-                int off = 0;
+                long long dst = -1;
                 if (lane == 0) {
                     item_cnt[w] = c;
-                    off = atomicAdd(&row_cnt[row], c);
+                    const int off = atomicAdd(&row_cnt[row], c);
+                    const int64_t s0 = ctl.slot_off[row], cap = ctl.slot_off[row + 1] - s0;
+                    if ((int64_t)off + c <= cap) {
+                        dst = s0 + off;
+                    } else if (c > 0) {
+                        const unsigned long long p =
+                            atomicAdd(ctl.pool_fill, (unsigned long long)c);
+                        if ((int64_t)p + c <= ctl.pool_cap) dst = ctl.pool_base + (int64_t)p;
+                    } else {
+                        dst = s0;  // an empty chunk needs no room
+                    }
+                    ctl.item_off[w] = dst;
+                    if (dst < 0) ctl.ovf[row] = 1;
                 }
-                off = __shfl_sync(FULL, off, 0);
-                const int64_t s0 = ctl.slot_off[row], cap = ctl.slot_off[row + 1] - s0;
-                keep = (int64_t)off + c <= cap;
-                if (lane == 0) {
-                    ctl.item_off[w] = keep ? off : -1;
-                    if (!keep) ctl.ovf[row] = 1;
-                }
-                out = s0 + off;
+                dst = __shfl_sync(FULL, dst, 0);
+                keep = dst >= 0;
+                out = dst;
             } else {
                 out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
             }

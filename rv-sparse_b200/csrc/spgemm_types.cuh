@@ -110,16 +110,21 @@ struct BinOffsets {
 //             and is left for the exact path instead of raising an error
 //   item_off  heavy FILL into slots: every chunk takes its place in the row's
 //             slot with an atomic add of its count to cnt[r] (so cnt[r] ends
-//             as the row's exact count and item_cnt holds every chunk's);
-//             item_off[w] is the chunk's offset in the slot, or -1 when the
-//             slot was full, in which case ovf[r] is set and the row is left
-//             for the exact fill
+//             as the row's exact count and item_cnt holds every chunk's); a
+//             chunk past the slot's end takes a place in the shared overflow
+//             pool [pool_base, pool_base + pool_cap) of the same buffer
+//             (*pool_fill counts its use); item_off[w] is where the chunk
+//             went, or -1 when the pool was full too, in which case ovf[r] is
+//             set and the row is left for the exact fill
 struct RowCtl {
     const int64_t* slot_off;
     const uint8_t* only;
     int learned;
-    int32_t* item_off;
+    int64_t* item_off;
     uint8_t* ovf;
+    unsigned long long* pool_fill;
+    int64_t pool_base;
+    int64_t pool_cap;
 };
 
 // Table bin of a warp row holding up to ub distinct columns: the smallest
