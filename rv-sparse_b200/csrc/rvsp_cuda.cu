@@ -151,7 +151,8 @@ constexpr int map_warps() {
     return w > 8 ? 8 : (w < 1 ? 1 : w);
 }
 
-constexpr int HEAVY_SMEM_MAX = 227 * 1024;  // largest dynamic shared memory of one CTA
+constexpr int HEAVY_SMEM_MAX = 227 * 1024;  // largest shared memory of one CTA
+constexpr int HEAVY_SMEM_STATIC = 1024;     // room kept for k_heavy's static shared memory
 
 // resident CTAs per SM of every warp-bin kernel (launches fill the GPU once
 // and the warps pull rows from a counter)
@@ -183,8 +184,12 @@ static void set_mode_attrs() {
     set_warp_attr<1024, MODE>();
     set_warp_attr<2048, MODE>();
     set_warp_attr<4096, MODE>();
-    cudaFuncSetAttribute(k_heavy<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         HEAVY_SMEM_MAX);
+    // the heavy kernel's own static shared memory comes out of the same
+    // 227 KB: its dynamic part may use all but HEAVY_SMEM_STATIC of it
+    if (cudaFuncSetAttribute(k_heavy<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             HEAVY_SMEM_MAX - HEAVY_SMEM_STATIC) != cudaSuccess)
+        fprintf(stderr, "rvsp: k_heavy shared-memory attribute not set: %s\n",
+                cudaGetErrorString(cudaGetLastError()));
 }
 
 // Heavy kernel shape for every chunk width: chunks (warps) per CTA, the
@@ -195,8 +200,8 @@ static void set_mode_attrs() {
 // groups from a counter.
 int heavy_group(int cw_log2) {
     int g = HEAVY_GROUP_MAX;
-    // (1 KB left for the kernel's static shared memory)
-    while (g > 1 && heavy_grp_smem_bytes(FILL, 1 << cw_log2, g) > HEAVY_SMEM_MAX - 1024) --g;
+    while (g > 1 && heavy_grp_smem_bytes(FILL, 1 << cw_log2, g) > HEAVY_SMEM_MAX - HEAVY_SMEM_STATIC)
+        --g;
     return g;
 }
 static int g_heavy_ctas[3][HEAVY_CW_LOG2_MAX + 1];
