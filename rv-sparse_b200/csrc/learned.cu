@@ -83,9 +83,12 @@ __global__ void __launch_bounds__(AN_TILE)
             // the prediction is used only where it buys a smaller table than
             // the upper bound would; otherwise the row gets the bound's table
             // and a slot of ub entries, which cannot overflow
+            // With heavy slots (out.hmask) a heavy row stays heavy: the sweep
+            // counts it chunk by chunk, so it never needs the exact recount,
+            // which leaves heavy rows out.
             const int c = max(cap_pred[row], 1);
             const int pb = table_bin(c, P);  // table class of the prediction
-            if (pb < b) {
+            if (pb < b && !(b == BIN_HEAVY && out.hmask)) {
                 lb = pb;
                 cap = c;
                 predicted = 1;

@@ -1621,6 +1621,9 @@ __global__ void __launch_bounds__(HEAVY_GROUP_MAX * 32)
             } else {
                 out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
             }
+            // writes into C stay inside the row (counts that disagree with
+            // this fill would only come from an operand changed in between)
+            const int64_t lim = ctl.item_off ? INT64_MAX : (int64_t)c_rp[row + 1];
             for (int x0 = 0; x0 < nw; x0 += 32) {
                 unsigned word = 0u;
                 if (x0 + lane < nw) {
@@ -1634,9 +1637,11 @@ __global__ void __launch_bounds__(HEAVY_GROUP_MAX * 32)
                     const int b = __ffs(word) - 1;
                     word &= word - 1;
                     const int col = (x0 + lane) * 32 + b;
-                    if (keep) {
+                    if (keep && pos < lim) {
                         c_ci[pos] = lo + col;
                         c_v[pos] = acc[col];
+                    } else if (keep) {
+                        atomicOr(err, ERR_STRUCTURE);
                     }
                     acc[col] = 0.0f;
                     ++pos;
