@@ -14,6 +14,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -192,20 +193,26 @@ static void set_mode_attrs() {
                 cudaGetErrorString(cudaGetLastError()));
 }
 
-// Heavy kernel shape for every chunk width: chunks (warps) per CTA, the
-// largest group up to HEAVY_GROUP_MAX whose FILL accumulators, bitmaps and
-// staging fit one CTA's shared memory (every mode of a plan shares the
-// padded work items, hence one group size per chunk width), and the resident
-// CTAs per SM of each mode; the launches fill the GPU once and the CTAs pull
-// groups from a counter.
-int heavy_group(int cw_log2) {
-    int g = HEAVY_GROUP_MAX;
-    while (g > 1 && heavy_grp_smem_bytes(FILL, 1 << cw_log2, g) > HEAVY_SMEM_MAX - HEAVY_SMEM_STATIC)
-        --g;
-    return g;
-}
+// Heavy kernel shape for every mode and chunk width. A row's work items are
+// padded to a multiple of HEAVY_GROUP_MAX, so any group size dividing it
+// (8, 4, 2, 1) keeps every group inside one row, and each mode takes its own:
+// COUNT, whose warps hold only a bitmap, the full group of 8 (each B-row
+// lookup shared by 8 chunks); FILL and REUSE, whose warps hold a float per
+// column, 2 (measured on R-MAT 2^20 at 2^10..2^12-column chunks: larger
+// groups cost resident warps and wait on their slowest warp at every batch,
+// smaller ones repeat the lookups), or the largest smaller group that fits.
+// The launches fill the GPU once and the CTAs pull groups from a counter.
+// RVSP_HEAVY_GROUP="count,fill,reuse" in the environment overrides the
+// choice (each a divisor of 8 that fits).
+static int g_heavy_g[3][HEAVY_CW_LOG2_MAX + 1];
 static int g_heavy_ctas[3][HEAVY_CW_LOG2_MAX + 1];
 static int g_sms = 148;
+
+int heavy_group(int mode, int cw_log2) { return g_heavy_g[mode][cw_log2]; }
+
+static bool heavy_fits(int mode, int cl, int g) {
+    return heavy_grp_smem_bytes(mode, 1 << cl, g) <= HEAVY_SMEM_MAX - HEAVY_SMEM_STATIC;
+}
 
 static std::once_flag g_attr_once;
 void init_kernel_attributes() {
@@ -216,18 +223,35 @@ void init_kernel_attributes() {
         int dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess)
             cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+        int forced[3] = {0, 0, 0};
+        if (const char* e = getenv("RVSP_HEAVY_GROUP"))
+            if (sscanf(e, "%d,%d,%d", &forced[0], &forced[1], &forced[2]) != 3)
+                forced[0] = forced[1] = forced[2] = 0;
         for (int cl = HEAVY_CW_LOG2_MIN; cl <= HEAVY_CW_LOG2_MAX; ++cl) {
             const void* fns[3] = {(const void*)k_heavy<COUNT>, (const void*)k_heavy<FILL>,
                                   (const void*)k_heavy<REUSE>};
-            const int G = heavy_group(cl);
             for (int m = 0; m < 3; ++m) {
-                int n = 0;
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                        &n, fns[m], G * 32, heavy_grp_smem_bytes(m, 1 << cl, G)) != cudaSuccess) {
-                    cudaGetLastError();
-                    n = 1;
+                int ctas[HEAVY_GROUP_MAX + 1] = {};
+                for (int g = HEAVY_GROUP_MAX; g >= 1; g >>= 1) {
+                    if (!heavy_fits(m, cl, g)) continue;
+                    int n = 0;
+                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                            &n, fns[m], g * 32, heavy_grp_smem_bytes(m, 1 << cl, g)) != cudaSuccess) {
+                        cudaGetLastError();
+                        n = 0;
+                    }
+                    ctas[g] = n;
                 }
-                g_heavy_ctas[m][cl] = n > 0 ? n : 1;
+                int pick = 1;
+                for (int g = m == COUNT ? HEAVY_GROUP_MAX : 2; g >= 1; g >>= 1)
+                    if (ctas[g] > 0) {
+                        pick = g;
+                        break;
+                    }
+                const int f = forced[m];
+                if (f > 0 && HEAVY_GROUP_MAX % f == 0 && ctas[f] > 0) pick = f;
+                g_heavy_g[m][cl] = pick;
+                g_heavy_ctas[m][cl] = ctas[pick] > 0 ? ctas[pick] : 1;
             }
         }
         cudaGetLastError();
@@ -326,7 +350,7 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
         } else if (plan->n_items > 0) {
             KTime kt(plan->stream, plan->capturing, KF_HEAVY_COUNT + MODE);
             const int cl = plan->params.heavy_cw_log2;
-            const int G = heavy_group(cl);
+            const int G = heavy_group(MODE, cl);
             const int ngroups = plan->n_items / G;
             const int64_t fill = (int64_t)g_sms * g_heavy_ctas[MODE][cl];
             const int grid = (int)std::min<int64_t>(ngroups, fill);
@@ -461,7 +485,7 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     {
         KTime kt(plan->stream, plan->capturing, KF_ANALYSIS);
         k_analyze<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(
-            A, B, out, plan->params, heavy_group(plan->params.heavy_cw_log2));
+            A, B, out, plan->params, HEAVY_GROUP_MAX);
     }
     note_launch(plan, 1);
     int st = scan_counts(plan, plan->tile_hist.as<int32_t>(), NUM_BINS * tiles, nullptr,
@@ -569,7 +593,7 @@ void launch_bin_scatter(rvsp_cuda_plan* plan, const uint8_t* bin, const int32_t*
     k_bin_scatter<<<(unsigned)((M + AN_TILE - 1) / AN_TILE), AN_TILE, 0, plan->stream>>>(
         (int32_t)M, bin, tile_off, plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
         bin_rows, &misc->item_cursor, heavy_items ? plan->items.as<HeavyItem>() : nullptr,
-        heavy_group(plan->params.heavy_cw_log2));
+        HEAVY_GROUP_MAX);
     note_launch(plan, 1);
 }
 
