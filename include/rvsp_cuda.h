@@ -346,10 +346,20 @@ RVSP_CUDA_API int rvsp_cuda_plan_row_stats(rvsp_cuda_plan_t plan, float *feat_ou
  * path), [3] sum of the counts, [4] sum of the predicted capacities and
  * [6] sum of the upper bounds of predicted rows that fit, [5] rows finished
  * by the exact path, and (n >= 8) [7] rows sized by the prediction whose
- * exact count exceeds the predicted capacity: the misprediction count. In a
- * structure-filling numeric every such row is re-run ([7] == [1]); in the
- * descriptor's count a row whose hash table still held it needs no re-run. */
+ * exact count exceeds the predicted capacity: the misprediction count, and
+ * (n >= 10) [8] entries of heavy rows placed in the shared overflow pool
+ * and [9] that pool's capacity. In the one-shot product heavy rows are
+ * sized by the prediction too; a heavy row counts in [1] only when some of
+ * its chunks found room neither in its slot nor in the pool (it is filled
+ * again), in [7] whenever its count passes its capacity. In the descriptor's
+ * count a row whose hash table still held it needs no re-run.
+ * No reference counterpart (the reference has no learned sizing). */
 RVSP_CUDA_API int rvsp_cuda_plan_learned_stats(rvsp_cuda_plan_t plan, int64_t *out, int32_t n);
+
+/* The same statistics for the calling thread's last learned one-shot product
+ * (rvsp_cuda_spgemm_f32 with RVSP_CUDA_ALGO_LEARNED); RVSP_ERROR_INVALID_ARGUMENT
+ * before the first one. No reference counterpart. */
+RVSP_CUDA_API int rvsp_cuda_oneshot_learned_stats(int64_t *out, int32_t n);
 
 /*
  * Allocation-free row pointer of C from per-row counts. No counterpart in the
@@ -395,7 +405,7 @@ RVSP_CUDA_API int64_t rvsp_cuda_launch_count(void);
  * RVSP_CUDA_KERNEL_FAMILIES. rvsp_cuda_kernel_family(i) names family i
  * (NULL out of range).
  */
-#define RVSP_CUDA_KERNEL_FAMILIES 13
+#define RVSP_CUDA_KERNEL_FAMILIES 15
 RVSP_CUDA_API int rvsp_cuda_kernel_timing(int on);
 RVSP_CUDA_API int rvsp_cuda_kernel_times(double *ms_out, int64_t *launches_out, int32_t n);
 RVSP_CUDA_API const char *rvsp_cuda_kernel_family(int32_t i);

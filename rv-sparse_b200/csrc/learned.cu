@@ -451,6 +451,8 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
     plan->items_counted = plan->n_items == 0 || fused;
     for (int i = 0; i < 8; ++i) plan->lstats[i] = plan->host_misc.lstats[i];
     plan->lstats[5] = plan->host_misc.n_need;
+    plan->lstats[8] = (int64_t)plan->host_misc.pool_fill;
+    plan->lstats[9] = plan->pool_cap;
     return RVSP_SUCCESS;
 }
 
@@ -591,7 +593,7 @@ int rvsp_cuda_plan_learned_stats(rvsp_cuda_plan_t plan, int64_t* out, int32_t n)
     if (!plan || !out) return RVSP_ERROR_NULL_POINTER;
     if (n < 7) return RVSP_ERROR_INVALID_ARGUMENT;
     if (plan->algo != RVSP_CUDA_ALGO_LEARNED || !plan->analysed) return RVSP_ERROR_INVALID_ARGUMENT;
-    memcpy(out, plan->lstats, sizeof(int64_t) * (n < 8 ? n : 8));
+    memcpy(out, plan->lstats, sizeof(int64_t) * (n < 10 ? n : 10));
     return RVSP_SUCCESS;
 }
 

@@ -176,3 +176,10 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
     if (op_counts_out) st = rvsp_cuda_op_counts(plan, op_counts_out, a_rows);
     return st;
 }
+
+extern "C" int rvsp_cuda_oneshot_learned_stats(int64_t* out, int32_t n) {
+    if (!out) return RVSP_ERROR_NULL_POINTER;
+    rvsp_cuda_plan_t plan = t_plan[1];
+    if (!plan) return RVSP_ERROR_INVALID_ARGUMENT;
+    return rvsp_cuda_plan_learned_stats(plan, out, n);
+}

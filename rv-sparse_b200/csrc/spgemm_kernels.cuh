@@ -143,8 +143,10 @@ struct AnalyzeOut {
     float4* feat;        // [rows] learned-model features (optional)
     int32_t* hist;       // [NUM_BINS] rows per bin
     int32_t* tile_hist;  // [NUM_BINS][tiles] rows per bin per tile (stable binning)
-    int64_t* totals;     // [0] heavy items, [1] products
+    int64_t* totals;     // [0] heavy items, [1] products, [2] heavy-row segments,
+                         // [3] heavy-row bucket histogram entries
     int64_t* bin_prod;   // [NUM_BINS] products per bin
+    int32_t* max_nch;    // most column chunks of a heavy row
     int32_t* err;        // ERR_* bits
 };
 
@@ -186,7 +188,7 @@ __global__ void __launch_bounds__(AN_TILE)
     __shared__ int32_t s_maxc[AN_TILE];
     __shared__ int32_t s_hist[NUM_BINS];
     __shared__ unsigned long long s_bprod[NUM_BINS];
-    __shared__ unsigned long long s_items, s_prod;
+    __shared__ unsigned long long s_items, s_prod, s_segs, s_hent;
     __shared__ int s_long;
 
     const int r0 = blockIdx.x * AN_TILE;
@@ -200,6 +202,8 @@ __global__ void __launch_bounds__(AN_TILE)
     if (t == 0) {
         s_items = 0;
         s_prod = 0;
+        s_segs = 0;
+        s_hent = 0;
         s_long = 0;
     }
     __syncthreads();
@@ -292,9 +296,18 @@ __global__ void __launch_bounds__(AN_TILE)
     // a heavy row's items are padded to whole groups of the heavy kernel
     const int nitems = (nch + heavy_group - 1) / heavy_group * heavy_group;
     const unsigned long long witems = warp_sum64((unsigned long long)nitems);
+    // heavy rows' bucket layout: segments of about HB_SEG products, and a
+    // histogram entry per (chunk, segment)
+    const int nseg = nch > 0 ? (int)max((int64_t)1, (ops + HB_SEG - 1) / HB_SEG) : 0;
+    const unsigned long long wsegs = warp_sum64((unsigned long long)nseg);
+    const unsigned long long whent = warp_sum64((unsigned long long)nch * (unsigned long long)nseg);
+    const int wmaxnch = __reduce_max_sync(FULL, (unsigned)nch);
+    if (lane_id() == 0 && wmaxnch > 0) atomicMax(out.max_nch, wmaxnch);
     if (lane_id() == 0) {
         if (wprod) atomicAdd(&s_prod, wprod);
         if (witems) atomicAdd(&s_items, witems);
+        if (wsegs) atomicAdd(&s_segs, wsegs);
+        if (whent) atomicAdd(&s_hent, whent);
     }
     __syncthreads();
     if (t < NUM_BINS) {
@@ -304,9 +317,21 @@ __global__ void __launch_bounds__(AN_TILE)
     }
     if (t == 0) {
         if (s_items) atomicAdd((unsigned long long*)&out.totals[0], s_items);
+        if (s_segs) atomicAdd((unsigned long long*)&out.totals[2], s_segs);
+        if (s_hent) atomicAdd((unsigned long long*)&out.totals[3], s_hent);
         atomicAdd((unsigned long long*)&out.totals[1], s_prod);
     }
 }
+
+// Where k_bin_scatter records the heavy rows' bucket layout (all null: not
+// recorded).
+struct HeavyRowsOut {
+    int32_t* nseg;                    // [rows] segments of each heavy row
+    int32_t* sbase;                   // [rows] first segment
+    int64_t* hbase;                   // [rows] first histogram entry
+    int32_t* seg_cursor;
+    unsigned long long* hist_cursor;
+};
 
 // Stable partition of rows by bin: tile_off[b * tiles + tile] is where the
 // tile's rows of bin b start in bin_rows (an exclusive scan of tile_hist), so
@@ -317,7 +342,7 @@ __global__ void __launch_bounds__(AN_TILE)
                   const int32_t* __restrict__ tile_off, const int32_t* __restrict__ chunk_lo,
                   const int32_t* __restrict__ nchunks, int32_t* __restrict__ bin_rows,
                   int32_t* __restrict__ item_cursor, HeavyItem* __restrict__ items,
-                  int heavy_group) {
+                  int heavy_group, const int64_t* __restrict__ ops, HeavyRowsOut hro) {
     __shared__ int32_t s_wc[AN_TILE / 32][NUM_BINS];
     const int t = threadIdx.x, lane = lane_id(), warp = t >> 5;
     const int row = blockIdx.x * AN_TILE + t;
@@ -342,6 +367,13 @@ __global__ void __launch_bounds__(AN_TILE)
         const int lo = chunk_lo[row];
         for (int c = 0; c < padded; ++c)
             items[first + c] = HeavyItem{row, c < n ? lo + c : -1, first, 0};
+        if (hro.nseg) {  // the row's segments and histogram entries (k_analyze's rule)
+            const int ns = (int)max((int64_t)1, (ops[row] + HB_SEG - 1) / HB_SEG);
+            hro.nseg[row] = ns;
+            hro.sbase[row] = atomicAdd(hro.seg_cursor, ns);
+            hro.hbase[row] = (int64_t)atomicAdd(hro.hist_cursor,
+                                                (unsigned long long)n * (unsigned long long)ns);
+        }
     }
 }
 
@@ -1429,6 +1461,113 @@ __device__ __forceinline__ void heavy_segments(const CsrView& B, int s, int len,
     }
 }
 
+// End of a heavy work item w (row `row`, chunk starting at column lo) for
+// the calling warp, whose accumulator and bitmap hold the chunk: COUNT
+// records the chunk's count (and adds it to the row's); FILL writes the
+// chunk's columns in order with their values at the chunk's place in C (or,
+// in the learned sweep, in the row's slot or the overflow pool, RowCtl);
+// REUSE writes the values at the chunk's known positions in C. The bitmap
+// and accumulator are left zeroed for the warp's next item (REUSE zeroes its
+// accumulator when it starts an item).
+template <int MODE>
+__device__ __forceinline__ void heavy_finish(
+    const CsrView& B, int w, const HeavyItem& it, int row, int lo, int cw, float* acc,
+    unsigned* bits, int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
+    const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
+    int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err,
+    const RowCtl& ctl) {
+    const int lane = lane_id();
+    const int nw = cw >> 5;
+    __syncwarp();
+    if (MODE == COUNT) {
+        int c = 0;
+        for (int x = lane; x < nw; x += 32) {
+            c += __popc(bits[x]);
+            bits[x] = 0u;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+        if (lane == 0) {
+            item_cnt[w] = c;
+            if (c && row_cnt) atomicAdd(&row_cnt[row], c);
+        }
+    } else if (MODE == FILL) {
+        // lane l writes the present columns of bitmap word x0 + l; the
+        // words' popcounts give each lane its first output position
+        int64_t out;
+        bool keep = true;
+        if (ctl.item_off) {
+            // learned sweep: the chunk takes the next place in its row's
+            // slot (c_ci / c_v are the slot buffers), else in the shared
+            // overflow pool; a chunk that finds no room only clears its
+            // bitmap and accumulator
+            int c = 0;
+            for (int x = lane; x < nw; x += 32) c += __popc(bits[x]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+            long long dst = -1;
+            if (lane == 0) {
+                item_cnt[w] = c;
+                const int off = atomicAdd(&row_cnt[row], c);
+                const int64_t s0 = ctl.slot_off[row], cap = ctl.slot_off[row + 1] - s0;
+                if ((int64_t)off + c <= cap) {
+                    dst = s0 + off;
+                } else if (c > 0) {
+                    const unsigned long long p =
+                        atomicAdd(ctl.pool_fill, (unsigned long long)c);
+                    if ((int64_t)p + c <= ctl.pool_cap) dst = ctl.pool_base + (int64_t)p;
+                } else {
+                    dst = s0;  // an empty chunk needs no room
+                }
+                ctl.item_off[w] = dst;
+                if (dst < 0) ctl.ovf[row] = 1;
+            }
+            dst = __shfl_sync(FULL, dst, 0);
+            keep = dst >= 0;
+            out = dst;
+        } else {
+            out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
+        }
+        // writes into C stay inside the row (counts that disagree with
+        // this fill would only come from an operand changed in between)
+        const int64_t lim = ctl.item_off ? INT64_MAX : (int64_t)c_rp[row + 1];
+        for (int x0 = 0; x0 < nw; x0 += 32) {
+            unsigned word = 0u;
+            if (x0 + lane < nw) {
+                word = bits[x0 + lane];
+                bits[x0 + lane] = 0u;
+            }
+            const int pc = __popc(word);
+            const int incl = warp_incl_scan(pc);
+            int64_t pos = out + (incl - pc);
+            while (word) {
+                const int b = __ffs(word) - 1;
+                word &= word - 1;
+                const int col = (x0 + lane) * 32 + b;
+                if (keep && pos < lim) {
+                    c_ci[pos] = lo + col;
+                    c_v[pos] = acc[col];
+                } else if (keep) {
+                    atomicOr(err, ERR_STRUCTURE);
+                }
+                acc[col] = 0.0f;
+                ++pos;
+            }
+            out += __shfl_sync(FULL, incl, 31);
+        }
+    } else {
+        const int hi = (int)min((int64_t)lo + cw, (int64_t)B.cols);
+        const int r0 = c_rp[row], r1 = c_rp[row + 1];
+        const int s = warp_lower_bound(c_ci, r0, r1, lo);
+        const int t2 = warp_lower_bound(c_ci, s, r1, hi);
+        for (int q = s + lane; q < t2; q += 32) {
+            const int col = c_ci[q] - lo;
+            c_v[q] = (unsigned)col < (unsigned)cw ? acc[col] : 0.0f;
+        }
+    }
+    __syncwarp();
+}
+
 // Heavy rows, grouped. The work items are (row, column chunk) pairs, each
 // row's items padded to a multiple of the group size G (padding items have
 // chunk -1), so G consecutive items never cross rows. One CTA of G warps
@@ -1571,94 +1710,272 @@ __global__ void __launch_bounds__(HEAVY_GROUP_MAX * 32)
             if (MODE == COUNT && lane == 0) item_cnt[w] = 0;  // padding item
             continue;
         }
+        heavy_finish<MODE>(B, w, it, row, lo, cw, acc, bits, item_cnt, row_cnt, item_scan, c_rp,
+                           c_ci, c_v, err, ctl);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Heavy rows, bucketed by column chunk (COUNT and FILL). A warp walking a
+// heavy row's A entries once per chunk pays for every (entry, chunk) pair,
+// which on power-law products (hundreds of entries, under one product per
+// entry and chunk) costs more than the products themselves. Here every heavy
+// row is cut into segments of about HB_SEG products (consecutive A entries);
+// per segment one warp
+//   k_hhist     counts the segment's products per column chunk of its row
+//   (scan)      the counts, chunk-major then segment, become bucket offsets:
+//               chunk c of a row gets one contiguous bucket in which the
+//               segments' products follow each other in A-row order
+//   k_hscatter  walks the segment again in the reference's product order and
+//               writes each product's column (and its rounded product a*b)
+//               to its chunk's bucket; lanes of one step that go to the same
+//               chunk are ranked in lane order, so every bucket keeps the
+//               products of its chunk in A-row order
+// and per work item (row, chunk) one warp
+//   k_hacc      reads its bucket (contiguous, coalesced) into the presence
+//               bitmap (COUNT, FILL) and the accumulator from +0.0f (FILL,
+//               same-column products of a step combined in lane order), then
+//               ends the item like the grouped kernel (heavy_finish).
+// Every A entry is walked twice in all (three times with a separate value
+// scatter), whatever the number of chunks; values keep the reference's order.
+// ---------------------------------------------------------------------------
+constexpr int HB_WARPS = 2;         // warps per CTA of k_hhist / k_hscatter
+
+struct HSeg {
+    int32_t row;
+    int32_t e0, e1;  // A entries [e0, e1)
+    int32_t k;       // segment index within its row
+};
+
+// Bucket layout of a plan's heavy rows.
+struct HBuckets {
+    const int32_t* nseg;     // [rows] segments of each heavy row
+    const int64_t* hbase;    // [rows] first histogram entry of each heavy row
+    const int32_t* chunk_lo; // [rows] first column chunk of each heavy row
+    const int32_t* nchunks;  // [rows] column chunks of each heavy row
+    const HSeg* segs;
+    int32_t nsegs;
+    int32_t* hist;           // [H] products per (row, chunk, segment), chunk-major
+    const int64_t* hoff;     // [H + 1] exclusive scan of hist: bucket starts
+    int32_t* pcol;           // [products of the heavy rows] bucketed columns
+    float* pval;             //   and rounded products a*b
+};
+
+// Segments of the heavy rows: one warp per row. Entry j belongs to segment
+// min(P(j) / HB_SEG, nseg - 1), P(j) the products of the row's entries
+// before j, so segments are contiguous entry ranges (an entry with more than
+// HB_SEG products leaves empty segments behind it).
+__global__ void __launch_bounds__(256)
+    k_hsegs(CsrView A, CsrView B, const int32_t* __restrict__ rows, int32_t n,
+            const int32_t* __restrict__ nseg, const int32_t* __restrict__ sbase,
+            HSeg* __restrict__ segs, int32_t* __restrict__ err) {
+    const int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = lane_id();
+    if (wg >= n) return;
+    const int row = rows[wg];
+    int a0, a1;
+    row_range(A, row, &a0, &a1, err);
+    const int ns = nseg[row];
+    HSeg* sg = segs + sbase[row];
+    if (lane == 0) sg[0].e0 = a0;
+    long long run = 0;  // products of the entries before this batch
+    int prev = 0;       // segment of the entry before this batch
+    for (int base = a0; base < a1; base += 32) {
+        const int j = base + lane;
+        long long len = 0;
+        if (j < a1) {
+            int bs, be;
+            row_range(B, A.ci[j], &bs, &be, err);
+            len = be - bs;
+        }
+        long long incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const long long pj = run + incl - len;
+        const int sj = j < a1 ? (int)min(pj / HB_SEG, (long long)ns - 1) : ns - 1;
+        int p = __shfl_up_sync(FULL, sj, 1);
+        if (lane == 0) p = prev;
+        if (j < a1)
+            for (int k = p + 1; k <= sj; ++k) sg[k].e0 = j;  // segments starting at entry j
+        const int last = min(31, a1 - 1 - base);
+        run += __shfl_sync(FULL, incl, 31);
+        prev = __shfl_sync(FULL, sj, last);
+    }
+    if (lane == 0)
+        for (int k = prev + 1; k < ns; ++k) sg[k].e0 = a1;
+    __syncwarp();
+    for (int k = lane; k < ns; k += 32) {
+        sg[k].row = row;
+        sg[k].k = k;
+        sg[k].e1 = k + 1 < ns ? sg[k + 1].e0 : a1;
+    }
+}
+
+// Products per (row, chunk, segment): one warp per segment, a shared
+// histogram of the row's chunks (nch_max ints per warp).
+__global__ void __launch_bounds__(HB_WARPS * 32)
+    k_hhist(CsrView A, CsrView B, HBuckets hb, int cw_log2, int nch_max,
+            int32_t* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    int32_t* h = reinterpret_cast<int32_t*>(smem) + warp * nch_max;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < hb.nsegs;
+         s += nwarps) {
+        const HSeg sg = hb.segs[s];
+        const int clo = hb.chunk_lo[sg.row], nch = hb.nchunks[sg.row];
+        if (nch > nch_max) {  // not a heavy row of this layout (a broken plan)
+            if (lane == 0) atomicOr(err, ERR_STRUCTURE);
+            continue;
+        }
+        for (int c = lane; c < nch; c += 32) h[c] = 0;
         __syncwarp();
-        if (MODE == COUNT) {
-            int c = 0;
-            for (int x = lane; x < nw; x += 32) {
-                c += __popc(bits[x]);
-                bits[x] = 0u;
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
-            if (lane == 0) {
-                item_cnt[w] = c;
-                if (c && row_cnt) atomicAdd(&row_cnt[row], c);
-            }
-        } else if (MODE == FILL) {
-            // lane l writes the present columns of bitmap word x0 + l; the
-            // words' popcounts give each lane its first output position
-            int64_t out;
-            bool keep = true;
-            if (ctl.item_off) {
-                // learned sweep: the chunk takes the next place in its row's
-                // slot (c_ci / c_v are the slot buffers), else in the shared
-                // overflow pool; a chunk that finds no room only clears its
-                // bitmap and accumulator
-                int c = 0;
-                for (int x = lane; x < nw; x += 32) c += __popc(bits[x]);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
-                long long dst = -1;
-                if (lane == 0) {
-                    item_cnt[w] = c;
-                    const int off = atomicAdd(&row_cnt[row], c);
-                    const int64_t s0 = ctl.slot_off[row], cap = ctl.slot_off[row + 1] - s0;
-                    if ((int64_t)off + c <= cap) {
-                        dst = s0 + off;
-                    } else if (c > 0) {
-                        const unsigned long long p =
-                            atomicAdd(ctl.pool_fill, (unsigned long long)c);
-                        if ((int64_t)p + c <= ctl.pool_cap) dst = ctl.pool_base + (int64_t)p;
-                    } else {
-                        dst = s0;  // an empty chunk needs no room
-                    }
-                    ctl.item_off[w] = dst;
-                    if (dst < 0) ctl.ovf[row] = 1;
-                }
-                dst = __shfl_sync(FULL, dst, 0);
-                keep = dst >= 0;
-                out = dst;
-            } else {
-                out = (int64_t)c_rp[row] + (item_scan[w] - item_scan[it.first]);
-            }
-            // writes into C stay inside the row (counts that disagree with
-            // this fill would only come from an operand changed in between)
-            const int64_t lim = ctl.item_off ? INT64_MAX : (int64_t)c_rp[row + 1];
-            for (int x0 = 0; x0 < nw; x0 += 32) {
-                unsigned word = 0u;
-                if (x0 + lane < nw) {
-                    word = bits[x0 + lane];
-                    bits[x0 + lane] = 0u;
-                }
-                const int pc = __popc(word);
-                const int incl = warp_incl_scan(pc);
-                int64_t pos = out + (incl - pc);
-                while (word) {
-                    const int b = __ffs(word) - 1;
-                    word &= word - 1;
-                    const int col = (x0 + lane) * 32 + b;
-                    if (keep && pos < lim) {
-                        c_ci[pos] = lo + col;
-                        c_v[pos] = acc[col];
-                    } else if (keep) {
-                        atomicOr(err, ERR_STRUCTURE);
-                    }
-                    acc[col] = 0.0f;
-                    ++pos;
-                }
-                out += __shfl_sync(FULL, incl, 31);
-            }
-        } else {
-            const int hi = (int)min((int64_t)lo + cw, (int64_t)B.cols);
-            const int r0 = c_rp[row], r1 = c_rp[row + 1];
-            const int s = warp_lower_bound(c_ci, r0, r1, lo);
-            const int t2 = warp_lower_bound(c_ci, s, r1, hi);
-            for (int q = s + lane; q < t2; q += 32) {
-                const int col = c_ci[q] - lo;
-                c_v[q] = (unsigned)col < (unsigned)cw ? acc[col] : 0.0f;
-            }
+        walk_products<false>(A, B, sg.e0, sg.e1, err,
+                             [&](int, bool pv, int col, float, float, bool) {
+                                 if (pv) {
+                                     const int c = (col >> cw_log2) - clo;
+                                     if ((unsigned)c < (unsigned)nch) atomicAdd(&h[c], 1);
+                                     else atomicOr(err, ERR_STRUCTURE);
+                                 }
+                                 return false;
+                             });
+        __syncwarp();
+        const int ns = hb.nseg[sg.row];
+        const int64_t base = hb.hbase[sg.row] + sg.k;
+        for (int c = lane; c < nch; c += 32) hb.hist[base + (int64_t)c * ns] = h[c];
+        __syncwarp();
+    }
+}
+
+// Bucketed products: one warp per segment walks it again in product order;
+// the segment's part of every chunk bucket [start, end) is held in shared
+// memory (nch_max pairs of int64 per warp) and its start advances as the
+// products land. COLS writes the columns, VALS the rounded products.
+template <bool COLS, bool VALS>
+__global__ void __launch_bounds__(HB_WARPS * 32)
+    k_hscatter(CsrView A, CsrView B, HBuckets hb, int cw_log2, int nch_max,
+               int32_t* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    long long* cur = reinterpret_cast<long long*>(smem) + 2 * warp * nch_max;
+    long long* end = cur + nch_max;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < hb.nsegs;
+         s += nwarps) {
+        const HSeg sg = hb.segs[s];
+        const int clo = hb.chunk_lo[sg.row], nch = hb.nchunks[sg.row];
+        if (nch > nch_max) {
+            if (lane == 0) atomicOr(err, ERR_STRUCTURE);
+            continue;
+        }
+        const int ns = hb.nseg[sg.row];
+        const int64_t base = hb.hbase[sg.row] + sg.k;
+        for (int c = lane; c < nch; c += 32) {
+            cur[c] = hb.hoff[base + (int64_t)c * ns];
+            end[c] = hb.hoff[base + (int64_t)c * ns + 1];
         }
         __syncwarp();
+        walk_products<VALS>(A, B, sg.e0, sg.e1, err,
+                            [&](int, bool pv, int col, float bv, float av, bool) {
+                                int c = pv ? (col >> cw_log2) - clo : -1;
+                                if (pv && (unsigned)c >= (unsigned)nch) {
+                                    atomicOr(err, ERR_STRUCTURE);
+                                    pv = false;
+                                }
+                                const unsigned peers =
+                                    __match_any_sync(FULL, pv ? c : (0x40000000 | lane));
+                                const int leader = __ffs(peers) - 1;
+                                long long at = 0;
+                                if (pv && lane == leader) {
+                                    at = cur[c];
+                                    cur[c] = at + __popc(peers);
+                                }
+                                at = __shfl_sync(FULL, at, leader);
+                                const long long pos = at + __popc(peers & ((1u << lane) - 1));
+                                if (pv) {
+                                    if (pos < end[c]) {
+                                        if (COLS) hb.pcol[pos] = col;
+                                        if (VALS) hb.pval[pos] = __fmul_rn(av, bv);
+                                    } else {
+                                        atomicOr(err, ERR_STRUCTURE);
+                                    }
+                                }
+                                return false;
+                            });
+        __syncwarp();
+    }
+}
+
+// Work items from their buckets: one warp per item, items pulled from a
+// counter by a grid that fills the GPU once. COUNT and FILL only (REUSE
+// keeps the grouped kernel, which needs no bucketed products).
+template <int MODE>
+__global__ void __launch_bounds__(256)
+    k_hacc(const CsrView B, HBuckets hb, const HeavyItem* __restrict__ items, int nitems,
+           int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
+           const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
+           int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err,
+           RowCtl ctl, int cw_log2, int32_t* __restrict__ queue) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int cw = 1 << cw_log2;
+    const int nw = cw >> 5;
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    unsigned char* mine = smem + warp * heavy_smem_bytes(MODE, cw);
+    float* acc = reinterpret_cast<float*>(mine);
+    unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * cw));
+    if (MODE != COUNT) {
+        float4* a4 = reinterpret_cast<float4*>(acc);
+        for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (int x = lane; x < nw; x += 32) bits[x] = 0u;
+    __syncwarp();
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = atomicAdd(queue, 1);
+        w = __shfl_sync(FULL, w, 0);
+        if (w >= nitems) break;
+        const HeavyItem it = items[w];
+        if (it.chunk < 0) {
+            if (MODE == COUNT && lane == 0) item_cnt[w] = 0;  // padding item
+            continue;
+        }
+        const int row = it.row;
+        if (ctl.only && !ctl.only[row]) continue;
+        const int lo = it.chunk << cw_log2;
+        const int cl = it.chunk - hb.chunk_lo[row];
+        const int ns = hb.nseg[row];
+        const int64_t hi0 = hb.hbase[row] + (int64_t)cl * ns;
+        const long long q0 = hb.hoff[hi0], q1 = hb.hoff[hi0 + ns];
+        // two steps of 32 products loaded before either is accumulated
+        for (long long b0 = q0; b0 < q1; b0 += 64) {
+            const long long qa = b0 + lane, qb = b0 + 32 + lane;
+            int ca = -1, cb = -1;
+            float va = 0.0f, vb = 0.0f;
+            if (qa < q1) {
+                ca = hb.pcol[qa] - lo;
+                if (MODE != COUNT) va = hb.pval[qa];
+            }
+            if (qb < q1) {
+                cb = hb.pcol[qb] - lo;
+                if (MODE != COUNT) vb = hb.pval[qb];
+            }
+            const bool oka = qa < q1 && (unsigned)ca < (unsigned)cw;
+            const bool okb = qb < q1 && (unsigned)cb < (unsigned)cw;
+            if ((qa < q1 && !oka) || (qb < q1 && !okb)) atomicOr(err, ERR_STRUCTURE);
+            if (oka) atomicOr(&bits[ca >> 5], 1u << (ca & 31));
+            if (okb) atomicOr(&bits[cb >> 5], 1u << (cb & 31));
+            if (MODE != COUNT) {
+                ordered_add(acc, oka ? ca : 0, oka, va);
+                __syncwarp();
+                if (b0 + 32 < q1) ordered_add(acc, okb ? cb : 0, okb, vb);
+            }
+            __syncwarp();
+        }
+        heavy_finish<MODE>(B, w, it, row, lo, cw, acc, bits, item_cnt, row_cnt, item_scan, c_rp,
+                           c_ci, c_v, err, ctl);
     }
 }
 

@@ -96,6 +96,12 @@ struct HeavyAux {
 };
 constexpr int DIR_MIN_LEN = 32;
 
+// Heavy rows bucketed by column chunk (COUNT and FILL): a heavy row is cut
+// into segments of about HB_SEG products, one warp each; the path takes
+// products whose heavy rows have at most HB_NCH_MAX column chunks.
+constexpr int HB_SEG = 1 << 16;
+constexpr int HB_NCH_MAX = 4096;
+
 struct BinOffsets {
     int32_t off[NUM_BINS];
 };

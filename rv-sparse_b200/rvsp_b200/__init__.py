@@ -135,6 +135,7 @@ _PROTOS = {
     "rvsp_cuda_plan_collect_features": (C.c_int, [_VP, C.c_int]),
     "rvsp_cuda_plan_row_stats": (C.c_int, [_VP, _VP, _VP, _VP, _I32]),
     "rvsp_cuda_plan_learned_stats": (C.c_int, [_VP, _VP, _I32]),
+    "rvsp_cuda_oneshot_learned_stats": (C.c_int, [_VP, _I32]),
     "rvsp_cuda_row_ptr_noalloc": (C.c_int, [_VP, _I32, _VP, C.POINTER(_I64), _VP]),
     "rvsp_cuda_plan_set_params": (C.c_int, [_VP, _VP, _I32]),
     "rvsp_cuda_plan_get_params": (C.c_int, [_VP, _VP, _I32]),
@@ -193,7 +194,7 @@ def launch_count() -> int:
     return lib().rvsp_cuda_launch_count()
 
 
-KERNEL_FAMILIES = 13
+KERNEL_FAMILIES = 15
 
 
 def kernel_timing(on: bool) -> None:
@@ -386,11 +387,22 @@ class Plan:
         return feat[:n], cnt[:n], ub[:n]
 
     def learned_stats(self):
-        out = np.zeros(8, np.int64)
-        check(self.L.rvsp_cuda_plan_learned_stats(self.h, out.ctypes.data, 8), "learned_stats")
-        keys = ["predicted_rows", "overflowed_rows", "exact_by_size_rows", "fit_nnz",
-                "fit_capacity", "exact_rows", "fit_upper_bound", "underpredicted_rows"]
-        return dict(zip(keys, out.tolist()))
+        out = np.zeros(len(LEARNED_STATS), np.int64)
+        check(self.L.rvsp_cuda_plan_learned_stats(self.h, out.ctypes.data, out.size),
+              "learned_stats")
+        return dict(zip(LEARNED_STATS, out.tolist()))
+
+
+LEARNED_STATS = ("predicted_rows", "overflowed_rows", "exact_by_size_rows", "fit_nnz",
+                 "fit_capacity", "exact_rows", "fit_upper_bound", "underpredicted_rows",
+                 "pool_entries", "pool_capacity")
+
+
+def oneshot_learned_stats():
+    """Learned-path statistics of this thread's last learned one-shot product."""
+    out = np.zeros(len(LEARNED_STATS), np.int64)
+    check(lib().rvsp_cuda_oneshot_learned_stats(out.ctypes.data, out.size), "oneshot stats")
+    return dict(zip(LEARNED_STATS, out.tolist()))
 
 
 def set_default_params(params=None):
