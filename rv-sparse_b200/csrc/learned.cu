@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(256)
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += nwarps) {
         const HeavyItem it = items[w];
-        if (it.chunk < 0 || !hmask[it.row] || need[it.row]) continue;
+        if (!hmask[it.row] || need[it.row]) continue;
         const int k = item_cnt[w];
         const int64_t src = item_off[w];
         const int64_t dst = (int64_t)c_rp[it.row] + (item_scan[w] - item_scan[it.first]);

@@ -152,8 +152,7 @@ constexpr int map_warps() {
     return w > 8 ? 8 : (w < 1 ? 1 : w);
 }
 
-constexpr int HEAVY_SMEM_MAX = 227 * 1024;  // largest shared memory of one CTA
-constexpr int HEAVY_SMEM_STATIC = 1024;     // room kept for k_heavy's static shared memory
+constexpr int HEAVY_SMEM_MAX = 227 * 1024;  // largest dynamic shared memory of one CTA
 
 // resident CTAs per SM of every warp-bin kernel (launches fill the GPU once
 // and the warps pull rows from a counter)
@@ -185,60 +184,17 @@ static void set_mode_attrs() {
     set_warp_attr<1024, MODE>();
     set_warp_attr<2048, MODE>();
     set_warp_attr<4096, MODE>();
-    // the heavy kernel's own static shared memory comes out of the same
-    // 227 KB: its dynamic part may use all but HEAVY_SMEM_STATIC of it
-    if (cudaFuncSetAttribute(k_heavy<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             HEAVY_SMEM_MAX - HEAVY_SMEM_STATIC) != cudaSuccess)
-        fprintf(stderr, "rvsp: k_heavy shared-memory attribute not set: %s\n",
-                cudaGetErrorString(cudaGetLastError()));
-    if (MODE != REUSE &&
-        cudaFuncSetAttribute(k_hacc<MODE == REUSE ? COUNT : MODE>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, HEAVY_SMEM_MAX) !=
-            cudaSuccess)
-        fprintf(stderr, "rvsp: k_hacc shared-memory attribute not set: %s\n",
-                cudaGetErrorString(cudaGetLastError()));
+    cudaFuncSetAttribute(k_heavy<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         HEAVY_SMEM_MAX);
 }
 
-// the bucket kernels hold per-warp chunk tables of up to HB_NCH_MAX entries
-static void set_bucket_attrs() {
-    const int hist = HB_WARPS * 4 * HB_NCH_MAX, scat = HB_WARPS * 16 * HB_NCH_MAX;
-    bool ok = cudaFuncSetAttribute(k_hhist, cudaFuncAttributeMaxDynamicSharedMemorySize, hist) ==
-              cudaSuccess;
-    ok &= cudaFuncSetAttribute(k_hscatter<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               scat) == cudaSuccess;
-    ok &= cudaFuncSetAttribute(k_hscatter<true, false>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, scat) == cudaSuccess;
-    ok &= cudaFuncSetAttribute(k_hscatter<false, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, scat) == cudaSuccess;
-    if (!ok)
-        fprintf(stderr, "rvsp: bucket kernels' shared-memory attribute not set: %s\n",
-                cudaGetErrorString(cudaGetLastError()));
-}
-
-// Heavy kernel shape for every mode and chunk width. A row's work items are
-// padded to a multiple of HEAVY_GROUP_MAX, so any group size dividing it
-// (8, 4, 2, 1) keeps every group inside one row, and each mode takes its own:
-// COUNT, whose warps hold only a bitmap, the full group of 8 (each B-row
-// lookup shared by 8 chunks); FILL and REUSE, whose warps hold a float per
-// column, 2 (measured on R-MAT 2^20 at 2^10..2^12-column chunks: larger
-// groups cost resident warps and wait on their slowest warp at every batch,
-// smaller ones repeat the lookups), or the largest smaller group that fits.
-// The launches fill the GPU once and the CTAs pull groups from a counter.
-// RVSP_HEAVY_GROUP="count,fill,reuse" in the environment overrides the
-// choice (each a divisor of 8 that fits).
-static int g_heavy_g[3][HEAVY_CW_LOG2_MAX + 1];
+// Heavy kernel shape for every mode and chunk width: warps per CTA chosen to
+// keep the most warps resident per SM (each warp holds its own accumulator
+// and bitmap in shared memory), and the resident CTAs per SM; the launches
+// fill the GPU once and the warps pull work items from a counter.
+static int g_heavy_w[3][HEAVY_CW_LOG2_MAX + 1];
 static int g_heavy_ctas[3][HEAVY_CW_LOG2_MAX + 1];
-// warps per CTA (up to 8, as many as their accumulators let fit) and resident
-// CTAs per SM of the bucketed item kernel, per mode and chunk width
-static int g_hacc_w[2][HEAVY_CW_LOG2_MAX + 1];
-static int g_hacc_ctas[2][HEAVY_CW_LOG2_MAX + 1];
 static int g_sms = 148;
-
-int heavy_group(int mode, int cw_log2) { return g_heavy_g[mode][cw_log2]; }
-
-static bool heavy_fits(int mode, int cl, int g) {
-    return heavy_grp_smem_bytes(mode, 1 << cl, g) <= HEAVY_SMEM_MAX - HEAVY_SMEM_STATIC;
-}
 
 static std::once_flag g_attr_once;
 void init_kernel_attributes() {
@@ -246,52 +202,31 @@ void init_kernel_attributes() {
         set_mode_attrs<COUNT>();
         set_mode_attrs<FILL>();
         set_mode_attrs<REUSE>();
-        set_bucket_attrs();
         int dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess)
             cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-        int forced[3] = {0, 0, 0};
-        if (const char* e = getenv("RVSP_HEAVY_GROUP"))
-            if (sscanf(e, "%d,%d,%d", &forced[0], &forced[1], &forced[2]) != 3)
-                forced[0] = forced[1] = forced[2] = 0;
         for (int cl = HEAVY_CW_LOG2_MIN; cl <= HEAVY_CW_LOG2_MAX; ++cl) {
             const void* fns[3] = {(const void*)k_heavy<COUNT>, (const void*)k_heavy<FILL>,
                                   (const void*)k_heavy<REUSE>};
             for (int m = 0; m < 3; ++m) {
-                int ctas[HEAVY_GROUP_MAX + 1] = {};
-                for (int g = HEAVY_GROUP_MAX; g >= 1; g >>= 1) {
-                    if (!heavy_fits(m, cl, g)) continue;
+                const size_t per = (size_t)heavy_smem_bytes(m, 1 << cl);
+                int best_w = 1, best_n = 1, best = 0;
+                for (int W = 1; W <= HEAVY_MAX_WARPS; ++W) {
+                    if (W * per > (size_t)HEAVY_SMEM_MAX) break;
                     int n = 0;
-                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                            &n, fns[m], g * 32, heavy_grp_smem_bytes(m, 1 << cl, g)) != cudaSuccess) {
+                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fns[m], W * 32, W * per) !=
+                        cudaSuccess) {
                         cudaGetLastError();
-                        n = 0;
+                        continue;
                     }
-                    ctas[g] = n;
-                }
-                int pick = 1;
-                for (int g = m == COUNT ? HEAVY_GROUP_MAX : 2; g >= 1; g >>= 1)
-                    if (ctas[g] > 0) {
-                        pick = g;
-                        break;
+                    if (n * W > best) {
+                        best = n * W;
+                        best_w = W;
+                        best_n = n;
                     }
-                const int f = forced[m];
-                if (f > 0 && HEAVY_GROUP_MAX % f == 0 && ctas[f] > 0) pick = f;
-                g_heavy_g[m][cl] = pick;
-                g_heavy_ctas[m][cl] = ctas[pick] > 0 ? ctas[pick] : 1;
-            }
-            const void* hfns[2] = {(const void*)k_hacc<COUNT>, (const void*)k_hacc<FILL>};
-            for (int m = 0; m < 2; ++m) {
-                int W = 8;
-                while (W > 1 && W * heavy_smem_bytes(m, 1 << cl) > HEAVY_SMEM_MAX) --W;
-                int n = 0;
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                        &n, hfns[m], W * 32, W * heavy_smem_bytes(m, 1 << cl)) != cudaSuccess) {
-                    cudaGetLastError();
-                    n = 1;
                 }
-                g_hacc_w[m][cl] = W;
-                g_hacc_ctas[m][cl] = n > 0 ? n : 1;
+                g_heavy_w[m][cl] = best_w;
+                g_heavy_ctas[m][cl] = best_n;
             }
         }
         cudaGetLastError();
@@ -354,10 +289,6 @@ static void launch_warp(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
 }
 
 template <int MODE>
-static void launch_heavy_buckets(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B,
-                                 const RowOut& o, const RowCtl& ctl);
-
-template <int MODE>
 static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B,
                         const RowOut& o) {
     const int32_t* rows = o.learned_bins ? plan->lbin_rows.as<int32_t>() : plan->bin_rows.as<int32_t>();
@@ -392,26 +323,21 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
                 default: launch_warp<4096, MODE>(plan, A, B, b, o); break;
             }
         } else if (plan->n_items > 0) {
+            KTime kt(plan->stream, plan->capturing, KF_HEAVY_COUNT + MODE);
             RowCtl ctl = o.ctl;
             if (o.learned_bins) ctl.only = plan->hmask.as<uint8_t>();  // rows kept heavy
-            if (MODE != REUSE && plan->hb_ok) {
-                launch_heavy_buckets<MODE == REUSE ? COUNT : MODE>(plan, A, B, o, ctl);
-                continue;
-            }
-            KTime kt(plan->stream, plan->capturing, KF_HEAVY_COUNT + MODE);
             const int cl = plan->params.heavy_cw_log2;
-            const int G = heavy_group(MODE, cl);
-            const int ngroups = plan->n_items / G;
+            const int W = g_heavy_w[MODE][cl];
             const int64_t fill = (int64_t)g_sms * g_heavy_ctas[MODE][cl];
-            const int grid = (int)std::min<int64_t>(ngroups, fill);
+            const int grid = (int)std::min<int64_t>((plan->n_items + W - 1) / W, fill);
             const HeavyAux aux{plan->bmeta.as<int4>(), plan->bdoff.as<int64_t>(),
                                plan->dir_ok ? plan->bdir.as<int32_t>() : nullptr,
                                plan->ameta_ok ? plan->ameta.as<int4>() : nullptr,
                                plan->ameta_ok ? plan->adoff.as<int32_t>() : nullptr};
             int32_t* queue = &plan->misc.as<Misc>()->heavy_queue;
             cudaMemsetAsync(queue, 0, sizeof(int32_t), plan->stream);
-            k_heavy<MODE><<<grid, G * 32, heavy_grp_smem_bytes(MODE, 1 << cl, G), plan->stream>>>(
-                A, B, plan->items.as<HeavyItem>(), ngroups, G, plan->item_cnt.as<int32_t>(),
+            k_heavy<MODE><<<grid, W * 32, W * heavy_smem_bytes(MODE, 1 << cl), plan->stream>>>(
+                A, B, plan->items.as<HeavyItem>(), plan->n_items, plan->item_cnt.as<int32_t>(),
                 o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, ctl, cl,
                 aux, queue);
             note_launch(plan, 1);
@@ -529,12 +455,10 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     AnalyzeOut out{plan->ops.as<int64_t>(), plan->ub.as<int32_t>(), plan->bin.as<uint8_t>(),
                    plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
                    features ? plan->feat.as<float4>() : nullptr, misc->hist,
-                   plan->tile_hist.as<int32_t>(), misc->totals, misc->bin_prod, &misc->max_nch,
-                   &misc->err};
+                   plan->tile_hist.as<int32_t>(), misc->totals, misc->bin_prod, &misc->err};
     {
         KTime kt(plan->stream, plan->capturing, KF_ANALYSIS);
-        k_analyze<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(
-            A, B, out, plan->params, HEAVY_GROUP_MAX);
+        k_analyze<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(A, B, out, plan->params);
     }
     note_launch(plan, 1);
     int st = scan_counts(plan, plan->tile_hist.as<int32_t>(), NUM_BINS * tiles, nullptr,
@@ -562,7 +486,6 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     ENS(plan->item_cnt, (size_t)plan->n_items * 4);
     ENS(plan->item_scan, ((size_t)plan->n_items + 1) * 8);
 #undef ENS
-    plan_heavy_buckets(plan);
     launch_bin_scatter(plan, plan->bin.as<uint8_t>(), plan->tile_off.as<int32_t>(),
                        plan->bin_rows.as<int32_t>(), true);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "analysis launch");
@@ -640,114 +563,9 @@ void launch_bin_scatter(rvsp_cuda_plan* plan, const uint8_t* bin, const int32_t*
     const int64_t M = plan->a_rows;
     Misc* misc = plan->misc.as<Misc>();
     KTime kt(plan->stream, plan->capturing, KF_ANALYSIS);
-    HeavyRowsOut hro{nullptr, nullptr, nullptr, nullptr, nullptr};
-    if (heavy_items && plan->hb_ok)
-        hro = HeavyRowsOut{plan->hnseg.as<int32_t>(), plan->hsbase.as<int32_t>(),
-                           plan->hbase.as<int64_t>(), &misc->seg_cursor, &misc->hist_cursor};
     k_bin_scatter<<<(unsigned)((M + AN_TILE - 1) / AN_TILE), AN_TILE, 0, plan->stream>>>(
         (int32_t)M, bin, tile_off, plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
-        bin_rows, &misc->item_cursor, heavy_items ? plan->items.as<HeavyItem>() : nullptr,
-        HEAVY_GROUP_MAX, plan->ops.as<int64_t>(), hro);
-    note_launch(plan, 1);
-}
-
-// Whether the analysed product's heavy rows take the bucketed COUNT / FILL
-// (HBuckets): they do when every heavy row has at most HB_NCH_MAX column
-// chunks and the bucket buffers fit (the bucketed columns and products take
-// 8 bytes per product of the heavy rows, within half the free memory);
-// otherwise the grouped kernel counts and fills them. Allocates the buffers.
-void plan_heavy_buckets(rvsp_cuda_plan* plan) {
-    plan->hb_ok = plan->hb_built = plan->hb_cols = plan->hb_vals = false;
-    if (plan->n_items <= 0) return;
-    const Misc& hm = plan->host_misc;
-    plan->hb_nsegs = (int32_t)std::min<int64_t>(hm.totals[2], INT32_MAX);
-    plan->hb_hist_n = hm.totals[3];
-    plan->hb_max_nch = hm.max_nch;
-    plan->hb_products = hm.bin_prod[BIN_HEAVY];
-    if (hm.max_nch <= 0 || hm.max_nch > HB_NCH_MAX || hm.totals[2] > INT32_MAX) return;
-    const int64_t M = plan->a_rows;
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
-        cudaGetLastError();
-        return;
-    }
-    const size_t need = 8 * (size_t)plan->hb_products + 12 * (size_t)plan->hb_hist_n +
-                        16 * (size_t)plan->hb_nsegs + 16 * (size_t)M;
-    if (need > free_b / 2) return;
-    plan->hb_ok = plan->hnseg.ensure(4 * (size_t)M) == cudaSuccess &&
-                  plan->hsbase.ensure(4 * (size_t)M) == cudaSuccess &&
-                  plan->hbase.ensure(8 * (size_t)M) == cudaSuccess &&
-                  plan->hsegs.ensure(sizeof(HSeg) * (size_t)plan->hb_nsegs) == cudaSuccess &&
-                  plan->hhist.ensure(4 * (size_t)plan->hb_hist_n) == cudaSuccess &&
-                  plan->hhoff.ensure(8 * ((size_t)plan->hb_hist_n + 1)) == cudaSuccess &&
-                  plan->hpcol.ensure(4 * (size_t)plan->hb_products) == cudaSuccess &&
-                  plan->hpval.ensure(4 * (size_t)plan->hb_products) == cudaSuccess &&
-                  plan->scan_tmp.ensure(8 * (size_t)((plan->hb_hist_n + SCAN_TILE - 1) /
-                                                     SCAN_TILE)) == cudaSuccess;
-    cudaGetLastError();  // a refused allocation only means the grouped kernel
-}
-
-// Bucketed COUNT / FILL of the heavy rows (MODE COUNT or FILL): the bucket
-// layout once per analysis (segments, histogram, scan), the columns once per
-// analysis, the products whenever the values may have changed, then one warp
-// per work item.
-template <int MODE>
-static void launch_heavy_buckets(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B,
-                                 const RowOut& o, const RowCtl& ctl) {
-    Misc* misc = plan->misc.as<Misc>();
-    const int cl = plan->params.heavy_cw_log2;
-    const int nch = plan->hb_max_nch;
-    HBuckets hb{plan->hnseg.as<int32_t>(), plan->hbase.as<int64_t>(),
-                plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
-                plan->hsegs.as<HSeg>(), plan->hb_nsegs, plan->hhist.as<int32_t>(),
-                plan->hhoff.as<int64_t>(), plan->hpcol.as<int32_t>(), plan->hpval.as<float>()};
-    const int64_t seg_grid = std::min<int64_t>(((int64_t)plan->hb_nsegs + HB_WARPS - 1) / HB_WARPS,
-                                               (int64_t)g_sms * 16);
-    if (!plan->hb_built) {
-        const int32_t nh = plan->bin_count[BIN_HEAVY];
-        KTime kt(plan->stream, plan->capturing, KF_HEAVY_BUCKETS);
-        {
-            k_hsegs<<<(unsigned)(((int64_t)nh * 32 + 255) / 256), 256, 0, plan->stream>>>(
-                A, B, plan->bin_rows.as<int32_t>() + plan->offs.off[BIN_HEAVY], nh,
-                plan->hnseg.as<int32_t>(), plan->hsbase.as<int32_t>(), plan->hsegs.as<HSeg>(),
-                &misc->err);
-        }
-        {
-            k_hhist<<<(unsigned)seg_grid, HB_WARPS * 32, HB_WARPS * 4 * nch, plan->stream>>>(
-                A, B, hb, cl, nch, &misc->err);
-        }
-        note_launch(plan, 2);
-        // cannot fail: plan_heavy_buckets sized the scan's workspace
-        scan_counts(plan, plan->hhist.as<int32_t>(), plan->hb_hist_n, plan->hhoff.as<int64_t>(),
-                    nullptr, &misc->hb_total);
-        plan->hb_built = true;
-    }
-    const bool cols = !plan->hb_cols, vals = MODE == FILL && !plan->hb_vals;
-    if (cols || vals) {
-        KTime kt(plan->stream, plan->capturing, KF_HEAVY_SCATTER);
-        const size_t sm = (size_t)HB_WARPS * 16 * nch;
-        if (cols && vals)
-            k_hscatter<true, true><<<(unsigned)seg_grid, HB_WARPS * 32, sm, plan->stream>>>(
-                A, B, hb, cl, nch, &misc->err);
-        else if (cols)
-            k_hscatter<true, false><<<(unsigned)seg_grid, HB_WARPS * 32, sm, plan->stream>>>(
-                A, B, hb, cl, nch, &misc->err);
-        else
-            k_hscatter<false, true><<<(unsigned)seg_grid, HB_WARPS * 32, sm, plan->stream>>>(
-                A, B, hb, cl, nch, &misc->err);
-        note_launch(plan, 1);
-        plan->hb_cols = true;
-        if (MODE == FILL) plan->hb_vals = true;
-    }
-    KTime kt(plan->stream, plan->capturing, KF_HEAVY_COUNT + MODE);
-    const int W = g_hacc_w[MODE][cl];
-    const int64_t fill = (int64_t)g_sms * g_hacc_ctas[MODE][cl];
-    const int grid = (int)std::min<int64_t>(((int64_t)plan->n_items + W - 1) / W, fill);
-    int32_t* queue = &misc->heavy_queue;
-    cudaMemsetAsync(queue, 0, sizeof(int32_t), plan->stream);
-    k_hacc<MODE><<<grid, W * 32, W * heavy_smem_bytes(MODE, 1 << cl), plan->stream>>>(
-        B, hb, plan->items.as<HeavyItem>(), plan->n_items, plan->item_cnt.as<int32_t>(), o.cnt,
-        plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, ctl, cl, queue);
+        bin_rows, &misc->item_cursor, heavy_items ? plan->items.as<HeavyItem>() : nullptr);
     note_launch(plan, 1);
 }
 
@@ -918,7 +736,7 @@ const char* rvsp_cuda_kernel_family(int32_t i) {
     static const char* names[KF_NUM] = {
         "k_tiny<COUNT>", "k_tiny<FILL>", "k_tiny_reuse", "k_warp<COUNT>", "k_warp<FILL>",
         "k_warp_reuse", "k_heavy<COUNT>", "k_heavy<FILL>", "k_heavy<REUSE>", "analysis",
-        "scan", "learned_sizing", "k_compact", "heavy_buckets", "heavy_scatter"};
+        "scan", "learned_sizing", "k_compact"};
     return i >= 0 && i < KF_NUM ? names[i] : nullptr;
 }
 
@@ -961,8 +779,7 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
                       &p->list_off, &p->lbin, &p->lcap, &p->ltile_hist, &p->ltile_off,
                       &p->lbin_rows, &p->need, &p->pflag, &p->hmask, &p->hovf,
                       &p->item_off, &p->bmeta, &p->bdcount, &p->bdscan, &p->bdoff, &p->bdir,
-                      &p->ameta, &p->adoff, &p->hnseg, &p->hsbase, &p->hbase, &p->hsegs,
-                      &p->hhist, &p->hhoff, &p->hpcol, &p->hpval};
+                      &p->ameta, &p->adoff};
     for (DevBuf* b : bufs) b->release();
     if (p->side) {
         cudaStreamSynchronize(p->side);
@@ -1111,7 +928,6 @@ int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t*
     if (!plan || !a_rp || !b_rp || !c_rp || !c_ci || !c_v) return RVSP_ERROR_NULL_POINTER;
     if (!a_ci || !a_v || !b_ci || !b_v) return RVSP_ERROR_NULL_POINTER;
     if (!plan->analysed) return RVSP_ERROR_INVALID_ARGUMENT;
-    plan->hb_vals = false;  // the operands' values may have changed since the last fill
     cudaError_t e;
     const int64_t M = plan->a_rows, nnz = plan->c_nnz;
     const bool dev_rp = is_dev(c_rp), dev_ci = is_dev(c_ci), dev_v = is_dev(c_v);

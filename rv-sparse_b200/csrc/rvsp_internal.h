@@ -29,11 +29,7 @@ struct DevBuf {
 struct Misc {
     int32_t hist[NUM_BINS];    // rows per bin
     int32_t cursor[NUM_BINS];  // bin scatter cursors
-    int64_t totals[4];         // heavy items, products, heavy-row segments, bucket entries
-    int32_t max_nch;           // most column chunks of a heavy row
-    int32_t seg_cursor;        // heavy-row segment allocation cursor
-    unsigned long long hist_cursor;  // heavy-row histogram allocation cursor
-    int64_t hb_total;          // bucketed products (scan total)
+    int64_t totals[2];         // heavy items, products
     int32_t item_cursor;
     int32_t overflow;          // a 32-bit row pointer would overflow
     int64_t scan_total;        // nnz(C)
@@ -103,8 +99,6 @@ enum KernelFamily : int {
     KF_SCAN,      // prefix sums
     KF_LEARNED,   // inference, predicted bins, re-run masks
     KF_COMPACT,   // slot -> C copies of the learned path
-    KF_HEAVY_BUCKETS,  // heavy rows' segments, product histogram and its scan
-    KF_HEAVY_SCATTER,  // heavy rows' products into their chunk buckets
     KF_NUM
 };
 bool ktime_enabled();
@@ -190,15 +184,6 @@ struct rvsp_cuda_plan {
     rvsp::DevBuf hmask, hovf, item_off;
     int64_t pool_cap = 0;
 
-    // heavy rows bucketed by column chunk (HBuckets): per-row segment count,
-    // first segment and first histogram entry, the segments, the histogram
-    // and its scan, the bucketed columns and products; hb_ok when the
-    // analysed product takes this path, then built / cols / vals say which
-    // parts are current (the values for the operand values last scattered)
-    rvsp::DevBuf hnseg, hsbase, hbase, hsegs, hhist, hhoff, hpcol, hpval;
-    bool hb_ok = false, hb_built = false, hb_cols = false, hb_vals = false;
-    int32_t hb_nsegs = 0, hb_max_nch = 0;
-    int64_t hb_hist_n = 0, hb_products = 0;
     bool heavy_slots = false;  // the last learned analysis sized heavy rows by prediction
 
     // numeric-only CUDA graph
@@ -221,7 +206,6 @@ int scan_counts(rvsp_cuda_plan* plan, const int32_t* in, int64_t n, int64_t* out
 void note_launch(rvsp_cuda_plan* plan, int n);
 void reset_graph(rvsp_cuda_plan* plan);
 int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B);
-void plan_heavy_buckets(rvsp_cuda_plan* plan);
 void launch_bin_scatter(rvsp_cuda_plan* plan, const uint8_t* bin, const int32_t* tile_off,
                         int32_t* bin_rows, bool heavy_items);
 int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool fused);

@@ -11,9 +11,8 @@
 //                  (row, column-chunk) work items
 //   k_tiny<MODE>   thread per row, rows with <= 32 products
 //   k_warp<CAP,..> warp per row, shared-memory hash table of CAP slots
-//   k_heavy<..>    CTA per (row, group of column chunks), a warp per chunk:
-//                  dense shared-memory accumulator + occupancy bitmap over
-//                  CW columns, B-row lookups shared by the group
+//   k_heavy<..>    warp per (row, column chunk), dense shared-memory
+//                  accumulator + occupancy bitmap over CW columns
 //   k_scan_*       exclusive scan of row counts into C's row pointer
 //
 // Each row kernel runs in one of three modes:
@@ -143,10 +142,8 @@ struct AnalyzeOut {
     float4* feat;        // [rows] learned-model features (optional)
     int32_t* hist;       // [NUM_BINS] rows per bin
     int32_t* tile_hist;  // [NUM_BINS][tiles] rows per bin per tile (stable binning)
-    int64_t* totals;     // [0] heavy items, [1] products, [2] heavy-row segments,
-                         // [3] heavy-row bucket histogram entries
+    int64_t* totals;     // [0] heavy items, [1] products
     int64_t* bin_prod;   // [NUM_BINS] products per bin
-    int32_t* max_nch;    // most column chunks of a heavy row
     int32_t* err;        // ERR_* bits
 };
 
@@ -180,7 +177,7 @@ __device__ __forceinline__ void warp_bin_add(int key, int nkeys, unsigned long l
 constexpr int AN_SHORT = 32;
 
 __global__ void __launch_bounds__(AN_TILE)
-    k_analyze(CsrView A, CsrView B, AnalyzeOut out, BinParams P, int heavy_group) {
+    k_analyze(CsrView A, CsrView B, AnalyzeOut out, BinParams P) {
     __shared__ int32_t s_rp[AN_TILE + 1];
     __shared__ unsigned long long s_ops[AN_TILE];
     __shared__ int32_t s_maxlen[AN_TILE];
@@ -188,7 +185,7 @@ __global__ void __launch_bounds__(AN_TILE)
     __shared__ int32_t s_maxc[AN_TILE];
     __shared__ int32_t s_hist[NUM_BINS];
     __shared__ unsigned long long s_bprod[NUM_BINS];
-    __shared__ unsigned long long s_items, s_prod, s_segs, s_hent;
+    __shared__ unsigned long long s_items, s_prod;
     __shared__ int s_long;
 
     const int r0 = blockIdx.x * AN_TILE;
@@ -202,8 +199,6 @@ __global__ void __launch_bounds__(AN_TILE)
     if (t == 0) {
         s_items = 0;
         s_prod = 0;
-        s_segs = 0;
-        s_hent = 0;
         s_long = 0;
     }
     __syncthreads();
@@ -293,21 +288,10 @@ __global__ void __launch_bounds__(AN_TILE)
     }
     warp_bin_add(b, NUM_BINS, (unsigned long long)ops, s_hist, s_bprod);
     const unsigned long long wprod = warp_sum64((unsigned long long)ops);
-    // a heavy row's items are padded to whole groups of the heavy kernel
-    const int nitems = (nch + heavy_group - 1) / heavy_group * heavy_group;
-    const unsigned long long witems = warp_sum64((unsigned long long)nitems);
-    // heavy rows' bucket layout: segments of about HB_SEG products, and a
-    // histogram entry per (chunk, segment)
-    const int nseg = nch > 0 ? (int)max((int64_t)1, (ops + HB_SEG - 1) / HB_SEG) : 0;
-    const unsigned long long wsegs = warp_sum64((unsigned long long)nseg);
-    const unsigned long long whent = warp_sum64((unsigned long long)nch * (unsigned long long)nseg);
-    const int wmaxnch = __reduce_max_sync(FULL, (unsigned)nch);
-    if (lane_id() == 0 && wmaxnch > 0) atomicMax(out.max_nch, wmaxnch);
+    const unsigned long long witems = warp_sum64((unsigned long long)nch);
     if (lane_id() == 0) {
         if (wprod) atomicAdd(&s_prod, wprod);
         if (witems) atomicAdd(&s_items, witems);
-        if (wsegs) atomicAdd(&s_segs, wsegs);
-        if (whent) atomicAdd(&s_hent, whent);
     }
     __syncthreads();
     if (t < NUM_BINS) {
@@ -317,21 +301,9 @@ __global__ void __launch_bounds__(AN_TILE)
     }
     if (t == 0) {
         if (s_items) atomicAdd((unsigned long long*)&out.totals[0], s_items);
-        if (s_segs) atomicAdd((unsigned long long*)&out.totals[2], s_segs);
-        if (s_hent) atomicAdd((unsigned long long*)&out.totals[3], s_hent);
         atomicAdd((unsigned long long*)&out.totals[1], s_prod);
     }
 }
-
-// Where k_bin_scatter records the heavy rows' bucket layout (all null: not
-// recorded).
-struct HeavyRowsOut {
-    int32_t* nseg;                    // [rows] segments of each heavy row
-    int32_t* sbase;                   // [rows] first segment
-    int64_t* hbase;                   // [rows] first histogram entry
-    int32_t* seg_cursor;
-    unsigned long long* hist_cursor;
-};
 
 // Stable partition of rows by bin: tile_off[b * tiles + tile] is where the
 // tile's rows of bin b start in bin_rows (an exclusive scan of tile_hist), so
@@ -341,8 +313,7 @@ __global__ void __launch_bounds__(AN_TILE)
     k_bin_scatter(int32_t rows, const uint8_t* __restrict__ bin,
                   const int32_t* __restrict__ tile_off, const int32_t* __restrict__ chunk_lo,
                   const int32_t* __restrict__ nchunks, int32_t* __restrict__ bin_rows,
-                  int32_t* __restrict__ item_cursor, HeavyItem* __restrict__ items,
-                  int heavy_group, const int64_t* __restrict__ ops, HeavyRowsOut hro) {
+                  int32_t* __restrict__ item_cursor, HeavyItem* __restrict__ items) {
     __shared__ int32_t s_wc[AN_TILE / 32][NUM_BINS];
     const int t = threadIdx.x, lane = lane_id(), warp = t >> 5;
     const int row = blockIdx.x * AN_TILE + t;
@@ -359,21 +330,10 @@ __global__ void __launch_bounds__(AN_TILE)
                     __popc(peers & ((1u << lane) - 1));
     bin_rows[pos] = row;
     if (b == BIN_HEAVY && items) {
-        // whole groups of heavy_group items (the cursor stays a multiple of
-        // it), the padding items marked by chunk -1
         const int n = nchunks[row];
-        const int padded = (n + heavy_group - 1) / heavy_group * heavy_group;
-        const int first = atomicAdd(item_cursor, padded);
+        const int first = atomicAdd(item_cursor, n);
         const int lo = chunk_lo[row];
-        for (int c = 0; c < padded; ++c)
-            items[first + c] = HeavyItem{row, c < n ? lo + c : -1, first, 0};
-        if (hro.nseg) {  // the row's segments and histogram entries (k_analyze's rule)
-            const int ns = (int)max((int64_t)1, (ops[row] + HB_SEG - 1) / HB_SEG);
-            hro.nseg[row] = ns;
-            hro.sbase[row] = atomicAdd(hro.seg_cursor, ns);
-            hro.hbase[row] = (int64_t)atomicAdd(hro.hist_cursor,
-                                                (unsigned long long)n * (unsigned long long)ns);
-        }
+        for (int c = 0; c < n; ++c) items[first + c] = HeavyItem{row, lo + c, first, 0};
     }
 }
 
@@ -1568,45 +1528,29 @@ __device__ __forceinline__ void heavy_finish(
     __syncwarp();
 }
 
-// Heavy rows, grouped. The work items are (row, column chunk) pairs, each
-// row's items padded to a multiple of the group size G (padding items have
-// chunk -1), so G consecutive items never cross rows. One CTA of G warps
-// takes a group at a time from a counter; warp w owns the group's chunk w
-// (its accumulator and bitmap), so every column is still added by one warp
-// in A-row order. The A row is walked 32 * G entries at a time: first each
-// thread looks up one entry's B row once for the whole group and stages the
-// G + 1 positions where its B row crosses the group's chunk boundaries
-// (from the B row's chunk directory, a short scan of a short row, or a
-// binary search), then each warp walks its own chunk's segments from that
-// staging in shared memory. The expensive lookup is paid once per (A entry,
-// group) instead of once per (A entry, chunk).
-constexpr int HEAVY_GROUP_MAX = 8;
-
-// Shared memory of the staging: per entry of a batch (32 * G entries) its
-// G + 1 boundary positions and its A value.
-__host__ __device__ constexpr int heavy_stage_bytes(int g) {
-    return 32 * g * (g + 1) * 4 + 32 * g * 4;
-}
-__host__ __device__ constexpr int heavy_grp_smem_bytes(int mode, int cw, int g) {
-    return heavy_stage_bytes(g) + g * heavy_smem_bytes(mode, cw);
-}
+// Heavy rows: one warp per work item (row, chunk of cw = 2^cw_log2
+// columns), items pulled one at a time from a counter by a grid that fills
+// the GPU once (a warp that drew a light item takes the next one instead of
+// idling beside a heavy one). The warp walks the row's A entries 32 at a
+// time; each lane finds the part of its B row that falls in the chunk from
+// the B row's metadata and, for long rows, its column-chunk directory (a
+// binary search otherwise), and heavy_segments accumulates the segments in
+// A-row order. The A row is re-read once per chunk; the products once in
+// all.
+constexpr int HEAVY_MAX_WARPS = 32;
 
 template <int MODE>
-__global__ void __launch_bounds__(HEAVY_GROUP_MAX * 32)
-    k_heavy(CsrView A, CsrView B, const HeavyItem* __restrict__ items, int ngroups, int G,
+__global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
+    k_heavy(CsrView A, CsrView B, const HeavyItem* __restrict__ items, int nitems,
             int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
             const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
             int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err,
             RowCtl ctl, int cw_log2, HeavyAux aux, int32_t* __restrict__ queue) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_group;
     const int cw = 1 << cw_log2;
     const int nw = cw >> 5;  // bitmap words
-    const int warp = threadIdx.x >> 5, lane = lane_id(), t = threadIdx.x;
-    const int E = 32 * G, SP = G + 1;
-    int32_t* split = reinterpret_cast<int32_t*>(smem);             // [E][G + 1]
-    float* s_av = reinterpret_cast<float*>(smem + 4 * E * SP);     // [E]
-    unsigned char* mine = smem + heavy_stage_bytes(G) + warp * heavy_smem_bytes(MODE, cw);
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    unsigned char* mine = smem + warp * heavy_smem_bytes(MODE, cw);
     float* acc = reinterpret_cast<float*>(mine);
     unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * cw));
 
@@ -1619,318 +1563,6 @@ __global__ void __launch_bounds__(HEAVY_GROUP_MAX * 32)
     }
     if (MODE != REUSE)
         for (int x = lane; x < nw; x += 32) bits[x] = 0u;
-    for (;;) {
-        __syncthreads();  // the previous group's staging is no longer read
-        if (t == 0) s_group = atomicAdd(queue, 1);
-        __syncthreads();
-        const int gi = s_group;
-        if (gi >= ngroups) break;
-        const int i0 = gi * G;
-        const HeavyItem head = items[i0];
-        const int row = head.row;
-        if (head.chunk < 0 || (ctl.only && !ctl.only[row])) continue;  // CTA-uniform
-        const int w = i0 + warp;  // this warp's item
-        const HeavyItem it = items[w];
-        const bool active = it.chunk >= 0;  // warp-uniform
-        const int lo = active ? it.chunk << cw_log2 : 0;
-        if (MODE == REUSE && active) {
-            float4* a4 = reinterpret_cast<float4*>(acc);
-            for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
-            __syncwarp();
-        }
-        int a0, a1;
-        row_range(A, row, &a0, &a1, err);
-        for (int base = a0; base < a1; base += E) {
-            // stage: thread t looks up entry base + t for the whole group
-            {
-                const int j = base + t;
-                int32_t* sp = split + t * SP;
-                int4 m = make_int4(0, 0, 0, -1);
-                int64_t d = -1;
-                float av = 0.0f;
-                if (j < a1) {
-                    if (aux.ameta) {
-                        m = aux.ameta[j];
-                        if (aux.dir) d = aux.adoff[j];
-                    } else {
-                        const int k = A.ci[j];
-                        if ((unsigned)k >= (unsigned)B.rows) {
-                            atomicOr(err, ERR_STRUCTURE);
-                        } else {
-                            m = aux.meta[k];
-                            if (aux.dir) d = aux.doff[k];
-                        }
-                    }
-                    if (MODE != COUNT) av = A.v[j];
-                }
-                s_av[t] = av;
-                const int fc = m.z >> cw_log2;
-                int q = m.x;  // monotone cursor of the scan / search
-                for (int b = 0; b <= G; ++b) {
-                    const int64_t X = (int64_t)(head.chunk + b) << cw_log2;  // boundary column
-                    int pos;
-                    if (m.y <= m.x || X <= m.z) {
-                        pos = m.x;
-                    } else if (X > m.w) {
-                        pos = m.y;
-                    } else if (d >= 0) {
-                        // the chunk directory: first position at or past the
-                        // start of chunk head.chunk + b (inside the row's chunks)
-                        pos = aux.dir[d + (head.chunk + b - fc)];
-                        pos = min(max(pos, m.x), m.y);  // only a broken operand is outside
-                    } else if (m.y - m.x <= 32) {
-                        while (q < m.y && __ldg(B.ci + q) < X) ++q;
-                        pos = q;
-                    } else {
-                        q = seq_lower_bound(B.ci, q, m.y, (int)X);
-                        pos = q;
-                    }
-                    sp[b] = pos;
-                }
-            }
-            __syncthreads();
-            if (active) {
-                const int ne = min(E, a1 - base);
-                for (int sub = 0; sub < ne; sub += 32) {
-                    const int e = sub + lane;
-                    int s = 0, len = 0;
-                    float av = 0.0f;
-                    if (e < ne) {
-                        s = split[e * SP + warp];
-                        len = max(split[e * SP + warp + 1] - s, 0);
-                        av = s_av[e];
-                    }
-                    if (__any_sync(FULL, len > 0))
-                        heavy_segments<MODE>(B, s, len, av, lo, cw, acc, bits, err);
-                }
-            }
-            __syncthreads();
-        }
-        if (!active) {
-            if (MODE == COUNT && lane == 0) item_cnt[w] = 0;  // padding item
-            continue;
-        }
-        heavy_finish<MODE>(B, w, it, row, lo, cw, acc, bits, item_cnt, row_cnt, item_scan, c_rp,
-                           c_ci, c_v, err, ctl);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Heavy rows, bucketed by column chunk (COUNT and FILL). A warp walking a
-// heavy row's A entries once per chunk pays for every (entry, chunk) pair,
-// which on power-law products (hundreds of entries, under one product per
-// entry and chunk) costs more than the products themselves. Here every heavy
-// row is cut into segments of about HB_SEG products (consecutive A entries);
-// per segment one warp
-//   k_hhist     counts the segment's products per column chunk of its row
-//   (scan)      the counts, chunk-major then segment, become bucket offsets:
-//               chunk c of a row gets one contiguous bucket in which the
-//               segments' products follow each other in A-row order
-//   k_hscatter  walks the segment again in the reference's product order and
-//               writes each product's column (and its rounded product a*b)
-//               to its chunk's bucket; lanes of one step that go to the same
-//               chunk are ranked in lane order, so every bucket keeps the
-//               products of its chunk in A-row order
-// and per work item (row, chunk) one warp
-//   k_hacc      reads its bucket (contiguous, coalesced) into the presence
-//               bitmap (COUNT, FILL) and the accumulator from +0.0f (FILL,
-//               same-column products of a step combined in lane order), then
-//               ends the item like the grouped kernel (heavy_finish).
-// Every A entry is walked twice in all (three times with a separate value
-// scatter), whatever the number of chunks; values keep the reference's order.
-// ---------------------------------------------------------------------------
-constexpr int HB_WARPS = 2;         // warps per CTA of k_hhist / k_hscatter
-
-struct HSeg {
-    int32_t row;
-    int32_t e0, e1;  // A entries [e0, e1)
-    int32_t k;       // segment index within its row
-};
-
-// Bucket layout of a plan's heavy rows.
-struct HBuckets {
-    const int32_t* nseg;     // [rows] segments of each heavy row
-    const int64_t* hbase;    // [rows] first histogram entry of each heavy row
-    const int32_t* chunk_lo; // [rows] first column chunk of each heavy row
-    const int32_t* nchunks;  // [rows] column chunks of each heavy row
-    const HSeg* segs;
-    int32_t nsegs;
-    int32_t* hist;           // [H] products per (row, chunk, segment), chunk-major
-    const int64_t* hoff;     // [H + 1] exclusive scan of hist: bucket starts
-    int32_t* pcol;           // [products of the heavy rows] bucketed columns
-    float* pval;             //   and rounded products a*b
-};
-
-// Segments of the heavy rows: one warp per row. Entry j belongs to segment
-// min(P(j) / HB_SEG, nseg - 1), P(j) the products of the row's entries
-// before j, so segments are contiguous entry ranges (an entry with more than
-// HB_SEG products leaves empty segments behind it).
-__global__ void __launch_bounds__(256)
-    k_hsegs(CsrView A, CsrView B, const int32_t* __restrict__ rows, int32_t n,
-            const int32_t* __restrict__ nseg, const int32_t* __restrict__ sbase,
-            HSeg* __restrict__ segs, int32_t* __restrict__ err) {
-    const int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = lane_id();
-    if (wg >= n) return;
-    const int row = rows[wg];
-    int a0, a1;
-    row_range(A, row, &a0, &a1, err);
-    const int ns = nseg[row];
-    HSeg* sg = segs + sbase[row];
-    if (lane == 0) sg[0].e0 = a0;
-    long long run = 0;  // products of the entries before this batch
-    int prev = 0;       // segment of the entry before this batch
-    for (int base = a0; base < a1; base += 32) {
-        const int j = base + lane;
-        long long len = 0;
-        if (j < a1) {
-            int bs, be;
-            row_range(B, A.ci[j], &bs, &be, err);
-            len = be - bs;
-        }
-        long long incl = len;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const long long y = __shfl_up_sync(FULL, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const long long pj = run + incl - len;
-        const int sj = j < a1 ? (int)min(pj / HB_SEG, (long long)ns - 1) : ns - 1;
-        int p = __shfl_up_sync(FULL, sj, 1);
-        if (lane == 0) p = prev;
-        if (j < a1)
-            for (int k = p + 1; k <= sj; ++k) sg[k].e0 = j;  // segments starting at entry j
-        const int last = min(31, a1 - 1 - base);
-        run += __shfl_sync(FULL, incl, 31);
-        prev = __shfl_sync(FULL, sj, last);
-    }
-    if (lane == 0)
-        for (int k = prev + 1; k < ns; ++k) sg[k].e0 = a1;
-    __syncwarp();
-    for (int k = lane; k < ns; k += 32) {
-        sg[k].row = row;
-        sg[k].k = k;
-        sg[k].e1 = k + 1 < ns ? sg[k + 1].e0 : a1;
-    }
-}
-
-// Products per (row, chunk, segment): one warp per segment, a shared
-// histogram of the row's chunks (nch_max ints per warp).
-__global__ void __launch_bounds__(HB_WARPS * 32)
-    k_hhist(CsrView A, CsrView B, HBuckets hb, int cw_log2, int nch_max,
-            int32_t* __restrict__ err) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = lane_id();
-    int32_t* h = reinterpret_cast<int32_t*>(smem) + warp * nch_max;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < hb.nsegs;
-         s += nwarps) {
-        const HSeg sg = hb.segs[s];
-        const int clo = hb.chunk_lo[sg.row], nch = hb.nchunks[sg.row];
-        if (nch > nch_max) {  // not a heavy row of this layout (a broken plan)
-            if (lane == 0) atomicOr(err, ERR_STRUCTURE);
-            continue;
-        }
-        for (int c = lane; c < nch; c += 32) h[c] = 0;
-        __syncwarp();
-        walk_products<false>(A, B, sg.e0, sg.e1, err,
-                             [&](int, bool pv, int col, float, float, bool) {
-                                 if (pv) {
-                                     const int c = (col >> cw_log2) - clo;
-                                     if ((unsigned)c < (unsigned)nch) atomicAdd(&h[c], 1);
-                                     else atomicOr(err, ERR_STRUCTURE);
-                                 }
-                                 return false;
-                             });
-        __syncwarp();
-        const int ns = hb.nseg[sg.row];
-        const int64_t base = hb.hbase[sg.row] + sg.k;
-        for (int c = lane; c < nch; c += 32) hb.hist[base + (int64_t)c * ns] = h[c];
-        __syncwarp();
-    }
-}
-
-// Bucketed products: one warp per segment walks it again in product order;
-// the segment's part of every chunk bucket [start, end) is held in shared
-// memory (nch_max pairs of int64 per warp) and its start advances as the
-// products land. COLS writes the columns, VALS the rounded products.
-template <bool COLS, bool VALS>
-__global__ void __launch_bounds__(HB_WARPS * 32)
-    k_hscatter(CsrView A, CsrView B, HBuckets hb, int cw_log2, int nch_max,
-               int32_t* __restrict__ err) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = lane_id();
-    long long* cur = reinterpret_cast<long long*>(smem) + 2 * warp * nch_max;
-    long long* end = cur + nch_max;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < hb.nsegs;
-         s += nwarps) {
-        const HSeg sg = hb.segs[s];
-        const int clo = hb.chunk_lo[sg.row], nch = hb.nchunks[sg.row];
-        if (nch > nch_max) {
-            if (lane == 0) atomicOr(err, ERR_STRUCTURE);
-            continue;
-        }
-        const int ns = hb.nseg[sg.row];
-        const int64_t base = hb.hbase[sg.row] + sg.k;
-        for (int c = lane; c < nch; c += 32) {
-            cur[c] = hb.hoff[base + (int64_t)c * ns];
-            end[c] = hb.hoff[base + (int64_t)c * ns + 1];
-        }
-        __syncwarp();
-        walk_products<VALS>(A, B, sg.e0, sg.e1, err,
-                            [&](int, bool pv, int col, float bv, float av, bool) {
-                                int c = pv ? (col >> cw_log2) - clo : -1;
-                                if (pv && (unsigned)c >= (unsigned)nch) {
-                                    atomicOr(err, ERR_STRUCTURE);
-                                    pv = false;
-                                }
-                                const unsigned peers =
-                                    __match_any_sync(FULL, pv ? c : (0x40000000 | lane));
-                                const int leader = __ffs(peers) - 1;
-                                long long at = 0;
-                                if (pv && lane == leader) {
-                                    at = cur[c];
-                                    cur[c] = at + __popc(peers);
-                                }
-                                at = __shfl_sync(FULL, at, leader);
-                                const long long pos = at + __popc(peers & ((1u << lane) - 1));
-                                if (pv) {
-                                    if (pos < end[c]) {
-                                        if (COLS) hb.pcol[pos] = col;
-                                        if (VALS) hb.pval[pos] = __fmul_rn(av, bv);
-                                    } else {
-                                        atomicOr(err, ERR_STRUCTURE);
-                                    }
-                                }
-                                return false;
-                            });
-        __syncwarp();
-    }
-}
-
-// Work items from their buckets: one warp per item, items pulled from a
-// counter by a grid that fills the GPU once. COUNT and FILL only (REUSE
-// keeps the grouped kernel, which needs no bucketed products).
-template <int MODE>
-__global__ void __launch_bounds__(256)
-    k_hacc(const CsrView B, HBuckets hb, const HeavyItem* __restrict__ items, int nitems,
-           int32_t* __restrict__ item_cnt, int32_t* __restrict__ row_cnt,
-           const int64_t* __restrict__ item_scan, const int32_t* __restrict__ c_rp,
-           int32_t* __restrict__ c_ci, float* __restrict__ c_v, int32_t* __restrict__ err,
-           RowCtl ctl, int cw_log2, int32_t* __restrict__ queue) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int cw = 1 << cw_log2;
-    const int nw = cw >> 5;
-    const int warp = threadIdx.x >> 5, lane = lane_id();
-    unsigned char* mine = smem + warp * heavy_smem_bytes(MODE, cw);
-    float* acc = reinterpret_cast<float*>(mine);
-    unsigned* bits = reinterpret_cast<unsigned*>(mine + (MODE == COUNT ? 0 : 4 * cw));
-    if (MODE != COUNT) {
-        float4* a4 = reinterpret_cast<float4*>(acc);
-        for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    for (int x = lane; x < nw; x += 32) bits[x] = 0u;
     __syncwarp();
     for (;;) {
         int w = 0;
@@ -1938,41 +1570,58 @@ __global__ void __launch_bounds__(256)
         w = __shfl_sync(FULL, w, 0);
         if (w >= nitems) break;
         const HeavyItem it = items[w];
-        if (it.chunk < 0) {
-            if (MODE == COUNT && lane == 0) item_cnt[w] = 0;  // padding item
-            continue;
-        }
         const int row = it.row;
         if (ctl.only && !ctl.only[row]) continue;
         const int lo = it.chunk << cw_log2;
-        const int cl = it.chunk - hb.chunk_lo[row];
-        const int ns = hb.nseg[row];
-        const int64_t hi0 = hb.hbase[row] + (int64_t)cl * ns;
-        const long long q0 = hb.hoff[hi0], q1 = hb.hoff[hi0 + ns];
-        // two steps of 32 products loaded before either is accumulated
-        for (long long b0 = q0; b0 < q1; b0 += 64) {
-            const long long qa = b0 + lane, qb = b0 + 32 + lane;
-            int ca = -1, cb = -1;
-            float va = 0.0f, vb = 0.0f;
-            if (qa < q1) {
-                ca = hb.pcol[qa] - lo;
-                if (MODE != COUNT) va = hb.pval[qa];
-            }
-            if (qb < q1) {
-                cb = hb.pcol[qb] - lo;
-                if (MODE != COUNT) vb = hb.pval[qb];
-            }
-            const bool oka = qa < q1 && (unsigned)ca < (unsigned)cw;
-            const bool okb = qb < q1 && (unsigned)cb < (unsigned)cw;
-            if ((qa < q1 && !oka) || (qb < q1 && !okb)) atomicOr(err, ERR_STRUCTURE);
-            if (oka) atomicOr(&bits[ca >> 5], 1u << (ca & 31));
-            if (okb) atomicOr(&bits[cb >> 5], 1u << (cb & 31));
-            if (MODE != COUNT) {
-                ordered_add(acc, oka ? ca : 0, oka, va);
-                __syncwarp();
-                if (b0 + 32 < q1) ordered_add(acc, okb ? cb : 0, okb, vb);
-            }
+        const int hi = (int)min((int64_t)lo + cw, (int64_t)B.cols);
+        if (MODE == REUSE) {
+            float4* a4 = reinterpret_cast<float4*>(acc);
+            for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
             __syncwarp();
+        }
+        int a0, a1;
+        row_range(A, row, &a0, &a1, err);
+        for (int base = a0; base < a1; base += 32) {
+            const int j = base + lane;
+            int s = 0, len = 0;
+            float av = 0.0f;
+            if (j < a1) {
+                // {start, end, first column, last column} of B row A.ci[j],
+                // and its directory offset
+                int4 m = make_int4(0, 0, 0, -1);
+                int64_t d = -1;
+                if (aux.ameta) {
+                    m = aux.ameta[j];
+                    if (aux.dir) d = aux.adoff[j];
+                } else {
+                    const int k = A.ci[j];
+                    if ((unsigned)k >= (unsigned)B.rows) {
+                        atomicOr(err, ERR_STRUCTURE);
+                    } else {
+                        m = aux.meta[k];
+                        if (aux.dir) d = aux.doff[k];
+                    }
+                }
+                if (m.y > m.x && m.w >= lo && m.z < hi) {
+                    int t;
+                    if (d >= 0) {
+                        const int c = it.chunk - (m.z >> cw_log2);
+                        s = m.z >= lo ? m.x : aux.dir[d + c];
+                        t = m.w < hi ? m.y : aux.dir[d + c + 1];
+                        // only an unsorted row (a broken operand) leaves a
+                        // directory entry unwritten: stay inside the row
+                        s = min(max(s, m.x), m.y);
+                        t = min(max(t, s), m.y);
+                    } else {
+                        s = m.z >= lo ? m.x : seq_lower_bound(B.ci, m.x, m.y, lo);
+                        t = m.w < hi ? m.y : seq_lower_bound(B.ci, s, m.y, hi);
+                    }
+                    len = t - s;
+                    if (MODE != COUNT) av = A.v[j];
+                }
+            }
+            if (__any_sync(FULL, len > 0))
+                heavy_segments<MODE>(B, s, len, av, lo, cw, acc, bits, err);
         }
         heavy_finish<MODE>(B, w, it, row, lo, cw, acc, bits, item_cnt, row_cnt, item_scan, c_rp,
                            c_ci, c_v, err, ctl);

@@ -70,8 +70,7 @@ __host__ __device__ inline bool bin_params_valid(const BinParams& p) {
            p.heavy_cw_log2 >= HEAVY_CW_LOG2_MIN && p.heavy_cw_log2 <= HEAVY_CW_LOG2_MAX;
 }
 
-// Work item of the heavy kernel: a column chunk of a heavy row (chunk -1:
-// padding that completes the row's last group of chunks).
+// Work item of the heavy kernel: a column chunk of a heavy row.
 struct HeavyItem {
     int32_t row;
     int32_t chunk;
@@ -95,12 +94,6 @@ struct HeavyAux {
     const int32_t* adoff;
 };
 constexpr int DIR_MIN_LEN = 32;
-
-// Heavy rows bucketed by column chunk (COUNT and FILL): a heavy row is cut
-// into segments of about HB_SEG products, one warp each; the path takes
-// products whose heavy rows have at most HB_NCH_MAX column chunks.
-constexpr int HB_SEG = 1 << 16;
-constexpr int HB_NCH_MAX = 4096;
 
 struct BinOffsets {
     int32_t off[NUM_BINS];
