@@ -141,7 +141,8 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
                        const int32_t* __restrict__ ub, int32_t* __restrict__ cnt,
                        uint8_t* __restrict__ need, const uint8_t* __restrict__ hmask,
                        const uint8_t* __restrict__ hovf,
-                       int32_t* __restrict__ n_need, int64_t* __restrict__ stats) {
+                       int32_t* __restrict__ n_need, int32_t* __restrict__ n_need_heavy,
+                       int64_t* __restrict__ stats) {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
     bool nd = false, ovf = false, big = false, pr = false, under = false;
     int64_t fitc = 0, fitcap = 0, fitub = 0;
@@ -163,7 +164,7 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
     }
     const unsigned mn = __ballot_sync(FULL, nd), mo = __ballot_sync(FULL, ovf && pr),
                    mb = __ballot_sync(FULL, big), mp = __ballot_sync(FULL, pr),
-                   mu = __ballot_sync(FULL, under);
+                   mu = __ballot_sync(FULL, under), mh = __ballot_sync(FULL, nd && big);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         fitc += __shfl_xor_sync(FULL, fitc, o);
@@ -172,6 +173,7 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
     }
     if ((threadIdx.x & 31) == 0) {
         if (mn) atomicAdd(n_need, __popc(mn));
+        if (mh) atomicAdd(n_need_heavy, __popc(mh));
         if (mp) atomicAdd((unsigned long long*)&stats[0], (unsigned long long)__popc(mp));
         if (mo) atomicAdd((unsigned long long*)&stats[1], (unsigned long long)__popc(mo));
         if (mb) atomicAdd((unsigned long long*)&stats[2], (unsigned long long)__popc(mb));
@@ -412,7 +414,8 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
             (int32_t)M, plan->lbin.as<uint8_t>(), plan->pflag.as<uint8_t>(),
             plan->lcap.as<int32_t>(), plan->ub.as<int32_t>(), plan->cnt.as<int32_t>(),
             plan->need.as<uint8_t>(), hslots ? plan->hmask.as<uint8_t>() : nullptr,
-            hslots ? plan->hovf.as<uint8_t>() : nullptr, &misc->n_need, misc->lstats);
+            hslots ? plan->hovf.as<uint8_t>() : nullptr, &misc->n_need, &misc->n_need_heavy,
+            misc->lstats);
     }
     note_launch(plan, 1);
     // exact counts of the rows the sweep could not finish (tiny rows never overflow)
@@ -464,10 +467,14 @@ int learned_finish(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, int
     if (plan->host_misc.n_need > 0) {
         RowOut fo{nullptr, plan->c_rp.as<int32_t>(), c_ci, c_v, &misc->err, false};
         fo.ctl.only = plan->need.as<uint8_t>();
-        const int32_t tiny = plan->bin_count[BIN_TINY];
+        // tiny rows never need it; heavy rows only when one of them did (the
+        // heavy kernel would otherwise pull every work item just to skip it)
+        const int32_t tiny = plan->bin_count[BIN_TINY], items = plan->n_items;
         plan->bin_count[BIN_TINY] = 0;
+        if (plan->host_misc.n_need_heavy == 0) plan->n_items = 0;
         run_rows(plan, FILL, A, B, fo);
         plan->bin_count[BIN_TINY] = tiny;
+        plan->n_items = items;
     }
     const int32_t* lrows = plan->lbin_rows.as<int32_t>();
     const int32_t nt = plan->lcount[BIN_TINY];

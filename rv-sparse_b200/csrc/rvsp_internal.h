@@ -44,7 +44,7 @@ struct Misc {
     int64_t list_total;        // scratch total of the product-offset scan
     int32_t lhist[NUM_BINS];   // learned path: rows per predicted-capacity bin
     int32_t n_need;            // learned path: rows sent to the exact path
-    int32_t pad3;
+    int32_t n_need_heavy;      //   of which heavy rows
     int64_t slot_total;        // learned path: sum of predicted capacities
     int64_t lstats[8];         // learned path statistics (see rvsp_cuda_plan_learned_stats)
     int64_t ltile_total;
