@@ -206,3 +206,59 @@ def test_trained_model_gains_over_upper_bound(gpu_lib):
         want = oneshot(M, M, algo=rv.RVSP_CUDA_ALGO_EXACT)
         got = oneshot(M, M, algo=rv.RVSP_CUDA_ALGO_LEARNED)
         assert np.array_equal(got[1], want[1]) and np.array_equal(bits(got[2]), bits(want[2]))
+
+
+@pytest.mark.skipif(not os.path.exists(SHIPPED), reason="no trained checkpoint shipped yet")
+def test_trained_model_saves_time_on_a_power_law_product(gpu_lib):
+    """What the trained network gains in time: on a power-law product (a row
+    panel of R-MAT 2^18, heavy rows holding almost every product) the learned
+    path fills C in one sweep into slots the network sizes, so it skips the
+    count pass the exact path makes, and must finish faster (median of 5 one-
+    shot products each) with C bit-identical. Without the network the only
+    safe slot of a row is its upper bound min(products, cols): the predicted
+    slots must take less (fit_capacity below fit_upper_bound)."""
+    import time
+
+    import torch
+
+    from rvsp_b200 import ranks
+    L = rv.lib()
+    assert L.rvsp_cuda_mlp_load(SHIPPED.encode()) == 0
+    R = gen.rmat(scale=18, edge_factor=16, seed=0)
+    ops = gen.row_products(R, R)
+    r0, r1 = ranks.row_panels(ops)[0]
+    dR = DevCSR(R)
+
+    def run(algo):
+        import ctypes as C
+        prp, pci, pv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        nnz = C.c_int32()
+        rv.check(L.rvsp_cuda_spgemm_f32(algo, r1 - r0, R.cols, R.cols,
+                                        rv.ptr(dR.row_ptr[r0:r1 + 1]), rv.ptr(dR.col_idx),
+                                        rv.ptr(dR.values), rv.ptr(dR.row_ptr), rv.ptr(dR.col_idx),
+                                        rv.ptr(dR.values), C.byref(prp), C.byref(pci),
+                                        C.byref(pv), C.byref(nnz), None))
+        return (prp.value, pci.value, pv.value), nnz.value
+
+    from gpu_util import d2h
+    times, outs = {}, {}
+    for algo in (rv.RVSP_CUDA_ALGO_EXACT, rv.RVSP_CUDA_ALGO_LEARNED):
+        rv.free_device(*run(algo)[0])  # warm-up
+        ts = []
+        for _ in range(5):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ptrs, n = run(algo)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+            outs[algo] = (d2h(ptrs[1], n, np.int32), d2h(ptrs[2], n, np.float32))
+            rv.free_device(*ptrs)
+        times[algo] = float(np.median(ts))
+    assert np.array_equal(outs[rv.RVSP_CUDA_ALGO_EXACT][0], outs[rv.RVSP_CUDA_ALGO_LEARNED][0])
+    assert np.array_equal(bits(outs[rv.RVSP_CUDA_ALGO_EXACT][1]),
+                          bits(outs[rv.RVSP_CUDA_ALGO_LEARNED][1]))
+    s = rv.oneshot_learned_stats()
+    print(f"exact {times[rv.RVSP_CUDA_ALGO_EXACT] * 1e3:.2f} ms, learned "
+          f"{times[rv.RVSP_CUDA_ALGO_LEARNED] * 1e3:.2f} ms, stats {s}")
+    assert times[rv.RVSP_CUDA_ALGO_LEARNED] < times[rv.RVSP_CUDA_ALGO_EXACT]
+    assert s["predicted_rows"] > 0 and s["fit_capacity"] < s["fit_upper_bound"]
