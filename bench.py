@@ -112,6 +112,14 @@ class ClockSampler:
                 stdout=self.file, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi's start-up queries the driver heavily: the timed region
+        # begins once its first sample is written
+        t0 = time.time()
+        while time.time() - t0 < 10 and self.proc.poll() is None:
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if not self.proc:
@@ -321,34 +329,45 @@ def run_headline(args):
             ptrs, n = _oneshot_dev(rv, v, dA, algo)
             rv.free_device(*ptrs)
 
-    def timed(algo, steps, warmup):
+    def timed(steps, warmup):
+        """Learned and exact steps alternate, so both run under the same
+        conditions (clock, power, host load); per algorithm: mean device ms
+        per step, launches of the learned steps, kernel-family totals."""
+        algos = (rv.RVSP_CUDA_ALGO_LEARNED, rv.RVSP_CUDA_ALGO_EXACT)
         for _ in range(warmup):
-            product(algo)
+            for algo in algos:
+                product(algo)
         torch.cuda.synchronize()
         ranks.barrier(dist)
         torch.cuda.synchronize()
-        rv.kernel_timing(True)
-        l0 = rv.launch_count()
-        evs = []
+        evs = {a: [] for a in algos}
+        kts = {a: {} for a in algos}
+        launches = 0
         for _ in range(steps):
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            product(algo)
-            e1.record()
-            evs.append((e0, e1))
-        torch.cuda.synchronize()
-        launches = rv.launch_count() - l0
-        kt = rv.kernel_times()
-        rv.kernel_timing(False)
+            for algo in algos:
+                flush.zero_()
+                rv.kernel_timing(True)
+                l0 = rv.launch_count()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                product(algo)
+                e1.record()
+                torch.cuda.synchronize()
+                if algo == algos[0]:
+                    launches += rv.launch_count() - l0
+                for k, (t, n) in rv.kernel_times().items():
+                    a = kts[algo].setdefault(k, [0.0, 0])
+                    a[0] += t
+                    a[1] += n
+                rv.kernel_timing(False)
+                evs[algo].append(e0.elapsed_time(e1))
         ranks.barrier(dist)
-        ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
-        return ranks.max_over_ranks(dist, ms), launches, kt
+        ms = {a: ranks.max_over_ranks(dist, statistics.mean(evs[a])) for a in algos}
+        return ms[algos[0]], ms[algos[1]], launches, kts[algos[0]], kts[algos[1]]
 
     sampler = ClockSampler()
     sampler.start()
-    ms_l, launches, kt_l = timed(rv.RVSP_CUDA_ALGO_LEARNED, args.steps, args.warmup)
-    ms_x, _, kt_x = timed(rv.RVSP_CUDA_ALGO_EXACT, args.steps, args.warmup)
+    ms_l, ms_x, launches, kt_l, kt_x = timed(args.steps, args.warmup)
     clocks = sampler.stop()
     value = 2.0 * P_all / (ms_l * 1e-3) / 1e9
     exact_gflops = 2.0 * P_all / (ms_x * 1e-3) / 1e9

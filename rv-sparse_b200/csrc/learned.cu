@@ -554,25 +554,25 @@ int learned_spgemm(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t
         cudaFree(v);
         return st ? st : fail(e, "learned product");
     }
-    if (!device_out) {  // host inputs: hand back malloc'd host arrays
-        int32_t* hrp = (int32_t*)malloc(((size_t)a_rows + 1) * 4);
-        int32_t* hci = (int32_t*)malloc(alloc * 4);
-        float* hv = (float*)malloc(alloc * 4);
+    if (!device_out) {  // host inputs: hand back host arrays that free() releases
+        int32_t* hrp = (int32_t*)host_alloc(((size_t)a_rows + 1) * 4);
+        int32_t* hci = (int32_t*)host_alloc(alloc * 4);
+        float* hv = (float*)host_alloc(alloc * 4);
         if (!hrp || !hci || !hv) {
             free(hrp);
             free(hci);
             free(hv);
-            cudaFree(rp);
-            cudaFree(ci);
-            cudaFree(v);
+            cudaFreeAsync(rp, plan->stream);
+            cudaFreeAsync(ci, plan->stream);
+            cudaFreeAsync(v, plan->stream);
             return RVSP_ERROR_ALLOCATION_FAILED;
         }
-        e = cudaMemcpy(hrp, rp, ((size_t)a_rows + 1) * 4, cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(hci, ci, (size_t)nnz * 4, cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(hv, v, (size_t)nnz * 4, cudaMemcpyDeviceToHost);
-        cudaFree(rp);
-        cudaFree(ci);
-        cudaFree(v);
+        e = copy_to_host(hrp, rp, ((size_t)a_rows + 1) * 4, plan->stream);
+        if (e == cudaSuccess) e = copy_to_host(hci, ci, (size_t)nnz * 4, plan->stream);
+        if (e == cudaSuccess) e = copy_to_host(hv, v, (size_t)nnz * 4, plan->stream);
+        cudaFreeAsync(rp, plan->stream);
+        cudaFreeAsync(ci, plan->stream);
+        cudaFreeAsync(v, plan->stream);
         if (e != cudaSuccess) {
             free(hrp);
             free(hci);

@@ -999,8 +999,7 @@ int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t*
             }
             if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "fill launch");
             if (!dev_ci) {
-                if ((e = cudaMemcpyAsync(c_ci, d_ci, (size_t)nnz * 4, cudaMemcpyDeviceToHost,
-                                         plan->stream)) != cudaSuccess)
+                if ((e = copy_to_host(c_ci, d_ci, (size_t)nnz * 4, plan->stream)) != cudaSuccess)
                     return fail(e, "col_idx copy");
                 plan->filled_host = c_ci;
             }
@@ -1013,9 +1012,7 @@ int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t*
             }
             if ((st = reuse_numeric(plan, A, B, d_ci, d_v, rp_fused ? c_rp : nullptr))) return st;
         }
-        if (!dev_v &&
-            (e = cudaMemcpyAsync(c_v, d_v, (size_t)nnz * 4, cudaMemcpyDeviceToHost,
-                                 plan->stream)) != cudaSuccess)
+        if (!dev_v && (e = copy_to_host(c_v, d_v, (size_t)nnz * 4, plan->stream)) != cudaSuccess)
             return fail(e, "values copy");
     }
     const bool all_dev = dev_rp && dev_ci && dev_v;
@@ -1203,6 +1200,10 @@ struct NoAllocAddr {
 };
 NoAllocAddr g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
 
+}  // namespace
+
+namespace rvsp {
+
 // Unique id of the calling thread's current CUDA context (cuCtxGetId: never
 // reused within the process), or 0 when the driver cannot tell, in which case
 // the caller resolves the address again.
@@ -1231,7 +1232,7 @@ unsigned long long current_context_id() {
     return id;
 }
 
-}  // namespace
+}  // namespace rvsp
 
 extern "C" {
 

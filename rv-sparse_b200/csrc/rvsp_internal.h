@@ -86,6 +86,14 @@ inline void trace_point(const char* what) {
     last = now;
 }
 bool is_dev(const void* p);
+// Unique id of the calling thread's current CUDA context, 0 when unknown.
+unsigned long long current_context_id();
+// Host arrays for results: free()-compatible; large ones 2 MiB aligned with
+// transparent huge pages advised.
+void* host_alloc(size_t bytes);
+// Device->host copy of bytes into dst, finished on return; large copies into
+// pageable memory are staged through pinned pieces and host threads.
+cudaError_t copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t stream);
 
 // Opt-in device timing of the kernels by family (rvsp_cuda_kernel_timing):
 // a KTime scope records a CUDA event pair around the launches it covers on

@@ -144,9 +144,9 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
                 return fail(e, "C alloc");
             }
         } else {
-            rp = (int32_t*)malloc(((size_t)a_rows + 1) * 4);
-            ci = (int32_t*)malloc(alloc * 4);
-            v = (float*)malloc(alloc * 4);
+            rp = (int32_t*)host_alloc(((size_t)a_rows + 1) * 4);
+            ci = (int32_t*)host_alloc(alloc * 4);
+            v = (float*)host_alloc(alloc * 4);
             if (!rp || !ci || !v) {
                 free(rp);
                 free(ci);

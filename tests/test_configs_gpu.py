@@ -7,6 +7,8 @@ oracle (the scalar Gustavson restatement, pinned to the reference kernel):
   learned;
 * the full-size tall-skinny product (2,000,000 x 100,000 times 100,000^2):
   every row of the heaviest 1 % by products plus 2,000 seeded rows;
+* a host C of several hundred MB (the staged device->host copy) against the
+  device-resident C of the same product;
 * batched uneven products: 64 seeded products of the 512-product
   configuration, including its largest, in one batched call, exact and
   learned; and all 512 in one call (their C passes 2^31 entries).
@@ -70,6 +72,18 @@ def test_rmat_row_panels_match_oracle(gpu_lib):
         want = oracle.spgemm_f32(R, R, r0, r1)
         for name, algo in ALGOS:
             _same(_panel_product(dR, dR, r0, r1, algo), want, f"panel {pi} [{r0},{r1}) {name}")
+
+
+def test_host_output_of_a_large_product_matches_the_device_output(gpu_lib):
+    """Host operands and a host C of several hundred MB: the one-shot copies C
+    out through the pinned staging ring and its host threads (copies of 64 MiB
+    and more), exact and learned; bit-identical to the device-resident C."""
+    from gpu_util import oneshot
+    R = gen.rmat(scale=16, edge_factor=16, seed=9)
+    for name, algo in ALGOS:
+        want = oneshot(R, R, algo=algo, device=True)
+        assert want[1].nbytes >= 64 << 20, "C too small to take the staged copy"
+        _same(oneshot(R, R, algo=algo, device=False), want, f"host C {name}")
 
 
 def _row_subset(A, rows):
