@@ -152,8 +152,10 @@ struct rvsp_cuda_plan {
     // when the product has chunked rows; dir_ok when the directory exists
     rvsp::DevBuf bmeta, bdcount, bdscan, bdoff, bdir;
     rvsp::DevBuf ameta, adoff;  // per A entry of heavy rows (HeavyAux)
+    rvsp::DevBuf bsmask;        // chunk presence of B rows without a directory
     bool ameta_ok = false;
     bool dir_ok = false;
+    int32_t smask_words = 0;    // words per B row of bsmask, 0: no masks
     int32_t bin_count[rvsp::NUM_BINS] = {};
     rvsp::BinOffsets offs = {};
     int32_t n_items = 0;

@@ -1302,11 +1302,32 @@ __global__ void k_bdir(CsrView B, int cw_log2, const int4* __restrict__ meta,
     }
 }
 
+// Chunk presence masks (HeavyAux::smask, zeroed before): one warp per B row
+// that spans several column chunks and has no directory; each entry sets its
+// chunk's bit. Rows with a directory or within one chunk keep zero words
+// (the heavy walk never reads them).
+__global__ void k_bmask(CsrView B, int cw_log2, const int4* __restrict__ meta,
+                        const int64_t* __restrict__ doff, int words, uint32_t* __restrict__ smask) {
+    const int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = lane_id();
+    if (k >= B.rows) return;
+    const int4 m = meta[k];
+    if (m.y <= m.x || (m.z >> cw_log2) == (m.w >> cw_log2)) return;
+    if (doff && doff[k] >= 0) return;
+    uint32_t* row = smask + k * words;
+    for (int q = m.x + lane; q < m.y; q += 32) {
+        const int c = B.ci[q] >> cw_log2;
+        // an unsorted row (a broken operand) cannot write outside its words
+        if (c >= 0 && (c >> 5) < words) atomicOr(row + (c >> 5), 1u << (c & 31));
+    }
+}
+
 // Heavy rows' A entries with their B row's metadata and directory offset
-// copied beside them (HeavyAux::ameta / adoff): the heavy walk then reads one
-// coalesced word pair per entry instead of a column index followed by two
-// gathers. One warp per heavy row; a column out of range flags
-// ERR_STRUCTURE and records an empty row.
+// copied beside them (HeavyAux::ameta / adoff; -(k + 2) for a B row k
+// without a directory): the heavy walk then reads one coalesced word pair
+// per entry instead of a column index followed by two gathers. One warp per
+// heavy row; a column out of range flags ERR_STRUCTURE and records an empty
+// row.
 __global__ void k_ameta(CsrView A, CsrView B, const int32_t* __restrict__ rows, int nrows,
                         const int4* __restrict__ meta, const int64_t* __restrict__ doff,
                         int4* __restrict__ ameta, int32_t* __restrict__ adoff,
@@ -1322,7 +1343,8 @@ __global__ void k_ameta(CsrView A, CsrView B, const int32_t* __restrict__ rows, 
         int d = -1;
         if ((unsigned)k < (unsigned)B.rows) {
             m = meta[k];
-            if (doff) d = (int)doff[k];
+            d = doff ? (int)doff[k] : -1;
+            if (d < 0) d = -(k + 2);
         } else {
             atomicOr(err, ERR_STRUCTURE);
         }
@@ -1533,9 +1555,9 @@ __device__ __forceinline__ void heavy_finish(
 // the GPU once (a warp that drew a light item takes the next one instead of
 // idling beside a heavy one). The warp walks the row's A entries 32 at a
 // time; each lane finds the part of its B row that falls in the chunk from
-// the B row's metadata and, for long rows, its column-chunk directory (a
-// binary search otherwise), and heavy_segments accumulates the segments in
-// A-row order. The A row is re-read once per chunk; the products once in
+// the B row's metadata and, for long rows, its column-chunk directory (for
+// the others the chunk's presence bit, then a binary search only when the
+// bit is set), and heavy_segments accumulates the segments in A-row order. The A row is re-read once per chunk; the products once in
 // all.
 constexpr int HEAVY_MAX_WARPS = 32;
 
@@ -1586,15 +1608,17 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
             int s = 0, len = 0;
             float av = 0.0f;
             if (j < a1) {
-                // {start, end, first column, last column} of B row A.ci[j],
-                // and its directory offset
+                // {start, end, first column, last column} of B row k =
+                // A.ci[j], and its directory offset (or k when it has none)
                 int4 m = make_int4(0, 0, 0, -1);
                 int64_t d = -1;
+                int k = -1;
                 if (aux.ameta) {
                     m = aux.ameta[j];
-                    if (aux.dir) d = aux.adoff[j];
+                    const int x = aux.adoff[j];
+                    if (x >= 0) d = x; else k = -(x + 2);
                 } else {
-                    const int k = A.ci[j];
+                    k = A.ci[j];
                     if ((unsigned)k >= (unsigned)B.rows) {
                         atomicOr(err, ERR_STRUCTURE);
                     } else {
@@ -1604,7 +1628,7 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
                 }
                 if (m.y > m.x && m.w >= lo && m.z < hi) {
                     int t;
-                    if (d >= 0) {
+                    if (d >= 0 && aux.dir) {
                         const int c = it.chunk - (m.z >> cw_log2);
                         s = m.z >= lo ? m.x : aux.dir[d + c];
                         t = m.w < hi ? m.y : aux.dir[d + c + 1];
@@ -1612,12 +1636,19 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
                         // directory entry unwritten: stay inside the row
                         s = min(max(s, m.x), m.y);
                         t = min(max(t, s), m.y);
+                    } else if (m.z >= lo && m.w < hi) {
+                        s = m.x;  // the whole row lies in the chunk
+                        t = m.y;
+                    } else if (aux.smask && k >= 0 &&
+                               !((aux.smask[(int64_t)k * aux.smask_words + (it.chunk >> 5)] >>
+                                  (it.chunk & 31)) & 1u)) {
+                        t = s;  // no entry of the row in this chunk
                     } else {
                         s = m.z >= lo ? m.x : seq_lower_bound(B.ci, m.x, m.y, lo);
                         t = m.w < hi ? m.y : seq_lower_bound(B.ci, s, m.y, hi);
                     }
                     len = t - s;
-                    if (MODE != COUNT) av = A.v[j];
+                    if (MODE != COUNT && len > 0) av = A.v[j];
                 }
             }
             if (__any_sync(FULL, len > 0))

@@ -88,10 +88,17 @@ struct HeavyAux {
     const int4* meta;
     const int64_t* doff;
     const int32_t* dir;
-    // the same per A entry of the heavy rows (ameta[j] = meta[A.ci[j]], adoff
-    // likewise, -1: no directory), or null: looked up through A.ci
+    // the same per A entry of the heavy rows (ameta[j] = meta[A.ci[j]];
+    // adoff[j] = the directory offset of B row k = A.ci[j], or -(k + 2) when
+    // it has none), or null: looked up through A.ci
     const int4* ameta;
     const int32_t* adoff;
+    // chunk presence of the B rows that span several chunks without a
+    // directory: bit c of row k's smask_words words is set when the row has
+    // an entry in column chunk c (a clear bit spares the row's two binary
+    // searches), or null
+    const uint32_t* smask;
+    int32_t smask_words;
 };
 constexpr int DIR_MIN_LEN = 32;
 
