@@ -191,8 +191,13 @@ static void set_mode_attrs() {
 // Heavy kernel shape for every mode and chunk width: warps per CTA chosen to
 // keep the most warps resident per SM (each warp holds its own accumulator
 // and bitmap in shared memory), and the resident CTAs per SM; the launches
-// fill the GPU once and the warps pull work items from a counter.
+// fill the GPU once and the CTAs pull batches of work items from a counter.
 static int g_heavy_w[3][HEAVY_CW_LOG2_MAX + 1];
+// dynamic shared memory of a heavy CTA of W warps: their accumulators and
+// bitmaps, then the CTA's work-batch word
+static size_t heavy_launch_smem(int mode, int cl, int W) {
+    return (size_t)W * heavy_smem_bytes(mode, 1 << cl) + 16;
+}
 static int g_heavy_ctas[3][HEAVY_CW_LOG2_MAX + 1];
 static int g_sms = 148;
 
@@ -209,17 +214,19 @@ void init_kernel_attributes() {
             const void* fns[3] = {(const void*)k_heavy<COUNT>, (const void*)k_heavy<FILL>,
                                   (const void*)k_heavy<REUSE>};
             for (int m = 0; m < 3; ++m) {
-                const size_t per = (size_t)heavy_smem_bytes(m, 1 << cl);
                 int best_w = 1, best_n = 1, best = 0;
                 for (int W = 1; W <= HEAVY_MAX_WARPS; ++W) {
-                    if (W * per > (size_t)HEAVY_SMEM_MAX) break;
+                    const size_t bytes = heavy_launch_smem(m, cl, W);
+                    if (bytes > (size_t)HEAVY_SMEM_MAX) break;
                     int n = 0;
-                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fns[m], W * 32, W * per) !=
+                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fns[m], W * 32, bytes) !=
                         cudaSuccess) {
                         cudaGetLastError();
                         continue;
                     }
-                    if (n * W > best) {
+                    // at equal resident warps the larger CTA: its item
+                    // batches (twice its warps) take fewer counter atomics
+                    if (n * W >= best) {
                         best = n * W;
                         best_w = W;
                         best_n = n;
@@ -338,7 +345,7 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
                                plan->smask_words};
             int32_t* queue = &plan->misc.as<Misc>()->heavy_queue;
             cudaMemsetAsync(queue, 0, sizeof(int32_t), plan->stream);
-            k_heavy<MODE><<<grid, W * 32, W * heavy_smem_bytes(MODE, 1 << cl), plan->stream>>>(
+            k_heavy<MODE><<<grid, W * 32, heavy_launch_smem(MODE, cl, W), plan->stream>>>(
                 A, B, plan->items.as<HeavyItem>(), plan->n_items, plan->item_cnt.as<int32_t>(),
                 o.cnt, plan->item_scan.as<int64_t>(), o.c_rp, o.c_ci, o.c_v, o.err, ctl, cl,
                 aux, queue);

@@ -115,7 +115,9 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
         plan->map_policy = 0;  // a one-shot product is never reused
     }
     int32_t a_nnz = 0, b_nnz = 0;
+    trace_point("one-shot: enter");
     if ((st = read_ends(plan, a_rp + a_rows, b_rp + a_cols, &a_nnz, &b_nnz))) return st;
+    trace_point("one-shot: operand nnz read");
     plan->params = default_params();
     const bool dev = is_dev(a_rp);
     keep_pool_memory();
@@ -154,6 +156,7 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
                 return RVSP_ERROR_ALLOCATION_FAILED;
             }
         }
+        trace_point("one-shot: C allocated");
         st = rvsp_cuda_numeric(plan, a_rp, a_ci, a_v, b_rp, b_ci, b_v, rp, ci, v, 1, nullptr);
         if (st) {
             if (dev) {

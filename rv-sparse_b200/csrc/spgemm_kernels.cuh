@@ -1551,9 +1551,9 @@ __device__ __forceinline__ void heavy_finish(
 }
 
 // Heavy rows: one warp per work item (row, chunk of cw = 2^cw_log2
-// columns), items pulled one at a time from a counter by a grid that fills
-// the GPU once (a warp that drew a light item takes the next one instead of
-// idling beside a heavy one). The warp walks the row's A entries 32 at a
+// columns), items pulled from a counter (in CTA batches, below) by a grid
+// that fills the GPU once (a warp that drew a light item takes the next one
+// instead of idling beside a heavy one). The warp walks the row's A entries 32 at a
 // time; each lane finds the part of its B row that falls in the chunk from
 // the B row's metadata and, for long rows, its column-chunk directory (for
 // the others the chunk's presence bit, then a binary search only when the
@@ -1586,11 +1586,40 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
     if (MODE != REUSE)
         for (int x = lane; x < nw; x += 32) bits[x] = 0u;
     __syncwarp();
+    // Work items come from the launch's counter in batches of twice the
+    // CTA's warps: the CTA's warps draw the batch's items one at a time from
+    // a (batch base, next index) word at the end of the dynamic shared
+    // memory, and the warp that draws index `batch` fetches the next batch.
+    // Warps that arrive while that fetch is in flight (index > batch) take
+    // a single item straight from the counter instead of waiting, so no
+    // warp ever waits on another. Every item is handed out exactly once;
+    // the batches keep the order of the item list (each CTA works on
+    // neighbouring items, the grid sweeps the list front to back) while
+    // the counter takes one atomic per batch instead of one per item.
+    const long long batch = 2 * (long long)(blockDim.x >> 5);
+    unsigned long long* s_q = reinterpret_cast<unsigned long long*>(
+        smem + (blockDim.x >> 5) * heavy_smem_bytes(MODE, cw));
+    if (threadIdx.x == 0) *s_q = (unsigned long long)batch;  // the first draw fetches
+    __syncthreads();
     for (;;) {
-        int w = 0;
-        if (lane == 0) w = atomicAdd(queue, 1);
-        w = __shfl_sync(FULL, w, 0);
-        if (w >= nitems) break;
+        long long wq = 0;
+        if (lane == 0) {
+            const unsigned long long o = atomicAdd(s_q, 1ull);
+            const long long b = (long long)(o >> 32);
+            const long long c = (long long)(o & 0xffffffffull);
+            if (c < batch) {
+                wq = b + c;
+            } else if (c == batch) {
+                const int nb = atomicAdd(queue, (int)batch);
+                atomicExch(s_q, ((unsigned long long)(unsigned)nb << 32) | 1ull);
+                wq = nb;
+            } else {
+                wq = atomicAdd(queue, 1);
+            }
+        }
+        wq = __shfl_sync(FULL, wq, 0);
+        if (wq >= nitems) break;
+        const int w = (int)wq;
         const HeavyItem it = items[w];
         const int row = it.row;
         if (ctl.only && !ctl.only[row]) continue;
