@@ -860,6 +860,32 @@ __device__ void warp_radix_sort(int32_t* keys, int32_t* tmp, int n, int32_t* his
     warp_radix_sort_core<8>(keys, tmp, n, (uint32_t)mn, 0, passes, hist);
 }
 
+// Work from a launch's counter in CTA batches. The CTA's warps draw
+// indices one at a time from a (batch base, next index) word in shared
+// memory; the warp that draws index `batch` fetches the next batch from the
+// counter. Warps that arrive while that fetch is in flight (index > batch)
+// take a single index straight from the counter instead of waiting, so no
+// warp ever waits on another, and every index is handed out exactly once.
+// The batches keep the order of the list (each CTA works on neighbouring
+// entries, the grid sweeps the list front to back) while the counter takes
+// one atomic per batch instead of one per entry: hundreds of millions of
+// atomics on one address otherwise (R-MAT 2^20 heavy items). The word
+// starts at `batch` (set before a __syncthreads), so the first draw
+// fetches. Called by lane 0; returns the index drawn.
+__device__ __forceinline__ long long draw_batched(unsigned long long* s_q, int32_t* queue,
+                                                  long long batch) {
+    const unsigned long long o = atomicAdd(s_q, 1ull);
+    const long long b = (long long)(o >> 32);
+    const long long c = (long long)(o & 0xffffffffull);
+    if (c < batch) return b + c;
+    if (c == batch) {
+        const int nb = atomicAdd(queue, (int)batch);
+        atomicExch(s_q, ((unsigned long long)(unsigned)nb << 32) | 1ull);
+        return nb;
+    }
+    return atomicAdd(queue, 1);
+}
+
 // Medium rows: one warp per row, a CAP-slot shared-memory table per warp.
 //   COUNT  hash-insert the row's columns, count the new ones
 //   FILL   COUNT's insert, compaction, radix sort -> sorted columns written;
@@ -891,7 +917,9 @@ __global__ void __launch_bounds__(WARPS * 32)
     const bool learned = MODE != REUSE && ctl.learned;
 
     for (;;) {
-        // rows are pulled one at a time from the launch's counter
+        // rows are pulled one at a time from the launch's counter (a CTA
+        // batch word like k_heavy's would cost the 512- and 1024-slot FILL
+        // tables a resident CTA per SM; one in global memory measured slower)
         int w = 0;
         if (lane == 0) w = atomicAdd(queue, 1);
         w = __shfl_sync(FULL, w, 0);
@@ -1586,37 +1614,16 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
     if (MODE != REUSE)
         for (int x = lane; x < nw; x += 32) bits[x] = 0u;
     __syncwarp();
-    // Work items come from the launch's counter in batches of twice the
-    // CTA's warps: the CTA's warps draw the batch's items one at a time from
-    // a (batch base, next index) word at the end of the dynamic shared
-    // memory, and the warp that draws index `batch` fetches the next batch.
-    // Warps that arrive while that fetch is in flight (index > batch) take
-    // a single item straight from the counter instead of waiting, so no
-    // warp ever waits on another. Every item is handed out exactly once;
-    // the batches keep the order of the item list (each CTA works on
-    // neighbouring items, the grid sweeps the list front to back) while
-    // the counter takes one atomic per batch instead of one per item.
+    // work items in CTA batches of twice the CTA's warps (draw_batched); the
+    // batch word follows the warps' accumulators and bitmaps
     const long long batch = 2 * (long long)(blockDim.x >> 5);
     unsigned long long* s_q = reinterpret_cast<unsigned long long*>(
         smem + (blockDim.x >> 5) * heavy_smem_bytes(MODE, cw));
-    if (threadIdx.x == 0) *s_q = (unsigned long long)batch;  // the first draw fetches
+    if (threadIdx.x == 0) *s_q = (unsigned long long)batch;
     __syncthreads();
     for (;;) {
         long long wq = 0;
-        if (lane == 0) {
-            const unsigned long long o = atomicAdd(s_q, 1ull);
-            const long long b = (long long)(o >> 32);
-            const long long c = (long long)(o & 0xffffffffull);
-            if (c < batch) {
-                wq = b + c;
-            } else if (c == batch) {
-                const int nb = atomicAdd(queue, (int)batch);
-                atomicExch(s_q, ((unsigned long long)(unsigned)nb << 32) | 1ull);
-                wq = nb;
-            } else {
-                wq = atomicAdd(queue, 1);
-            }
-        }
+        if (lane == 0) wq = draw_batched(s_q, queue, batch);
         wq = __shfl_sync(FULL, wq, 0);
         if (wq >= nitems) break;
         const int w = (int)wq;
