@@ -358,17 +358,20 @@ int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, b
     }
     plan->slot_total = plan->host_misc.slot_total;
     cudaError_t e;
-    size_t free_b = SIZE_MAX, total_b = 0;
-    // slots past 1 GiB must fit in half the free memory
-    if (fused && (size_t)plan->slot_total * 10 > (1ull << 30) &&
-        (e = cudaMemGetInfo(&free_b, &total_b)) != cudaSuccess)
-        return fail(e, "mem info");
     // heavy rows' chunks that outgrow their predicted slot share an overflow
     // pool of a quarter of the slots, after them in the same buffers
     plan->pool_cap = fused && plan->n_items > 0 ? plan->slot_total / 4 : 0;
     const int64_t tmp_total = plan->slot_total + plan->pool_cap;
+    size_t free_b = SIZE_MAX, total_b = 0;
+    // slot buffers that must grow past 1 GiB must fit in half the free
+    // memory (queried only then: the query waits behind any other client of
+    // the driver, e.g. a clock monitor, with the GPU idle)
+    if (fused && (size_t)tmp_total * 4 > plan->tmp_ci.cap &&
+        (size_t)plan->slot_total * 10 > (1ull << 30) &&
+        (e = cudaMemGetInfo(&free_b, &total_b)) != cudaSuccess)
+        return fail(e, "mem info");
     if (fused) {
-        if ((size_t)tmp_total * 8 > free_b / 2) {
+        if (free_b != SIZE_MAX && (size_t)tmp_total * 8 > free_b / 2) {
             g_err = "predicted capacity exceeds the memory budget";
             return RVSP_ERROR_ALLOCATION_FAILED;
         }

@@ -70,12 +70,17 @@ struct KPending {
     cudaEvent_t e0, e1;
 };
 static std::vector<KPending> g_ktime_pending;
+// events read out by a drain, reused by later scopes: creating and destroying
+// events are driver calls, which wait behind any other client of the driver
+// (a clock monitor, say) while the GPU runs dry inside the timed scope
+static std::vector<cudaEvent_t> g_ktime_free;
 static double g_ktime_ms[KF_NUM];
 static int64_t g_ktime_n[KF_NUM];
 
 bool ktime_enabled() { return g_ktime_on.load(std::memory_order_relaxed); }
 
-// Reads every queued pair (waiting for its end event) into the totals.
+// Reads every queued pair (waiting for its end event) into the totals; the
+// events go back to the free list.
 static void ktime_drain_locked() {
     for (const KPending& k : g_ktime_pending) {
         float ms = 0.0f;
@@ -83,33 +88,54 @@ static void ktime_drain_locked() {
             cudaEventElapsedTime(&ms, k.e0, k.e1) == cudaSuccess) {
             g_ktime_ms[k.fam] += ms;
             g_ktime_n[k.fam] += 1;
+            g_ktime_free.push_back(k.e0);
+            g_ktime_free.push_back(k.e1);
+        } else {
+            cudaEventDestroy(k.e0);
+            cudaEventDestroy(k.e1);
         }
-        cudaEventDestroy(k.e0);
-        cudaEventDestroy(k.e1);
     }
     g_ktime_pending.clear();
     cudaGetLastError();
 }
 
+// An event recorded on `stream`: a reused one when the free list has one
+// (a reused event that will not record, e.g. one from another device, is
+// destroyed and a new one made), else a new one; null on failure.
+static cudaEvent_t ktime_record(cudaStream_t stream) {
+    cudaEvent_t ev = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_ktime_mu);
+        if (!g_ktime_free.empty()) {
+            ev = g_ktime_free.back();
+            g_ktime_free.pop_back();
+        }
+    }
+    if (ev && cudaEventRecord(ev, stream) == cudaSuccess) return ev;
+    if (ev) cudaEventDestroy(ev);
+    cudaGetLastError();
+    ev = nullptr;
+    if (cudaEventCreate(&ev) != cudaSuccess || cudaEventRecord(ev, stream) != cudaSuccess) {
+        if (ev) cudaEventDestroy(ev);
+        cudaGetLastError();
+        return nullptr;
+    }
+    return ev;
+}
+
 KTime::KTime(cudaStream_t stream, bool capturing, int family) {
     if (!ktime_enabled() || capturing) return;
-    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventRecord(e0, stream) != cudaSuccess) {
-        if (e0) cudaEventDestroy(e0);
-        e0 = nullptr;
-        cudaGetLastError();
-        return;
-    }
+    e0 = ktime_record(stream);
+    if (!e0) return;
     st = stream;
     fam = family;
 }
 
 KTime::~KTime() {
     if (!e0) return;
-    cudaEvent_t e1 = nullptr;
-    if (cudaEventCreate(&e1) != cudaSuccess || cudaEventRecord(e1, st) != cudaSuccess) {
+    cudaEvent_t e1 = ktime_record(st);
+    if (!e1) {
         cudaEventDestroy(e0);
-        if (e1) cudaEventDestroy(e1);
-        cudaGetLastError();
         return;
     }
     std::lock_guard<std::mutex> lk(g_ktime_mu);
@@ -566,12 +592,12 @@ int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
     // stay in L2 (measured: R-MAT 2^18, 84 MB of copies, 5 % faster; R-MAT
     // 2^20, 335 MB, 12 % slower than the column-index walk whose per-B-row
     // metadata stays in L2).
+    // (no free-memory query: it is a driver call that waits behind any other
+    // client of the driver, e.g. a clock monitor, with the GPU idle)
     const int32_t nh = plan->bin_count[BIN_HEAVY];
     const size_t abytes = 20 * (size_t)plan->a_nnz;
     constexpr size_t AMETA_MAX_BYTES = 96u << 20;
-    size_t free_b = 0, total_b = 0;
     plan->ameta_ok = nh > 0 && abytes <= AMETA_MAX_BYTES &&
-                     cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && abytes <= free_b / 4 &&
                      plan->ameta.ensure(16 * (size_t)plan->a_nnz) == cudaSuccess &&
                      plan->adoff.ensure(4 * (size_t)plan->a_nnz) == cudaSuccess;
     cudaGetLastError();  // without the copies the walk looks up through A.ci
