@@ -23,7 +23,7 @@
 //                  counted them)
 //   C              scan of all counts -> row pointer; flagged rows are filled
 //                  in place by the exact FILL kernels, the rest are copied from
-//                  their slots (k_compact, k_compact_items)
+//                  their slots (k_compact, k_compact_rows, k_compact_items)
 //
 // Every row is computed by the same order-preserving kernels as the exact
 // path, so the result is bit-identical to it; a misprediction costs time,
@@ -184,6 +184,45 @@ __global__ void k_need(int32_t rows, const uint8_t* __restrict__ lbin,
     }
 }
 
+// Copy finished rows from their slots into C, one warp per row (the warp-bin
+// rows: tens to thousands of entries each), 128 entries per step with each
+// lane's four loads issued before its stores. Coalesced on both sides.
+__global__ void __launch_bounds__(256)
+    k_compact_rows(const int32_t* __restrict__ rows, int32_t n, const uint8_t* __restrict__ need,
+                   const int32_t* __restrict__ cnt, const int64_t* __restrict__ slot_off,
+                   const int32_t* __restrict__ c_rp, const int32_t* __restrict__ tmp_ci,
+                   const float* __restrict__ tmp_v, int32_t* __restrict__ c_ci,
+                   float* __restrict__ c_v) {
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n) return;
+    const int row = rows[w];
+    if (need[row]) return;
+    const int k = cnt[row];
+    const int64_t src = slot_off[row];
+    const int dst = c_rp[row];
+    for (int x0 = 0; x0 < k; x0 += 128) {
+        int32_t ci[4];
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int x = x0 + 32 * u + lane;
+            if (x < k) {
+                ci[u] = tmp_ci[src + x];
+                v[u] = tmp_v[src + x];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int x = x0 + 32 * u + lane;
+            if (x < k) {
+                c_ci[dst + x] = ci[u];
+                c_v[dst + x] = v[u];
+            }
+        }
+    }
+}
+
 // Copy finished rows from their slots into C: one warp per 32 consecutive
 // list entries; the lanes load the 32 rows' counts and offsets together, then
 // copy either the 32 rows' entries as one list (up to 64 entries a row on
@@ -264,9 +303,14 @@ __global__ void __launch_bounds__(256)
 }
 
 // Copy the chunks of heavy rows finished in their slots (or the overflow
-// pool) into C: one warp per work item (grid-stride), the chunk's entries from
-// where the sweep put them to their place in C (its row's start plus the
-// counts of the row's earlier chunks).
+// pool) into C, each chunk's entries from where the sweep put them to their
+// place in C (its row's start plus the counts of the row's earlier chunks).
+// One warp per 32 consecutive work items (grid-stride): lane l loads item l's
+// bookkeeping (all 32 items' loads in flight together), then the warp copies
+// the 32 chunks' entries as one list, 128 entries per step with each lane's
+// four loads issued before its stores; each lane finds its entry's chunk in
+// the scan of the chunks' counts. Items of a row are consecutive, so the
+// stores run contiguously through C.
 __global__ void __launch_bounds__(256)
     k_compact_items(const HeavyItem* __restrict__ items, int32_t n,
                     const uint8_t* __restrict__ hmask, const uint8_t* __restrict__ need,
@@ -276,16 +320,55 @@ __global__ void __launch_bounds__(256)
                     const float* __restrict__ tmp_v, int32_t* __restrict__ c_ci,
                     float* __restrict__ c_v) {
     const int lane = threadIdx.x & 31;
+    const int64_t groups = ((int64_t)n + 31) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += nwarps) {
-        const HeavyItem it = items[w];
-        if (!hmask[it.row] || need[it.row]) continue;
-        const int k = item_cnt[w];
-        const int64_t src = item_off[w];
-        const int64_t dst = (int64_t)c_rp[it.row] + (item_scan[w] - item_scan[it.first]);
-        for (int x = lane; x < k; x += 32) {
-            c_ci[dst + x] = tmp_ci[src + x];
-            c_v[dst + x] = tmp_v[src + x];
+    for (int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < groups;
+         g += nwarps) {
+        const int64_t w = (g << 5) + lane;
+        int k = 0;
+        int64_t src = 0, dst = 0;
+        if (w < n) {
+            const HeavyItem it = items[w];
+            if (hmask[it.row] && !need[it.row]) {
+                k = item_cnt[w];
+                src = item_off[w];
+                dst = (int64_t)c_rp[it.row] + (item_scan[w] - item_scan[it.first]);
+            }
+        }
+        int incl = k;  // inclusive scan of the chunks' counts over the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        for (int e0 = 0; e0 < total; e0 += 128) {
+            int32_t ci[4];
+            float v[4];
+            int64_t d[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = e0 + 32 * u + lane;
+                int j = 0;
+#pragma unroll
+                for (int st = 16; st >= 1; st >>= 1)
+                    if (__shfl_sync(FULL, incl, j + st - 1) <= e) j += st;
+                j = min(j, 31);
+                const int off = e - (__shfl_sync(FULL, incl, j) - __shfl_sync(FULL, k, j));
+                const int64_t sj = __shfl_sync(FULL, src, j);
+                d[u] = __shfl_sync(FULL, dst, j) + off;
+                if (e < total) {
+                    ci[u] = tmp_ci[sj + off];
+                    v[u] = tmp_v[sj + off];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (e0 + 32 * u + lane < total) {
+                    c_ci[d[u]] = ci[u];
+                    c_v[d[u]] = v[u];
+                }
+            }
         }
     }
 }
@@ -492,14 +575,14 @@ int learned_finish(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, int
     int32_t nw = 0;
     for (int b = BIN_WARP0; b < LBIN_EXACT; ++b) nw += plan->lcount[b];
     if (nw > 0) {
-        k_compact<<<(unsigned)(((int64_t)nw + 255) / 256), 256, 0, plan->stream>>>(
+        k_compact_rows<<<(unsigned)(((int64_t)nw * 32 + 255) / 256), 256, 0, plan->stream>>>(
             lrows + plan->loffs.off[BIN_WARP0], nw, plan->need.as<uint8_t>(),
             plan->cnt.as<int32_t>(), plan->slot_off.as<int64_t>(), plan->c_rp.as<int32_t>(),
             plan->tmp_ci.as<int32_t>(), plan->tmp_v.as<float>(), c_ci, c_v);
         note_launch(plan, 1);
     }
     if (plan->heavy_slots && plan->n_items > 0) {
-        const int64_t grid = std::min<int64_t>(((int64_t)plan->n_items + 7) / 8, 148 * 64);
+        const int64_t grid = std::min<int64_t>(((int64_t)plan->n_items + 255) / 256, 148 * 64);
         k_compact_items<<<(unsigned)grid, 256, 0, plan->stream>>>(
             plan->items.as<HeavyItem>(), plan->n_items, plan->hmask.as<uint8_t>(),
             plan->need.as<uint8_t>(), plan->item_cnt.as<int32_t>(), plan->item_off.as<int64_t>(),
