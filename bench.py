@@ -495,8 +495,9 @@ def committed_traffic(kernel, bytes_per_launch):
 def run_rmat_e2e(rv, A, ops, panels, args, torch):
     """The product through rvsp_spgemm_csr (learned backend) on host CSR:
     each panel's A (its row pointer rebased, its entries a view) and B = A are
-    host arrays; the library uploads them and hands C back in malloc'd host
-    memory, freed by rvsp_csr_destroy. Wall time of all panels per step."""
+    host arrays; the library uploads them and hands C back in host arrays
+    (staged through pinned memory), freed by rvsp_csr_destroy. Wall time of
+    all panels per step."""
     import ctypes as C
     L = rv.lib()
     hb = rv.csr_struct(A.rows, A.cols, A.nnz, A.row_ptr, A.col_idx, A.values)

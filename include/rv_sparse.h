@@ -22,8 +22,9 @@
  * memory of the current CUDA device; the backend detects which per pointer.
  * Host inputs are staged to the device; host outputs are copied back before
  * the call returns. One-shot outputs are allocated where the inputs live
- * (malloc and owns_data = RVSP_OWNS_HOST, or cudaMalloc and owns_data =
- * RVSP_OWNS_DEVICE); rvsp_csr_destroy frees either.
+ * (host memory that free() releases and owns_data = RVSP_OWNS_HOST, or
+ * device memory and owns_data = RVSP_OWNS_DEVICE); rvsp_csr_destroy frees
+ * either.
  *
  * Results: C's structure (row_ptr, col_idx) is bit-exact against the
  * reference scalar kernel. Values are computed in the reference's order

@@ -63,8 +63,9 @@ typedef enum
 
 /*
  * owns_data: 0 = caller-owned arrays (rvsp_csr_create), RVSP_OWNS_HOST = the
- * library malloc'd them (the reference's value 1), RVSP_OWNS_DEVICE = the CUDA
- * backend cudaMalloc'd them because the inputs were device-resident.
+ * library allocated them in host memory that free() releases (the
+ * reference's value 1), RVSP_OWNS_DEVICE = the CUDA backend allocated them in
+ * device memory because the inputs were device-resident.
  * rvsp_csr_destroy frees each kind with the matching call.
  */
 #define RVSP_OWNS_HOST 1

@@ -172,9 +172,11 @@ RVSP_CUDA_API int rvsp_cuda_op_counts(rvsp_cuda_plan_t plan, int64_t *op_counts_
  * (RVSP_SPGEMM_PARAMS, rv-sparse src/kernels/spgemm/rvsp_spgemm.h:68-82;
  * gustavson_core_f32.inc:66-193): analysis, C allocation, fill, numeric.
  * C's arrays are allocated by the callee where the inputs live (device
- * inputs: cudaMalloc, release with rvsp_cuda_free; host inputs: malloc,
- * release with free). op_counts_out is optional (a_rows entries, host or
- * device). algo is RVSP_CUDA_ALGO_EXACT or RVSP_CUDA_ALGO_LEARNED.
+ * inputs: device memory, release with rvsp_cuda_free; host inputs: host
+ * memory, release with free(); arrays of 64 MiB and more are 2 MiB aligned
+ * with transparent huge pages advised). op_counts_out is optional (a_rows
+ * entries, host or device). algo is RVSP_CUDA_ALGO_EXACT or
+ * RVSP_CUDA_ALGO_LEARNED.
  */
 RVSP_CUDA_API int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, int32_t b_cols,
                          const int32_t *a_row_ptr, const int32_t *a_col_idx,
