@@ -645,9 +645,9 @@ int learned_spgemm(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t
         int32_t* hci = (int32_t*)host_alloc(alloc * 4);
         float* hv = (float*)host_alloc(alloc * 4);
         if (!hrp || !hci || !hv) {
-            free(hrp);
-            free(hci);
-            free(hv);
+            host_free(hrp);
+            host_free(hci);
+            host_free(hv);
             cudaFreeAsync(rp, plan->stream);
             cudaFreeAsync(ci, plan->stream);
             cudaFreeAsync(v, plan->stream);
@@ -660,9 +660,9 @@ int learned_spgemm(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t
         cudaFreeAsync(ci, plan->stream);
         cudaFreeAsync(v, plan->stream);
         if (e != cudaSuccess) {
-            free(hrp);
-            free(hci);
-            free(hv);
+            host_free(hrp);
+            host_free(hci);
+            host_free(hv);
             return fail(e, "learned copy-out");
         }
         rp = hrp;

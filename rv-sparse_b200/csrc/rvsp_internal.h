@@ -89,8 +89,11 @@ bool is_dev(const void* p);
 // Unique id of the calling thread's current CUDA context, 0 when unknown.
 unsigned long long current_context_id();
 // Host arrays for results: free()-compatible; large ones 2 MiB aligned with
-// transparent huge pages advised.
+// transparent huge pages advised, or a released one taken from the cache.
 void* host_alloc(size_t bytes);
+// Release a host array (any free()-compatible block): large ones go to the
+// cache that host_alloc draws from, the rest to free().
+void host_free(void* p);
 // Device->host copy of bytes into dst, finished on return; large copies into
 // pageable memory are staged through pinned pieces and host threads.
 cudaError_t copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t stream);

@@ -150,9 +150,9 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
             ci = (int32_t*)host_alloc(alloc * 4);
             v = (float*)host_alloc(alloc * 4);
             if (!rp || !ci || !v) {
-                free(rp);
-                free(ci);
-                free(v);
+                host_free(rp);
+                host_free(ci);
+                host_free(v);
                 return RVSP_ERROR_ALLOCATION_FAILED;
             }
         }
@@ -164,9 +164,9 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
                 cudaFree(ci);
                 cudaFree(v);
             } else {
-                free(rp);
-                free(ci);
-                free(v);
+                host_free(rp);
+                host_free(ci);
+                host_free(v);
             }
             return st;
         }

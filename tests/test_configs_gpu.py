@@ -86,6 +86,32 @@ def test_host_output_of_a_large_product_matches_the_device_output(gpu_lib):
         _same(oneshot(R, R, algo=algo, device=False), want, f"host C {name}")
 
 
+def test_host_results_through_the_public_api_reuse_released_arrays(gpu_lib):
+    """rvsp_spgemm_csr with host operands, twice per backend, the first C
+    released by rvsp_csr_destroy before the second product (large released
+    arrays are kept and handed out again): every host C bit-identical to the
+    device-resident C of the same product."""
+    from gpu_util import oneshot
+    L = rv.lib()
+    R = gen.rmat(scale=16, edge_factor=16, seed=9)
+    S = gen.rmat(scale=16, edge_factor=14, seed=10)
+    for backend, algo in ((rv.RVSP_BACKEND_CUDA, rv.RVSP_CUDA_ALGO_EXACT),
+                          (rv.RVSP_BACKEND_CUDA_LEARNED, rv.RVSP_CUDA_ALGO_LEARNED)):
+        opts = rv.SpgemmOptions(backend, rv.RVSP_DTYPE_FP32, rv.RVSP_DTYPE_FP32)
+        for M in (R, S, R):
+            want = oneshot(M, M, algo=algo, device=True)
+            hm = rv.csr_struct(M.rows, M.cols, M.nnz, M.row_ptr, M.col_idx, M.values)
+            c = rv.CsrMatrix()
+            rv.check(L.rvsp_spgemm_csr(C.byref(hm), C.byref(hm), C.byref(c), C.byref(opts)),
+                     "rvsp_spgemm_csr")
+            assert c.owns_data == 1 and c.nnz == want[1].size
+            got = (np.ctypeslib.as_array((C.c_int32 * (M.rows + 1)).from_address(c.row_ptr)).copy(),
+                   np.ctypeslib.as_array((C.c_int32 * c.nnz).from_address(c.col_idx)).copy(),
+                   np.ctypeslib.as_array((C.c_float * c.nnz).from_address(c.values)).copy())
+            L.rvsp_csr_destroy(C.byref(c))
+            _same(got, want, f"public API host C, backend {backend}")
+
+
 def _row_subset(A, rows):
     """CSR of the given rows of A (in order)."""
     lens = np.diff(A.row_ptr.astype(np.int64))[rows]
