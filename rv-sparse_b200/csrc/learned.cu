@@ -426,7 +426,7 @@ static int learned_pre_sync(rvsp_cuda_plan* plan) {
 // every other row's columns and values wait in its slot (tmp_ci / tmp_v at
 // slot_off) for learned_finish; without, the sweep is the COUNT kernels with
 // tables sized by the prediction (the descriptor's structure analysis).
-int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool fused) {
+int learned_symbolic(rvsp_cuda_plan* plan, CsrView& A, CsrView& B, bool fused) {
     plan->heavy_slots = fused;
     int st = analyze(plan, A, B, true, learned_pre_sync);
     if (st) return st;

@@ -388,6 +388,10 @@ void run_rows(rvsp_cuda_plan* plan, int mode, const CsrView& A, const CsrView& B
 }
 
 // Exclusive scan of n int32 counts. total_dev receives the sum.
+// arrays of at most this many scan tiles (2048 counts each) take the
+// one-CTA scan
+constexpr int64_t SCAN_SINGLE_TILES = 4;
+
 int scan_counts(rvsp_cuda_plan* plan, const int32_t* in, int64_t n, int64_t* out64,
                 int32_t* out32, int64_t* total_dev) {
     const int64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
@@ -396,6 +400,12 @@ int scan_counts(rvsp_cuda_plan* plan, const int32_t* in, int64_t n, int64_t* out
     if (e != cudaSuccess) return fail(e, "scan workspace");
     int64_t* tmp = plan->scan_tmp.as<int64_t>();
     KTime kt(plan->stream, plan->capturing, KF_SCAN);
+    if (ntiles <= SCAN_SINGLE_TILES) {
+        k_scan_single<<<1, SCAN_TPB, 0, plan->stream>>>(in, n, total_dev, out64, out32,
+                                                        &plan->misc.as<Misc>()->overflow);
+        note_launch(plan, 1);
+        return RVSP_SUCCESS;
+    }
     k_scan_reduce<<<(unsigned)ntiles, SCAN_TPB, 0, plan->stream>>>(in, n, tmp);
     k_scan_tiles<<<1, SCAN_TPB, 0, plan->stream>>>(tmp, ntiles, total_dev);
     k_scan_apply<<<(unsigned)ntiles, SCAN_TPB, 0, plan->stream>>>(
@@ -465,7 +475,7 @@ int stage_operands(rvsp_cuda_plan* plan, const int32_t* a_rp, const int32_t* a_c
 
 // Analysis + binning. Leaves per-row op counts, bins and heavy items in the
 // plan; one device->host read of the bin histogram.
-int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool features,
+int analyze(rvsp_cuda_plan* plan, CsrView& A, CsrView& B, bool features,
             int (*pre_sync)(rvsp_cuda_plan*)) {
     const int64_t M = plan->a_rows;
     cudaError_t e;
@@ -490,7 +500,8 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     AnalyzeOut out{plan->ops.as<int64_t>(), plan->ub.as<int32_t>(), plan->bin.as<uint8_t>(),
                    plan->chunk_lo.as<int32_t>(), plan->nchunks.as<int32_t>(),
                    features ? plan->feat.as<float4>() : nullptr, misc->hist,
-                   plan->tile_hist.as<int32_t>(), misc->totals, misc->bin_prod, &misc->err};
+                   plan->tile_hist.as<int32_t>(), misc->totals, misc->bin_prod, &misc->err,
+                   misc->nnz_ab};
     {
         KTime kt(plan->stream, plan->capturing, KF_ANALYSIS);
         k_analyze<<<(unsigned)tiles, AN_TILE, 0, plan->stream>>>(A, B, out, plan->params);
@@ -508,6 +519,15 @@ int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool featu
     if (plan->host_misc.err) {
         g_err = "operand structure out of range (row_ptr or col_idx)";
         return RVSP_ERROR_INVALID_CSR;
+    }
+    // operands whose nnz the host did not know (-1): the analysis read it
+    if (plan->a_nnz < 0 || plan->b_nnz < 0) {
+        if (plan->host_misc.nnz_ab[0] < 0 || plan->host_misc.nnz_ab[1] < 0) {
+            g_err = "operand row pointer ends below zero";
+            return RVSP_ERROR_INVALID_CSR;
+        }
+        plan->a_nnz = A.nnz = plan->host_misc.nnz_ab[0];
+        plan->b_nnz = B.nnz = plan->host_misc.nnz_ab[1];
     }
     int32_t acc = 0;
     for (int b = 0; b < NUM_BINS; ++b) {
@@ -627,6 +647,14 @@ void launch_bin_scatter(rvsp_cuda_plan* plan, const uint8_t* bin, const int32_t*
 
 // Exact count + scan: C's row pointer in plan->c_rp, nnz in plan->c_nnz.
 int count_exact(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
+    int st = count_launch(plan, A, B);
+    return st ? st : count_read(plan);
+}
+
+// The count kernels and scans, enqueued only: C's row pointer lands in
+// plan->c_rp, the heavy chunks' offsets in plan->item_scan, nnz(C) in
+// Misc::scan_total.
+int count_launch(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
     cudaError_t e;
     const int64_t M = plan->a_rows;
     if ((e = cudaMemsetAsync(plan->cnt.p, 0, M * 4, plan->stream)) != cudaSuccess)
@@ -644,6 +672,13 @@ int count_exact(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B) {
     }
     plan->items_counted = true;
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "count launch");
+    return RVSP_SUCCESS;
+}
+
+// Waits for count_launch's work and takes nnz(C) into plan->c_nnz.
+int count_read(rvsp_cuda_plan* plan) {
+    cudaError_t e;
+    Misc* misc = plan->misc.as<Misc>();
     if ((e = cudaMemcpyAsync(&plan->host_misc, misc, sizeof(Misc), cudaMemcpyDeviceToHost,
                              plan->stream)) != cudaSuccess)
         return fail(e, "count read");
@@ -1087,6 +1122,101 @@ int rvsp_cuda_numeric(rvsp_cuda_plan_t plan, const int32_t* a_rp, const int32_t*
     }
     return RVSP_SUCCESS;
 }
+
+}  // extern "C"
+
+namespace rvsp {
+
+// Products up to which the one-shot allocates C at the product count (an
+// upper bound on nnz(C): at most 256 MB of C) and runs count, scan and fill
+// back to back, reading nnz(C) back once at the end instead of between the
+// count and the fill.
+constexpr int64_t ONESHOT_FUSED_PRODUCTS = int64_t(1) << 25;
+
+int oneshot_exact_device(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t b_cols,
+                         const int32_t* a_rp, const int32_t* a_ci, const float* a_v,
+                         const int32_t* b_rp, const int32_t* b_ci, const float* b_v,
+                         int32_t** c_rp_out, int32_t** c_ci_out, float** c_v_out,
+                         int64_t* c_nnz_out) {
+    plan->analysed = false;
+    plan->maps_ready = false;
+    plan->filled = nullptr;
+    plan->filled_host = nullptr;
+    reset_graph(plan);
+    plan->a_rows = a_rows;
+    plan->a_cols = a_cols;
+    plan->a_nnz = -1;  // read by the analysis
+    plan->b_rows = a_cols;
+    plan->b_cols = b_cols;
+    plan->b_nnz = -1;
+    memset(plan->key, 0, sizeof(plan->key));
+    CsrView A, B;
+    int st = stage_operands(plan, a_rp, a_ci, a_v, b_rp, b_ci, b_v, false, &A, &B);
+    if (st) return st;
+    if ((st = analyze(plan, A, B, plan->features))) return st;
+    const int64_t M = a_rows;
+    const bool fused = plan->products <= ONESHOT_FUSED_PRODUCTS;
+    int64_t cap;
+    if (fused) {
+        if ((st = count_launch(plan, A, B))) return st;
+        cap = plan->products;
+    } else {
+        if ((st = count_exact(plan, A, B))) return st;
+        cap = plan->c_nnz;
+    }
+    int32_t *rp = nullptr, *ci = nullptr;
+    float* v = nullptr;
+    const size_t alloc = cap > 0 ? (size_t)cap : 1;
+    cudaError_t e = cudaMallocAsync((void**)&rp, ((size_t)M + 1) * 4, plan->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&ci, alloc * 4, plan->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&v, alloc * 4, plan->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(rp, plan->c_rp.p, ((size_t)M + 1) * 4, cudaMemcpyDeviceToDevice,
+                            plan->stream);
+    Misc* misc = plan->misc.as<Misc>();
+    if (e == cudaSuccess) {
+        RowOut o{nullptr, plan->c_rp.as<int32_t>(), ci, v, &misc->err, false};
+        run_rows(plan, FILL, A, B, o);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&plan->host_misc, misc, sizeof(Misc), cudaMemcpyDeviceToHost,
+                            plan->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(plan->stream);
+    trace_point("one-shot exact (synced)");
+    const auto release = [&] {
+        if (rp) cudaFreeAsync(rp, plan->stream);
+        if (ci) cudaFreeAsync(ci, plan->stream);
+        if (v) cudaFreeAsync(v, plan->stream);
+    };
+    if (e != cudaSuccess) {
+        release();
+        return fail(e, "one-shot product");
+    }
+    if (plan->host_misc.err) {
+        release();
+        g_err = "operand structure out of range (row_ptr or col_idx)";
+        return RVSP_ERROR_INVALID_CSR;
+    }
+    if (fused) {
+        if (plan->host_misc.overflow || plan->host_misc.scan_total > INT32_MAX) {
+            release();
+            g_err = "nnz(C) exceeds INT32_MAX";
+            return RVSP_ERROR_ALLOCATION_FAILED;
+        }
+        plan->c_nnz = plan->host_misc.scan_total;
+    }
+    plan->analysed = true;
+    *c_rp_out = rp;
+    *c_ci_out = ci;
+    *c_v_out = v;
+    *c_nnz_out = plan->c_nnz;
+    return RVSP_SUCCESS;
+}
+
+}  // namespace rvsp
+
+extern "C" {
 
 int rvsp_cuda_op_counts(rvsp_cuda_plan_t plan, int64_t* out, int32_t n) {
     if (!plan || !out) return RVSP_ERROR_NULL_POINTER;

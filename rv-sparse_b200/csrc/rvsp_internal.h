@@ -52,6 +52,8 @@ struct Misc {
     int32_t heavy_queue;       // next heavy work item of the running launch
     int32_t row_queue;         // next row of the running warp-bin launch
     unsigned long long pool_fill;  // learned path: entries placed in the overflow pool
+    int32_t nnz_ab[2];         // nnz of A and B as the analysis read them (operands
+                               // whose nnz the host did not know)
 };
 
 // Output pointers of a row-kernel launch.
@@ -209,9 +211,19 @@ namespace rvsp {
 int stage_operands(rvsp_cuda_plan* plan, const int32_t* a_rp, const int32_t* a_ci,
                    const float* a_v, const int32_t* b_rp, const int32_t* b_ci, const float* b_v,
                    bool cache_index, CsrView* A, CsrView* B);
-int analyze(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool features,
+int analyze(rvsp_cuda_plan* plan, CsrView& A, CsrView& B, bool features,
             int (*pre_sync)(rvsp_cuda_plan*) = nullptr);
 int count_exact(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B);
+int count_launch(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B);
+int count_read(rvsp_cuda_plan* plan);
+// One-shot exact product of device-resident operands into new device arrays
+// (rvsp_cuda_spgemm_f32's exact path when every operand array is on the
+// device; the operands' nnz are read by the analysis).
+int oneshot_exact_device(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t b_cols,
+                         const int32_t* a_rp, const int32_t* a_ci, const float* a_v,
+                         const int32_t* b_rp, const int32_t* b_ci, const float* b_v,
+                         int32_t** c_rp_out, int32_t** c_ci_out, float** c_v_out,
+                         int64_t* c_nnz_out);
 void run_rows(rvsp_cuda_plan* plan, int mode, const CsrView& A, const CsrView& B,
               const RowOut& o);
 int scan_counts(rvsp_cuda_plan* plan, const int32_t* in, int64_t n, int64_t* out64,
@@ -221,7 +233,7 @@ void reset_graph(rvsp_cuda_plan* plan);
 int build_heavy_aux(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B);
 void launch_bin_scatter(rvsp_cuda_plan* plan, const uint8_t* bin, const int32_t* tile_off,
                         int32_t* bin_rows, bool heavy_items);
-int learned_symbolic(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, bool fused);
+int learned_symbolic(rvsp_cuda_plan* plan, CsrView& A, CsrView& B, bool fused);
 int learned_finish(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B, int32_t* c_ci,
                    float* c_v);
 int learned_spgemm(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t a_nnz,

@@ -114,15 +114,31 @@ extern "C" int rvsp_cuda_spgemm_f32(int algo, int32_t a_rows, int32_t a_cols, in
         if ((st = rvsp_cuda_plan_create(&plan, algo))) return st;
         plan->map_policy = 0;  // a one-shot product is never reused
     }
-    int32_t a_nnz = 0, b_nnz = 0;
+    int32_t a_nnz = -1, b_nnz = -1;
     trace_point("one-shot: enter");
-    if ((st = read_ends(plan, a_rp + a_rows, b_rp + a_cols, &a_nnz, &b_nnz))) return st;
-    trace_point("one-shot: operand nnz read");
-    plan->params = default_params();
     const bool dev = is_dev(a_rp);
+    // every operand array on the device: the analysis reads the operands'
+    // nnz itself (returned with the bin counts), no round trip of its own
+    const bool all_dev = dev && is_dev(a_ci) && is_dev(a_v) && is_dev(b_rp) && is_dev(b_ci) &&
+                         is_dev(b_v);
+    if (!all_dev && (st = read_ends(plan, a_rp + a_rows, b_rp + a_cols, &a_nnz, &b_nnz)))
+        return st;
+    trace_point("one-shot: operand nnz");
+    plan->params = default_params();
     keep_pool_memory();
 
-    if (algo == RVSP_CUDA_ALGO_LEARNED) {
+    if (algo == RVSP_CUDA_ALGO_EXACT && all_dev) {
+        int64_t nnz = 0;
+        int32_t *rp = nullptr, *ci = nullptr;
+        float* v = nullptr;
+        st = oneshot_exact_device(plan, a_rows, a_cols, b_cols, a_rp, a_ci, a_v, b_rp, b_ci, b_v,
+                                  &rp, &ci, &v, &nnz);
+        if (st) return st;
+        *c_rp_out = rp;
+        *c_ci_out = ci;
+        *c_v_out = v;
+        *c_nnz_out = (int32_t)nnz;
+    } else if (algo == RVSP_CUDA_ALGO_LEARNED) {
         st = learned_spgemm(plan, a_rows, a_cols, a_nnz, a_rp, a_ci, a_v, a_cols, b_cols,
                             b_nnz, b_rp, b_ci, b_v, dev ? 1 : 0, c_rp_out, c_ci_out, c_v_out,
                             c_nnz_out);

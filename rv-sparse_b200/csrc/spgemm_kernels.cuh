@@ -145,6 +145,7 @@ struct AnalyzeOut {
     int64_t* totals;     // [0] heavy items, [1] products
     int64_t* bin_prod;   // [NUM_BINS] products per bin
     int32_t* err;        // ERR_* bits
+    int32_t* nnz_ab;     // [2] nnz of A and B as the kernel used them (read back with the bins)
 };
 
 // Sum of a 64-bit value over the whole warp (result on every lane).
@@ -188,6 +189,16 @@ __global__ void __launch_bounds__(AN_TILE)
     __shared__ unsigned long long s_items, s_prod;
     __shared__ int s_long;
 
+    // An operand's nnz passed as -1 is not known on the host (a device-
+    // resident one-shot operand): it is the last entry of its row pointer,
+    // read here instead of in a host round trip of its own, and returned
+    // with the bin counts.
+    if (A.nnz < 0) A.nnz = A.rp[A.rows];
+    if (B.nnz < 0) B.nnz = B.rp[B.rows];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        out.nnz_ab[0] = A.nnz;
+        out.nnz_ab[1] = B.nnz;
+    }
     const int r0 = blockIdx.x * AN_TILE;
     const int nr = min(AN_TILE, A.rows - r0);
     const int t = threadIdx.x;
@@ -1800,6 +1811,50 @@ __global__ void __launch_bounds__(SCAN_TPB)
         if (out32) {
             out32[n] = (int32_t)tot;
             ovf |= tot > INT32_MAX;
+        }
+    }
+    if (ovf) atomicExch(overflow, 1);
+}
+
+// Short arrays: the whole exclusive scan in one CTA, tile after tile with a
+// running carry (one launch instead of three); outputs as k_scan_apply's.
+__global__ void __launch_bounds__(SCAN_TPB)
+    k_scan_single(const int32_t* __restrict__ in, int64_t n, int64_t* __restrict__ total,
+                  int64_t* __restrict__ out64, int32_t* __restrict__ out32,
+                  int32_t* __restrict__ overflow) {
+    __shared__ int64_t s_total;
+    int64_t carry = 0;
+    bool ovf = false;
+    for (int64_t t0 = 0; t0 < n; t0 += SCAN_TILE) {
+        const int64_t base = t0 + (int64_t)threadIdx.x * SCAN_ITEMS;
+        int32_t v[SCAN_ITEMS];
+        int64_t s = 0;
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS; ++i) {
+            v[i] = base + i < n ? in[base + i] : 0;
+            s += v[i];
+        }
+        int64_t run = carry + block_excl_scan64(s, &s_total);
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS; ++i) {
+            if (base + i < n) {
+                if (out64) out64[base + i] = run;
+                if (out32) {
+                    out32[base + i] = (int32_t)run;
+                    ovf |= run > INT32_MAX;
+                }
+            }
+            run += v[i];
+        }
+        carry += s_total;
+        __syncthreads();  // every thread has read s_total before the next tile's scan
+    }
+    if (threadIdx.x == 0) {
+        *total = carry;
+        if (out64) out64[n] = carry;
+        if (out32) {
+            out32[n] = (int32_t)carry;
+            ovf |= carry > INT32_MAX;
         }
     }
     if (ovf) atomicExch(overflow, 1);
