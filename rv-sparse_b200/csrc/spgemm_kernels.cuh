@@ -221,20 +221,39 @@ __global__ void __launch_bounds__(AN_TILE)
         if (s0 < 0 || s1 < s0 || s1 > A.nnz) {
             atomicOr(out.err, ERR_STRUCTURE);
         } else if (s1 - s0 <= AN_SHORT) {
-            for (int p = s0; p < s1; ++p) {
-                int bs, be;
-                row_range(B, A.ci[p], &bs, &be, out.err);
-                const int len = be - bs;
-                if (len > 0) {
-                    const int first = B.ci[bs], last = B.ci[be - 1];
-                    if (first < 0 || last >= B.cols || last < first) {
+            // four entries at a time, phase by phase (their B rows, the rows'
+            // bounds, the rows' first and last columns), so each phase's
+            // loads are in flight together instead of one chain per entry
+            for (int p0 = s0; p0 < s1; p0 += 4) {
+                int k[4], bs[4], be[4], first[4], last[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) k[u] = p0 + u < s1 ? A.ci[p0 + u] : 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    bs[u] = be[u] = 0;
+                    if (p0 + u < s1) row_range(B, k[u], &bs[u], &be[u], out.err);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    first[u] = 0;
+                    last[u] = -1;
+                    if (be[u] > bs[u]) {
+                        first[u] = B.ci[bs[u]];
+                        last[u] = B.ci[be[u] - 1];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int len = be[u] - bs[u];
+                    if (len <= 0) continue;
+                    if (first[u] < 0 || last[u] >= B.cols || last[u] < first[u]) {
                         atomicOr(out.err, ERR_STRUCTURE);
                         continue;
                     }
                     ops += (unsigned long long)len;
                     maxlen = max(maxlen, len);
-                    minc = min(minc, first);
-                    maxc = max(maxc, last);
+                    minc = min(minc, first[u]);
+                    maxc = max(maxc, last[u]);
                 }
             }
         } else {
