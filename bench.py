@@ -870,7 +870,12 @@ def compare_batched(rv, torch, steps, warmup, count=512):
             ptrs, n, offs, coffs = rv.spgemm_batched(dev_pairs, algo)
             rv.free_device(*ptrs)
         times[name] = _time(fn, steps, warmup, torch)
+    torch.cuda.synchronize()
+    rv.kernel_timing(True)
     ptrs, n, offs, coffs = rv.spgemm_batched(dev_pairs, rv.RVSP_CUDA_ALGO_LEARNED)
+    torch.cuda.synchronize()
+    kt = {k: round(v[0], 3) for k, v in rv.kernel_times().items() if v[1]}
+    rv.kernel_timing(False)
     total_rows = int(offs[-1])
     crp = _d2h(ptrs[0], total_rows + len(pairs), np.int32, torch).astype(np.int64)
     ok = True
@@ -893,7 +898,8 @@ def compare_batched(rv, torch, steps, warmup, count=512):
             "batched_learned_over_sequential": times["sequential_exact"] / times["batched_learned"],
             "batched_learned_over_batched_exact": times["batched_exact"] / times["batched_learned"],
             "products_checked_vs_oracle": check,
-            "spot_check_bit_exact_vs_oracle": bool(ok)}
+            "spot_check_bit_exact_vs_oracle": bool(ok),
+            "kernel_ms_batched_learned": kt}
 
 
 def run_extras(args, rv, torch):

@@ -407,7 +407,7 @@ RVSP_CUDA_API int64_t rvsp_cuda_launch_count(void);
  * RVSP_CUDA_KERNEL_FAMILIES. rvsp_cuda_kernel_family(i) names family i
  * (NULL out of range).
  */
-#define RVSP_CUDA_KERNEL_FAMILIES 13
+#define RVSP_CUDA_KERNEL_FAMILIES 14
 RVSP_CUDA_API int rvsp_cuda_kernel_timing(int on);
 RVSP_CUDA_API int rvsp_cuda_kernel_times(double *ms_out, int64_t *launches_out, int32_t n);
 RVSP_CUDA_API const char *rvsp_cuda_kernel_family(int32_t i);

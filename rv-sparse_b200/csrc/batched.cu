@@ -115,6 +115,7 @@ int pack(cudaStream_t st, int32_t count, const int32_t* rows, const int32_t* nnz
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(dtiles, tiles.data(), 8 * (count + 1), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
+        KTime kt(st, false, KF_PACK);
         k_pack<<<(unsigned)tiles[count], 256, 0, st>>>((const PackSrc*)dsrc, (const int64_t*)dtiles,
                                                        count, out->rp, out->ci, out->v, err);
         note_launch(nullptr, 1);

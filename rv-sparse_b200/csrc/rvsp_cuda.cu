@@ -827,7 +827,7 @@ const char* rvsp_cuda_kernel_family(int32_t i) {
     static const char* names[KF_NUM] = {
         "k_tiny<COUNT>", "k_tiny<FILL>", "k_tiny_reuse", "k_warp<COUNT>", "k_warp<FILL>",
         "k_warp_reuse", "k_heavy<COUNT>", "k_heavy<FILL>", "k_heavy<REUSE>", "analysis",
-        "scan", "learned_sizing", "k_compact"};
+        "scan", "learned_sizing", "k_compact", "batched_pack"};
     return i >= 0 && i < KF_NUM ? names[i] : nullptr;
 }
 

@@ -112,6 +112,7 @@ enum KernelFamily : int {
     KF_SCAN,      // prefix sums
     KF_LEARNED,   // inference, predicted bins, re-run masks
     KF_COMPACT,   // slot -> C copies of the learned path
+    KF_PACK,      // batched products: operands stacked into one product
     KF_NUM
 };
 bool ktime_enabled();

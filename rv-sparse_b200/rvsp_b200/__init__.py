@@ -194,7 +194,7 @@ def launch_count() -> int:
     return lib().rvsp_cuda_launch_count()
 
 
-KERNEL_FAMILIES = 13
+KERNEL_FAMILIES = 14
 
 
 def kernel_timing(on: bool) -> None:
