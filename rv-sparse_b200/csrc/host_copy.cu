@@ -33,6 +33,7 @@
 #include <thread>
 #include <vector>
 
+#include "rvsp_cuda.h"
 #include "rvsp_internal.h"
 
 namespace rvsp {
@@ -275,5 +276,4 @@ cudaError_t copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t 
 
 }  // namespace rvsp
 
-// For the C API (csrc/rvsp_api.c): release a host array the library allocated.
-extern "C" void rvsp_host_free(void* p) { rvsp::host_free(p); }
+extern "C" RVSP_CUDA_API void rvsp_cuda_host_free(void* p) { rvsp::host_free(p); }

@@ -15,10 +15,6 @@
 #include "rv_sparse.h"
 #include "rvsp_cuda.h"
 
-/* host_copy.cu: releases a host array the library allocated (free() or the
- * library's cache of released result arrays) */
-void rvsp_host_free(void *p);
-
 const char *rvsp_get_version(void)
 {
     return "0.1.0";
@@ -105,9 +101,9 @@ void rvsp_csr_destroy(rvsp_csr_matrix_t *A)
         return;
     if (A->owns_data == RVSP_OWNS_HOST)
     {
-        rvsp_host_free(A->row_ptr);
-        rvsp_host_free(A->col_idx);
-        rvsp_host_free(A->values);
+        rvsp_cuda_host_free(A->row_ptr);
+        rvsp_cuda_host_free(A->col_idx);
+        rvsp_cuda_host_free(A->values);
     }
     else if (A->owns_data == RVSP_OWNS_DEVICE)
     {

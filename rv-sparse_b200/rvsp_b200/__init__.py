@@ -91,6 +91,7 @@ _PROTOS = {
     "rvsp_cuda_last_error": (C.c_char_p, []),
     "rvsp_cuda_is_device_pointer": (C.c_int, [_VP]),
     "rvsp_cuda_free": (None, [_VP]),
+    "rvsp_cuda_host_free": (None, [_VP]),
     "rvsp_cuda_plan_create": (C.c_int, [C.POINTER(_VP), C.c_int]),
     "rvsp_cuda_plan_destroy": (None, [_VP]),
     "rvsp_cuda_plan_set_async": (C.c_int, [_VP, C.c_int]),
