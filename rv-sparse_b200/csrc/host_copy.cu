@@ -8,7 +8,10 @@
 // copy: about 2 GB/s for a C of several GB. Here the device copies C in
 // CHUNK-byte pieces into a ring of pinned buffers, and a team of host
 // threads moves each finished piece into the destination, so the PCIe
-// transfer, the destination's page faults and the host copies overlap. The
+// transfer, the destination's page faults and the host copies overlap.
+// Large pageable operands go up the same way in reverse (copy_to_device):
+// host threads fill the pinned pieces, each piece's upload is enqueued as
+// soon as it is full. The
 // arrays host_alloc hands out are 2 MiB aligned with transparent huge pages
 // advised, which cuts their page faults 512-fold, and free() releases them.
 //
@@ -41,7 +44,7 @@ namespace rvsp {
 namespace {
 
 constexpr size_t HUGE_PAGE = 2u << 20;
-constexpr size_t CHUNK = 16u << 20;      // one device->host piece
+constexpr size_t CHUNK = 32u << 20;      // one piece between device and host
 constexpr int RING = 16;                 // pinned pieces in flight
 constexpr size_t STAGED_MIN = 64u << 20;  // smaller copies go direct
 constexpr int MAX_DEVICES = 16;
@@ -122,6 +125,16 @@ size_t cache_cap() {
     return cap;
 }
 
+// a stream recording a CUDA graph takes no host waits: plain copies there
+bool capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return st != cudaStreamCaptureStatusNone;
+}
+
 bool pinned_host(const void* p) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -178,6 +191,9 @@ void host_free(void* p) {
 }
 
 cudaError_t copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    if (capturing(stream))  // recorded into the graph; no host wait allowed
+        return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream)
+                     : cudaSuccess;
     if (bytes == 0) return cudaStreamSynchronize(stream);
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
@@ -189,6 +205,7 @@ cudaError_t copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t 
     }
     std::lock_guard<std::mutex> hold(g_ring_mu[dev]);
     Ring& r = g_ring[dev];
+    trace_point("host copy-back: start");
     if (!ring_ready(r)) {
         e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream);
         return e == cudaSuccess ? cudaStreamSynchronize(stream) : e;
@@ -269,8 +286,94 @@ cudaError_t copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t 
     }
     cv.notify_all();
     for (auto& t : team) t.join();
+    trace_point("host copy-back (staged)");
     // every issued device copy has ended before a ring slot is used again
     const cudaError_t s = cudaStreamSynchronize(stream);
+    return err.load() != cudaSuccess ? (cudaError_t)err.load() : s;
+}
+
+cudaError_t copy_to_device(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    if (bytes == 0) return cudaSuccess;
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const int threads = copy_threads();
+    if (bytes < STAGED_MIN || dev < 0 || dev >= MAX_DEVICES || threads < 2 || pinned_host(src) ||
+        capturing(stream))
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
+    std::lock_guard<std::mutex> hold(g_ring_mu[dev]);
+    Ring& r = g_ring[dev];
+    if (!ring_ready(r)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
+    trace_point("host upload: start");
+    const size_t n = (bytes + CHUNK - 1) / CHUNK;
+    auto piece = [&](size_t i) { return i + 1 < n ? CHUNK : bytes - i * CHUNK; };
+    // filled[i % RING]: the last piece copied into that slot, + 1; issued:
+    // pieces whose upload is enqueued (a slot is free again once the upload
+    // of the piece RING before has completed: its event)
+    std::mutex mu;
+    std::condition_variable cv;
+    size_t issued = 0;
+    size_t filled[RING] = {};
+    std::atomic<size_t> next{0};
+    std::atomic<int> err{cudaSuccess};
+    auto worker = [&] {
+        cudaSetDevice(dev);
+        for (;;) {
+            const size_t i = next.fetch_add(1);
+            if (i >= n) return;
+            const int b = (int)(i % RING);
+            if (i >= (size_t)RING) {
+                {
+                    std::unique_lock<std::mutex> lk(mu);
+                    cv.wait(lk, [&] { return issued > i - RING || err.load() != cudaSuccess; });
+                }
+                if (err.load() != cudaSuccess) return;
+                const cudaError_t x = cudaEventSynchronize(r.ev[b]);
+                if (x != cudaSuccess) {
+                    {
+                        std::lock_guard<std::mutex> lk(mu);
+                        int none = cudaSuccess;
+                        err.compare_exchange_strong(none, (int)x);
+                    }
+                    cv.notify_all();
+                    return;
+                }
+            }
+            memcpy(r.pin[b], (const char*)src + i * CHUNK, piece(i));
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                filled[b] = i + 1;
+            }
+            cv.notify_all();
+        }
+    };
+    std::vector<std::thread> team;
+    team.reserve(threads);
+    for (int t = 0; t < threads; ++t) team.emplace_back(worker);
+    for (size_t i = 0; i < n; ++i) {
+        const int b = (int)(i % RING);
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&] { return filled[b] == i + 1 || err.load() != cudaSuccess; });
+            if (err.load() != cudaSuccess) break;
+        }
+        cudaError_t x = cudaMemcpyAsync((char*)dst + i * CHUNK, r.pin[b], piece(i),
+                                        cudaMemcpyHostToDevice, stream);
+        if (x == cudaSuccess) x = cudaEventRecord(r.ev[b], stream);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            if (x != cudaSuccess) err = (int)x;
+            else issued = i + 1;
+        }
+        cv.notify_all();
+        if (x != cudaSuccess) break;
+    }
+    cv.notify_all();
+    for (auto& t : team) t.join();
+    // the ring's pieces are free for the next user only once every upload
+    // from them has completed
+    const cudaError_t s = cudaStreamSynchronize(stream);
+    trace_point("host upload (staged)");
     return err.load() != cudaSuccess ? (cudaError_t)err.load() : s;
 }
 

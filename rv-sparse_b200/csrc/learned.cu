@@ -653,6 +653,7 @@ int learned_spgemm(rvsp_cuda_plan* plan, int32_t a_rows, int32_t a_cols, int32_t
             cudaFreeAsync(v, plan->stream);
             return RVSP_ERROR_ALLOCATION_FAILED;
         }
+        trace_point("learned: host C allocated");
         e = copy_to_host(hrp, rp, ((size_t)a_rows + 1) * 4, plan->stream);
         if (e == cudaSuccess) e = copy_to_host(hci, ci, (size_t)nnz * 4, plan->stream);
         if (e == cudaSuccess) e = copy_to_host(hv, v, (size_t)nnz * 4, plan->stream);

@@ -433,7 +433,7 @@ static int resolve(rvsp_cuda_plan* plan, DevBuf& buf, const void*& key, const T*
     if (!(cache_ok && key == ptr && buf.p)) {
         cudaError_t e = buf.ensure(n * sizeof(T));
         if (e != cudaSuccess) return fail(e, "staging alloc");
-        e = cudaMemcpyAsync(buf.p, ptr, n * sizeof(T), cudaMemcpyHostToDevice, plan->stream);
+        e = copy_to_device(buf.p, ptr, n * sizeof(T), plan->stream);
         if (e != cudaSuccess) return fail(e, "staging copy");
         key = ptr;
     }

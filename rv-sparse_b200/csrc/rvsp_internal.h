@@ -96,9 +96,14 @@ void* host_alloc(size_t bytes);
 // Release a host array (any free()-compatible block): large ones go to the
 // cache that host_alloc draws from, the rest to free().
 void host_free(void* p);
-// Device->host copy of bytes into dst, finished on return; large copies into
-// pageable memory are staged through pinned pieces and host threads.
+// Device->host copy of bytes into dst, finished on return (enqueued only on a
+// stream that is recording a graph); large copies into pageable memory are
+// staged through pinned pieces and host threads.
 cudaError_t copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t stream);
+// Host->device copy of bytes from src, enqueued on stream; large copies from
+// pageable memory are staged through the pinned pieces (those return once
+// the upload has completed), the rest are plain cudaMemcpyAsync calls.
+cudaError_t copy_to_device(void* dst, const void* src, size_t bytes, cudaStream_t stream);
 
 // Opt-in device timing of the kernels by family (rvsp_cuda_kernel_timing):
 // a KTime scope records a CUDA event pair around the launches it covers on
