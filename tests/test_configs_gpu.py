@@ -86,6 +86,21 @@ def test_host_output_of_a_large_product_matches_the_device_output(gpu_lib):
         _same(oneshot(R, R, algo=algo, device=False), want, f"host C {name}")
 
 
+def test_large_host_operands_are_uploaded_staged(gpu_lib):
+    """Host operands of 64 MiB and more per array go up through the pinned
+    pieces and host threads (B: 1,000,000 rows of 20 entries, 80 MB per
+    array): C bit-identical to the product of the same operands on the
+    device, exact and learned, and to the oracle."""
+    from gpu_util import oneshot
+    B = gen.uniform_fixed(rows=1_000_000, cols=1_000_000, per_row=20, seed=3)
+    A = gen.uniform_fixed(rows=2000, cols=1_000_000, per_row=4, seed=4)
+    assert B.col_idx.nbytes >= 64 << 20
+    want = oracle.spgemm_f32(A, B)
+    for name, algo in ALGOS:
+        _same(oneshot(A, B, algo=algo, device=False), want, f"host operands {name}")
+        _same(oneshot(A, B, algo=algo, device=True), want, f"device operands {name}")
+
+
 def test_host_results_through_the_public_api_reuse_released_arrays(gpu_lib):
     """rvsp_spgemm_csr with host operands, twice per backend, the first C
     released by rvsp_csr_destroy before the second product (large released
