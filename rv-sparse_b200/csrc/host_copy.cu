@@ -46,7 +46,8 @@ namespace {
 constexpr size_t HUGE_PAGE = 2u << 20;
 constexpr size_t CHUNK = 32u << 20;      // one piece between device and host
 constexpr int RING = 16;                 // pinned pieces in flight
-constexpr size_t STAGED_MIN = 64u << 20;  // smaller copies go direct
+constexpr size_t STAGED_MIN = 64u << 20;  // smaller copy-backs go direct
+constexpr size_t STAGED_MIN_UP = 16u << 20;  // smaller uploads go direct
 constexpr int MAX_DEVICES = 16;
 constexpr int MAX_THREADS = 16;
 
@@ -298,8 +299,8 @@ cudaError_t copy_to_device(void* dst, const void* src, size_t bytes, cudaStream_
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     const int threads = copy_threads();
-    if (bytes < STAGED_MIN || dev < 0 || dev >= MAX_DEVICES || threads < 2 || pinned_host(src) ||
-        capturing(stream))
+    if (bytes < STAGED_MIN_UP || dev < 0 || dev >= MAX_DEVICES || threads < 2 ||
+        pinned_host(src) || capturing(stream))
         return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
     std::lock_guard<std::mutex> hold(g_ring_mu[dev]);
     Ring& r = g_ring[dev];
