@@ -266,24 +266,58 @@ __global__ void __launch_bounds__(AN_TILE)
     }
     __syncthreads();
     if (s_long) {
-        // long rows: the CTA strides over the tile's entries, skipping short rows
+        // long rows: the CTA strides over the tile's entries, skipping short
+        // rows; a warp whose entries all fall in one row (a long row's
+        // stretch) combines them in registers and updates the row once,
+        // instead of 32 lanes contending for the same shared counters
         const int p0 = max(s_rp[0], 0), p1 = min(s_rp[nr], A.nnz);
-        for (int p = p0 + t; p < p1; p += blockDim.x) {
-            int lo = 0, hi = nr;  // largest i with s_rp[i] <= p
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (s_rp[mid] <= p) lo = mid; else hi = mid;
-            }
-            if (s_rp[lo + 1] - s_rp[lo] <= AN_SHORT) continue;
-            int bs, be;
-            row_range(B, A.ci[p], &bs, &be, out.err);
-            const int len = be - bs;
-            if (len > 0) {
-                const int first = B.ci[bs], last = B.ci[be - 1];
-                if (first < 0 || last >= B.cols || last < first) {
-                    atomicOr(out.err, ERR_STRUCTURE);
-                    continue;
+        const int lane = t & 31;
+        for (int base = p0 + (t & ~31); base < p1; base += blockDim.x) {
+            const int p = base + lane;
+            int lo = -1, len = 0, first = INT_MAX, last = -1;
+            if (p < p1) {
+                int l = 0, h = nr;  // largest i with s_rp[i] <= p
+                while (h - l > 1) {
+                    const int mid = (l + h) >> 1;
+                    if (s_rp[mid] <= p) l = mid; else h = mid;
                 }
+                if (s_rp[l + 1] - s_rp[l] > AN_SHORT) {
+                    int bs, be;
+                    row_range(B, A.ci[p], &bs, &be, out.err);
+                    if (be > bs) {
+                        const int f = B.ci[bs], g = B.ci[be - 1];
+                        if (f < 0 || g >= B.cols || g < f) {
+                            atomicOr(out.err, ERR_STRUCTURE);
+                        } else {
+                            lo = l;
+                            len = be - bs;
+                            first = f;
+                            last = g;
+                        }
+                    }
+                }
+            }
+            const unsigned has = __ballot_sync(FULL, lo >= 0);
+            if (!has) continue;
+            const int lead = __ffs(has) - 1;
+            const int lrow = __shfl_sync(FULL, lo, lead);
+            if (__all_sync(FULL, lo < 0 || lo == lrow)) {
+                unsigned long long sum = (unsigned long long)len;
+                int mxl = len, mnc = first, mxc = last;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    sum += __shfl_xor_sync(FULL, sum, o);
+                    mxl = max(mxl, __shfl_xor_sync(FULL, mxl, o));
+                    mnc = min(mnc, __shfl_xor_sync(FULL, mnc, o));
+                    mxc = max(mxc, __shfl_xor_sync(FULL, mxc, o));
+                }
+                if (lane == lead) {
+                    atomicAdd(&s_ops[lrow], sum);
+                    atomicMax(&s_maxlen[lrow], mxl);
+                    atomicMin(&s_minc[lrow], mnc);
+                    atomicMax(&s_maxc[lrow], mxc);
+                }
+            } else if (lo >= 0) {
                 atomicAdd(&s_ops[lo], (unsigned long long)len);
                 atomicMax(&s_maxlen[lo], len);
                 atomicMin(&s_minc[lo], first);
