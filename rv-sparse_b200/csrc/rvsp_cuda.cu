@@ -357,8 +357,9 @@ static void launch_bins(rvsp_cuda_plan* plan, const CsrView& A, const CsrView& B
             }
         } else if (plan->n_items > 0) {
             KTime kt(plan->stream, plan->capturing, KF_HEAVY_COUNT + MODE);
+            // (the learned sweep reaches here only with heavy slots, where every
+            // row of the heavy items is kept heavy: no row mask to check)
             RowCtl ctl = o.ctl;
-            if (o.learned_bins) ctl.only = plan->hmask.as<uint8_t>();  // rows kept heavy
             const int cl = plan->params.heavy_cw_log2;
             const int W = g_heavy_w[MODE][cl];
             const int64_t fill = (int64_t)g_sms * g_heavy_ctas[MODE][cl];
