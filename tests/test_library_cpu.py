@@ -143,3 +143,20 @@ def test_plan_requires_device_or_valid_algo():
         assert L.rvsp_cuda_plan_create(C.byref(p), rv.RVSP_CUDA_ALGO_EXACT) == -5
     L.rvsp_cuda_plan_destroy(None)
     assert L.rvsp_cuda_is_device_pointer(rv.ptr(np.zeros(4, np.int32))) == 0
+
+
+def test_host_free_takes_any_malloc_block():
+    """rvsp_cuda_host_free releases host result arrays: any block malloc (or
+    the library) returned, NULL included. Blocks of 64 MiB and more are kept
+    for reuse, at most four at a time (the oldest are freed): a run of large
+    releases passes through the keeping and the eviction."""
+    L = rv.lib()
+    libc = C.CDLL(None)
+    libc.malloc.restype = C.c_void_p
+    libc.malloc.argtypes = [C.c_size_t]
+    L.rvsp_cuda_host_free(None)
+    for mib in (1, 80, 80, 100, 70, 90, 200, 65, 2):
+        p = libc.malloc(mib << 20)
+        assert p
+        C.memset(p, 0xA5, mib << 20)
+        L.rvsp_cuda_host_free(p)
