@@ -1324,8 +1324,10 @@ __global__ void __launch_bounds__(WARPS * 32)
 // ---------------------------------------------------------------------------
 constexpr int HEAVY_SEG = 12;  // in-chunk B segments this long are walked on their own
 
+// COUNT walks two neighbouring chunks of a row at once (k_heavy): a bitmap of
+// 2 cw bits.
 __host__ __device__ constexpr int heavy_smem_bytes(int mode, int cw) {
-    return (mode == COUNT ? 0 : 4 * cw) + (mode == REUSE ? 0 : cw / 8);
+    return mode == COUNT ? cw / 4 : 4 * cw + (mode == REUSE ? 0 : cw / 8);
 }
 
 // First index in [lo, hi) with a[idx] >= target (hi if none); one thread.
@@ -1676,7 +1678,7 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
         for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     if (MODE != REUSE)
-        for (int x = lane; x < nw; x += 32) bits[x] = 0u;
+        for (int x = lane; x < (MODE == COUNT ? 2 * nw : nw); x += 32) bits[x] = 0u;
     __syncwarp();
     // work items in CTA batches of twice the CTA's warps (draw_batched); the
     // batch word follows the warps' accumulators and bitmaps
@@ -1694,8 +1696,18 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
         const HeavyItem it = items[w];
         const int row = it.row;
         if (ctl.only && !ctl.only[row]) continue;
+        // COUNT takes a row's chunks in pairs (its items k, k + 1 for even
+        // k, one walk over both chunks' columns): half the walks of the A
+        // row, half the lookups; the second item of a pair is skipped here
+        int span = 1;
+        if constexpr (MODE == COUNT) {
+            const int k = w - it.first;
+            if (k & 1) continue;
+            if (w + 1 < nitems && items[w + 1].first == it.first) span = 2;
+        }
+        const int wcw = span << cw_log2;  // columns walked
         const int lo = it.chunk << cw_log2;
-        const int hi = (int)min((int64_t)lo + cw, (int64_t)B.cols);
+        const int hi = (int)min((int64_t)lo + wcw, (int64_t)B.cols);
         if (MODE == REUSE) {
             float4* a4 = reinterpret_cast<float4*>(acc);
             for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1731,7 +1743,7 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
                     if (d >= 0 && aux.dir) {
                         const int c = it.chunk - (m.z >> cw_log2);
                         s = m.z >= lo ? m.x : aux.dir[d + c];
-                        t = m.w < hi ? m.y : aux.dir[d + c + 1];
+                        t = m.w < hi ? m.y : aux.dir[d + c + span];
                         // only an unsorted row (a broken operand) leaves a
                         // directory entry unwritten: stay inside the row
                         s = min(max(s, m.x), m.y);
@@ -1740,9 +1752,12 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
                         s = m.x;  // the whole row lies in the chunk
                         t = m.y;
                     } else if (aux.smask && k >= 0 &&
-                               !((aux.smask[(int64_t)k * aux.smask_words + (it.chunk >> 5)] >>
-                                  (it.chunk & 31)) & 1u)) {
-                        t = s;  // no entry of the row in this chunk
+                               !(((aux.smask[(int64_t)k * aux.smask_words + (it.chunk >> 5)] >>
+                                   (it.chunk & 31)) & 1u) ||
+                                 (span == 2 && ((aux.smask[(int64_t)k * aux.smask_words +
+                                                           ((it.chunk + 1) >> 5)] >>
+                                                 ((it.chunk + 1) & 31)) & 1u)))) {
+                        t = s;  // no entry of the row in this chunk (or pair)
                     } else {
                         s = m.z >= lo ? m.x : seq_lower_bound(B.ci, m.x, m.y, lo);
                         t = m.w < hi ? m.y : seq_lower_bound(B.ci, s, m.y, hi);
@@ -1752,10 +1767,29 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
                 }
             }
             if (__any_sync(FULL, len > 0))
-                heavy_segments<MODE>(B, s, len, av, lo, cw, acc, bits, err);
+                heavy_segments<MODE>(B, s, len, av, lo, wcw, acc, bits, err);
         }
-        heavy_finish<MODE>(B, w, it, row, lo, cw, acc, bits, item_cnt, row_cnt, item_scan, c_rp,
-                           c_ci, c_v, err, ctl);
+        if constexpr (MODE == COUNT) {
+            // each chunk of the walk: its count from its half of the bitmap
+            __syncwarp();
+            for (int h = 0; h < span; ++h) {
+                int c = 0;
+                for (int x = lane; x < nw; x += 32) {
+                    c += __popc(bits[h * nw + x]);
+                    bits[h * nw + x] = 0u;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+                if (lane == 0) {
+                    item_cnt[w + h] = c;
+                    if (c && row_cnt) atomicAdd(&row_cnt[row], c);
+                }
+            }
+            __syncwarp();
+        } else {
+            heavy_finish<MODE>(B, w, it, row, lo, cw, acc, bits, item_cnt, row_cnt, item_scan,
+                               c_rp, c_ci, c_v, err, ctl);
+        }
     }
 }
 
