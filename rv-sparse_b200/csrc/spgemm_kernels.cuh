@@ -1324,10 +1324,11 @@ __global__ void __launch_bounds__(WARPS * 32)
 // ---------------------------------------------------------------------------
 constexpr int HEAVY_SEG = 12;  // in-chunk B segments this long are walked on their own
 
-// COUNT walks two neighbouring chunks of a row at once (k_heavy): a bitmap of
-// 2 cw bits.
+// COUNT walks up to HEAVY_COUNT_SPAN neighbouring chunks of a row at once
+// (k_heavy): a bitmap of HEAVY_COUNT_SPAN cw bits.
+constexpr int HEAVY_COUNT_SPAN = 8;
 __host__ __device__ constexpr int heavy_smem_bytes(int mode, int cw) {
-    return mode == COUNT ? cw / 4 : 4 * cw + (mode == REUSE ? 0 : cw / 8);
+    return mode == COUNT ? HEAVY_COUNT_SPAN * cw / 8 : 4 * cw + (mode == REUSE ? 0 : cw / 8);
 }
 
 // First index in [lo, hi) with a[idx] >= target (hi if none); one thread.
@@ -1644,6 +1645,17 @@ __device__ __forceinline__ void heavy_finish(
     __syncwarp();
 }
 
+// Whether B row k (a row without a directory) has an entry in chunks
+// [c, c + span) by its presence mask (span <= 32: at most two words).
+__device__ __forceinline__ bool heavy_mask_any(const HeavyAux& aux, int k, int c, int span) {
+    const uint32_t* m = aux.smask + (int64_t)k * aux.smask_words;
+    const int w0 = c >> 5, b0 = c & 31;
+    uint64_t bits = m[w0] >> b0;
+    if (b0 + span > 32) bits |= (uint64_t)m[w0 + 1] << (32 - b0);
+    const uint64_t want = span >= 64 ? ~0ull : ((1ull << span) - 1);
+    return (bits & want) != 0;
+}
+
 // Heavy rows: one warp per work item (row, chunk of cw = 2^cw_log2
 // columns), items pulled from a counter (in CTA batches, below) by a grid
 // that fills the GPU once (a warp that drew a light item takes the next one
@@ -1678,7 +1690,7 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
         for (int x = lane; x < (cw >> 2); x += 32) a4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     if (MODE != REUSE)
-        for (int x = lane; x < (MODE == COUNT ? 2 * nw : nw); x += 32) bits[x] = 0u;
+        for (int x = lane; x < (MODE == COUNT ? HEAVY_COUNT_SPAN * nw : nw); x += 32) bits[x] = 0u;
     __syncwarp();
     // work items in CTA batches of twice the CTA's warps (draw_batched); the
     // batch word follows the warps' accumulators and bitmaps
@@ -1696,14 +1708,20 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
         const HeavyItem it = items[w];
         const int row = it.row;
         if (ctl.only && !ctl.only[row]) continue;
-        // COUNT takes a row's chunks in pairs (its items k, k + 1 for even
-        // k, one walk over both chunks' columns): half the walks of the A
-        // row, half the lookups; the second item of a pair is skipped here
+        // COUNT takes a row's chunks HEAVY_COUNT_SPAN at a time (its items
+        // k .. k + span - 1 for k a multiple of the span, one walk over their
+        // columns): fewer walks of the A row, fewer lookups; the other items
+        // of a group are skipped here
         int span = 1;
         if constexpr (MODE == COUNT) {
             const int k = w - it.first;
-            if (k & 1) continue;
-            if (w + 1 < nitems && items[w + 1].first == it.first) span = 2;
+            if (k % HEAVY_COUNT_SPAN) continue;
+            // the group's items that belong to this row (a row's items are
+            // consecutive)
+            const bool same = lane > 0 && lane < HEAVY_COUNT_SPAN && w + lane < nitems &&
+                              items[w + lane].first == it.first;
+            const unsigned m = __ballot_sync(FULL, same) | 1u;
+            span = __ffs(~m) - 1;
         }
         const int wcw = span << cw_log2;  // columns walked
         const int lo = it.chunk << cw_log2;
@@ -1752,12 +1770,8 @@ __global__ void __launch_bounds__(HEAVY_MAX_WARPS * 32)
                         s = m.x;  // the whole row lies in the chunk
                         t = m.y;
                     } else if (aux.smask && k >= 0 &&
-                               !(((aux.smask[(int64_t)k * aux.smask_words + (it.chunk >> 5)] >>
-                                   (it.chunk & 31)) & 1u) ||
-                                 (span == 2 && ((aux.smask[(int64_t)k * aux.smask_words +
-                                                           ((it.chunk + 1) >> 5)] >>
-                                                 ((it.chunk + 1) & 31)) & 1u)))) {
-                        t = s;  // no entry of the row in this chunk (or pair)
+                               !heavy_mask_any(aux, k, it.chunk, span)) {
+                        t = s;  // no entry of the row in these chunks
                     } else {
                         s = m.z >= lo ? m.x : seq_lower_bound(B.ci, m.x, m.y, lo);
                         t = m.w < hi ? m.y : seq_lower_bound(B.ci, s, m.y, hi);
