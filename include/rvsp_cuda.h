@@ -62,7 +62,7 @@ RVSP_CUDA_API void rvsp_cuda_free(void *device_ptr);
  * RVSP_OWNS_HOST; the counterpart of free() at rv-sparse
  * src/core/matrix.c:99-104). Such arrays may also be released with free();
  * through this call arrays of 64 MiB and more are kept (at most 4, within a
- * quarter of host memory, 32 GiB at most) and handed out again to later
+ * sixteenth of host memory, 32 GiB at most) and handed out again to later
  * products, whose copy-back then writes pages already mapped.
  * RVSP_HOST_CACHE=0 in the environment makes it a plain free(). NULL is
  * accepted. */

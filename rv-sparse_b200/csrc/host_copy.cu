@@ -20,7 +20,7 @@
 // again by host_alloc: a fresh array's pages are faulted in and zeroed by
 // the kernel inside the copy (38 GB/s with 16 threads into fresh pages),
 // while a cached one's are already mapped. The cache holds at most 4
-// arrays and a quarter of the host memory (32 GiB at most), frees the
+// arrays and a sixteenth of the host memory (32 GiB at most), frees the
 // oldest first, and RVSP_HOST_CACHE=0 turns it off. It keeps allocations
 // only: every product computes and copies its C in full.
 #include <malloc.h>
@@ -119,9 +119,11 @@ bool cache_on() {
 size_t cache_cap() {
     static const size_t cap = [] {
         const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGESIZE);
-        const size_t quarter = pages > 0 && page > 0 ? (size_t)pages * (size_t)page / 4 : 0;
+        // a sixteenth of host memory: one process per GPU, eight on a box,
+        // keep half of it at most between them
+        const size_t share = pages > 0 && page > 0 ? (size_t)pages * (size_t)page / 16 : 0;
         const size_t max = (size_t)32 << 30;
-        return quarter < max ? quarter : max;
+        return share < max ? share : max;
     }();
     return cap;
 }
