@@ -61,8 +61,11 @@ RANK = int(os.environ.get("RANK", "0"))
 WORLD = int(os.environ.get("WORLD_SIZE", "1"))
 LOCAL_RANK = int(os.environ.get("LOCAL_RANK", "0"))
 if WORLD > 1:
-    # one GPU per process: both this process's CUDA runtimes see it as device 0
-    os.environ["CUDA_VISIBLE_DEVICES"] = str(LOCAL_RANK)
+    # one GPU per process: both this process's CUDA runtimes see it as device
+    # 0 (the LOCAL_RANK-th of the GPUs the launcher made visible, if it chose)
+    _visible = [d for d in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if d.strip()]
+    os.environ["CUDA_VISIBLE_DEVICES"] = (_visible[LOCAL_RANK] if LOCAL_RANK < len(_visible)
+                                          else str(LOCAL_RANK))
 
 sys.path.insert(0, os.path.join(ROOT, "rv-sparse_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
