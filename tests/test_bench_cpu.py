@@ -96,3 +96,19 @@ def test_row_sample_is_a_csr_of_the_sampled_rows():
         assert np.array_equal(S.col_idx[S.row_ptr[i]:S.row_ptr[i + 1]], A.col_idx[a:b])
         assert np.array_equal(S.values[S.row_ptr[i]:S.row_ptr[i + 1]], A.values[a:b])
     assert Ps == int(ops[rows].sum())
+
+
+def test_each_rank_takes_its_own_visible_gpu():
+    """Under a launcher (WORLD_SIZE > 1) a rank keeps only the LOCAL_RANK-th
+    of the GPUs already visible to it (or GPU LOCAL_RANK when none are
+    named), before anything loads CUDA."""
+    import subprocess
+    import sys
+    code = "import os, bench; print(os.environ['CUDA_VISIBLE_DEVICES'])"
+    for visible, rank, want in (("4,5", "1", "5"), ("", "1", "1"), ("2,3,6", "0", "2")):
+        env = dict(os.environ, WORLD_SIZE="2", RANK=rank, LOCAL_RANK=rank,
+                   CUDA_VISIBLE_DEVICES=visible)
+        out = subprocess.run([sys.executable, "-c", code], env=env, cwd=ROOT,
+                             capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr[-500:]
+        assert out.stdout.strip().splitlines()[-1] == want
