@@ -309,8 +309,10 @@ __global__ void __launch_bounds__(256)
 // bookkeeping (all 32 items' loads in flight together), then the warp copies
 // the 32 chunks' entries as one list, 128 entries per step with each lane's
 // four loads issued before its stores; each lane finds its entry's chunk in
-// the scan of the chunks' counts. Items of a row are consecutive, so the
-// stores run contiguously through C.
+// the scan of the chunks' counts. A chunk's source and destination offsets
+// are kept less the chunk's first index in the list, so an entry's two
+// addresses are one shuffle each (40 registers: 6 CTAs per SM). Items of a
+// row are consecutive, so the stores run contiguously through C.
 __global__ void __launch_bounds__(256)
     k_compact_items(const HeavyItem* __restrict__ items, int32_t n,
                     const uint8_t* __restrict__ hmask, const uint8_t* __restrict__ need,
@@ -342,6 +344,8 @@ __global__ void __launch_bounds__(256)
             if (lane >= o) incl += y;
         }
         const int total = __shfl_sync(FULL, incl, 31);
+        src -= incl - k;
+        dst -= incl - k;
         for (int e0 = 0; e0 < total; e0 += 128) {
             int32_t ci[4];
             float v[4];
@@ -354,12 +358,11 @@ __global__ void __launch_bounds__(256)
                 for (int st = 16; st >= 1; st >>= 1)
                     if (__shfl_sync(FULL, incl, j + st - 1) <= e) j += st;
                 j = min(j, 31);
-                const int off = e - (__shfl_sync(FULL, incl, j) - __shfl_sync(FULL, k, j));
-                const int64_t sj = __shfl_sync(FULL, src, j);
-                d[u] = __shfl_sync(FULL, dst, j) + off;
+                const int64_t sj = __shfl_sync(FULL, src, j) + e;
+                d[u] = __shfl_sync(FULL, dst, j) + e;
                 if (e < total) {
-                    ci[u] = tmp_ci[sj + off];
-                    v[u] = tmp_v[sj + off];
+                    ci[u] = tmp_ci[sj];
+                    v[u] = tmp_v[sj];
                 }
             }
 #pragma unroll
