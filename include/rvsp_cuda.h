@@ -65,7 +65,11 @@ RVSP_CUDA_API void rvsp_cuda_free(void *device_ptr);
  * sixteenth of host memory, 32 GiB at most) and handed out again to later
  * products, whose copy-back then writes pages already mapped.
  * RVSP_HOST_CACHE=0 in the environment makes it a plain free(). NULL is
- * accepted. */
+ * accepted.
+ * Pageable host results of 64 MiB and more (and pageable operands of 16 MiB
+ * and more) move through a ring of pinned 32 MiB pieces that host threads
+ * fill or empty while the device copies the next ones; the threads are the
+ * process's cores, 16 at most, or RVSP_HOST_COPY_THREADS (1: plain copies). */
 RVSP_CUDA_API void rvsp_cuda_host_free(void *host_ptr);
 
 /*
