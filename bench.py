@@ -410,7 +410,7 @@ def run_headline(args):
         rv.free_device(*pl)
     nnz_c = int(ranks.sum_over_ranks(dist, int(row_nnz.sum())))
 
-    e2e = run_rmat_e2e(rv, A, ops, panels, args, torch)
+    e2e = run_rmat_e2e(rv, A, ops, panels, args, torch, dist)
     if RANK != 0:
         ranks.barrier(dist)
         if dist:
@@ -495,13 +495,17 @@ def committed_traffic(kernel, bytes_per_launch):
                               "algorithmic byte of a captured launch scaled to this launch"}
 
 
-def run_rmat_e2e(rv, A, ops, panels, args, torch):
+def run_rmat_e2e(rv, A, ops, panels, args, torch, dist=None):
     """The product through rvsp_spgemm_csr (learned backend) on host CSR:
     each panel's A (its row pointer rebased, its entries a view) and B = A are
     host arrays; the library uploads them and hands C back in host arrays
     (staged through pinned memory), freed by rvsp_csr_destroy. Wall time of
-    all panels per step."""
+    this rank's panels per step; with several ranks the timed steps start
+    after a barrier, the time is the slowest rank's and the products and
+    bytes are every rank's (the whole job)."""
     import ctypes as C
+
+    from rvsp_b200 import ranks
     L = rv.lib()
     hb = rv.csr_struct(A.rows, A.cols, A.nnz, A.row_ptr, A.col_idx, A.values)
     pa = []
@@ -526,13 +530,16 @@ def run_rmat_e2e(rv, A, ops, panels, args, torch):
 
     steps = max(1, min(args.steps, args.e2e_steps))
     step()  # warm-up
+    ranks.barrier(dist)
     ts = []
     for _ in range(steps):
         t0 = time.perf_counter()
         step()
         ts.append(time.perf_counter() - t0)
-    t = statistics.mean(ts)
-    P = int(sum(ops[r0:r1].sum() for r0, r1 in panels))
+    t = ranks.max_over_ranks(dist, statistics.mean(ts))
+    P = ranks.sum_over_ranks(dist, int(sum(ops[r0:r1].sum() for r0, r1 in panels)))
+    h2d = ranks.sum_over_ranks(dist, h2d)
+    d2h = ranks.sum_over_ranks(dist, d2h)
     return {"value": round(2.0 * P / t / 1e9, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "steps": steps,
             "api": "rvsp_spgemm_csr (RVSP_BACKEND_CUDA_LEARNED) per row panel, host A/B/C",

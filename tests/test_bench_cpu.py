@@ -112,3 +112,76 @@ def test_each_rank_takes_its_own_visible_gpu():
                              capture_output=True, text=True, timeout=300)
         assert out.returncode == 0, out.stderr[-500:]
         assert out.stdout.strip().splitlines()[-1] == want
+
+
+def _e2e_worker(rank, port, world, out_dir):
+    """One rank of the end-to-end leg with the library replaced by a stand-in
+    that returns a C of 10 entries a panel and takes rank-dependent time."""
+    import ctypes as C
+    import json
+    import time
+    import types
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      LOCAL_RANK=str(rank), WORLD_SIZE=str(world))
+    import rvsp_b200 as rv
+    from rvsp_b200 import ranks
+    bench = _bench()
+    dist = ranks.init("gloo", timeout_s=120)
+
+    class FakeLib:
+        def rvsp_spgemm_csr(self, a, b, c, opts):
+            time.sleep(0.01 * (rank + 1))
+            c._obj.nnz = 10
+            return 0
+
+        def rvsp_csr_destroy(self, c):
+            return 0
+
+    fake = FakeLib()
+    rvf = types.SimpleNamespace(lib=lambda: fake, csr_struct=rv.csr_struct,
+                                SpgemmOptions=rv.SpgemmOptions, CsrMatrix=rv.CsrMatrix,
+                                check=rv.check,
+                                RVSP_BACKEND_CUDA_LEARNED=rv.RVSP_BACKEND_CUDA_LEARNED,
+                                RVSP_DTYPE_FP32=rv.RVSP_DTYPE_FP32)
+    A = gen.rmat(scale=12, edge_factor=16, seed=5)
+    ops = gen.row_products(A, A)
+    panels_all = [(0, 64), (64, 128), (128, 200), (200, A.rows)]
+    panels = ranks.shard_panels(panels_all, ops, rank, world)
+    args = types.SimpleNamespace(steps=2, e2e_steps=2)
+    r = bench.run_rmat_e2e(rvf, A, ops, panels, args, None, dist)
+    with open(os.path.join(out_dir, f"e2e_{rank}.json"), "w") as f:
+        json.dump({"r": r, "panels": panels}, f)
+    ranks.barrier(dist)
+    dist.destroy_process_group()
+
+
+def test_e2e_leg_reports_the_whole_job_over_two_ranks(tmp_path):
+    """With two ranks the end-to-end number covers every rank's panels: the
+    products and bytes of both, over the slower rank's time, identical on
+    both ranks (what rank 0 prints)."""
+    import json
+    import socket
+
+    import torch.multiprocessing as mp
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    mp.spawn(_e2e_worker, args=(port, 2, str(tmp_path)), nprocs=2, join=True)
+    res = [json.load(open(tmp_path / f"e2e_{r}.json")) for r in range(2)]
+    A = gen.rmat(scale=12, edge_factor=16, seed=5)
+    ops = gen.row_products(A, A)
+    assert res[0]["r"] == res[1]["r"]
+    owned = [tuple(p) for x in res for p in x["panels"]]
+    assert sorted(owned) == [(0, 64), (64, 128), (128, 200), (200, A.rows)]
+    r = res[0]["r"]
+    # 10 C entries a panel (8 bytes each) plus each panel's row pointer
+    assert r["d2h_bytes_per_step"] == sum(4 * (r1 - r0 + 1) + 80 for r0, r1 in owned)
+    h2d = sum(4 * (r1 - r0 + 1 + A.rows + 1) + 8 * (int(A.row_ptr[r1] - A.row_ptr[r0]) + A.nnz)
+              for r0, r1 in owned)
+    assert r["h2d_bytes_per_step"] == h2d
+    # every rank's products over the slower rank's time (20 ms a call on rank 1)
+    assert r["ms_per_step"] >= 0.02 * len(res[1]["panels"]) * 1e3
+    want = 2.0 * int(ops.sum()) / (r["ms_per_step"] * 1e-3) / 1e9
+    assert abs(r["value"] - want) <= 0.01 * want
